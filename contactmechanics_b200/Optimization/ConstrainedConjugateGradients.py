@@ -1,0 +1,182 @@
+"""Polonsky-Keer constrained conjugate gradients on the B200.
+
+Drop-in for ``constrained_conjugate_gradients`` of
+ContactMechanics/Optimization/ConstrainedConjugateGradients.py (v1.8.3):
+same arguments, same ``OptimizeResult`` fields, same exceptions.  The whole
+iteration -- both operator applications, every masked reduction, the step
+length, the projection onto [0, hardness], the load constraint, the
+mixing step with its offset bisection and the convergence test -- runs on
+the device (``cm_ccg_solve`` of libcm_b200.so); the host only polls a
+convergence flag every few iterations.
+
+Differences that follow from keeping the loop on the device:
+* ``callback`` and ``logger`` see the final iteration only (the reference
+  calls them every iteration, :436-489);
+* masked (``np.ma``) heights and MPI domain decomposition are not supported;
+* a scalar ``hardness`` must be positive (the reference fails later, inside
+  its bisection, for ``hardness == 0``).
+
+Extra keyword ``precision``: "fp64" (default; reference arithmetic),
+"mixed" (FP32 fields and FFTs with FP64 reductions, then FP64 refinement
+iterations warm-started from the FP32 forces) or "fp32".
+"""
+import ctypes
+
+import numpy as np
+import scipy.optimize as optim
+
+from .. import _lib
+from ..Tools.Logger import quiet
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _device_f64(a, shape=None):
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        t = a.to(device="cuda", dtype=torch.float64).contiguous()
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64))).to("cuda")
+    if shape is not None:
+        t = t.reshape(shape)
+    return t
+
+
+def constrained_conjugate_gradients(substrate, topography, hardness=None, external_force=None,
+                                    offset=None, initial_displacements=None,
+                                    initial_forces=None, pentol=None, forcetol=1e-5,
+                                    thermotol=1e-6, mixfac=0.1, mixdecfac=0.95,
+                                    minmixsteps=10, maxiter=100000, logger=quiet,
+                                    callback=None, verbose=False, precision="fp64",
+                                    check_every=None, timeout=None):
+    """Equilibrium of an elastic half-space against a rigid topography
+    (ConstrainedConjugateGradients.py:47-509).
+
+    Returns a ``scipy.optimize.OptimizeResult`` with ``x`` (displacements on
+    the full domain), ``jac`` (forces on the topography, positive in
+    compression), ``active_set``, ``offset``, ``fun`` (elastic energy),
+    ``success``, ``message``, ``nit``, ``nfev``, ``maxcv`` and, with a
+    hardness, ``plastic``.
+    """
+    torch = _torch()
+    plan = getattr(substrate, "_plan", None)
+    if plan is None:
+        raise ValueError("substrate must be a contactmechanics_b200 half-space")
+    if not hasattr(topography, "nb_grid_pts"):
+        heights = topography
+    else:
+        heights = topography.heights()
+    if np.ma.isMaskedArray(heights):
+        raise NotImplementedError("masked topographies are not supported on the device path")
+    if substrate.dim not in (1, 2):
+        raise Exception(
+            f"Constrained conjugate gradient currently only implemented for 1 or 2 dimensions "
+            f"(Your substrate has {substrate.dim}.).")
+    as_torch = isinstance(heights, torch.Tensor) and heights.is_cuda
+    nb = tuple(substrate.nb_grid_pts)
+    tshape = nb if substrate.dim == 2 else (nb[0], 1)
+    dom = tuple(substrate.nb_domain_grid_pts)
+    dshape = dom if substrate.dim == 2 else (dom[0], 1)
+    if tuple(heights.shape) != nb:
+        raise ValueError("topography shape {} does not match the substrate's nb_grid_pts {}"
+                         .format(tuple(heights.shape), nb))
+    if hardness is not None:
+        h_arr = np.asarray(hardness.cpu() if isinstance(hardness, torch.Tensor) else hardness)
+        if h_arr.size != 1:
+            raise ValueError("The truth value of an array with more than one element is "
+                             "ambiguous. Use a.any() or a.all()")
+        hardness = float(h_arr)
+        if not hardness > 0:
+            raise ValueError("hardness must be positive")
+    if precision not in _lib.PRECISIONS:
+        raise ValueError("precision must be one of {}".format(sorted(_lib.PRECISIONS)))
+
+    h_dev = _device_f64(heights, tshape)
+    u0 = _device_f64(initial_displacements, dshape) if initial_displacements is not None else None
+    f0 = _device_f64(initial_forces, dshape) if initial_forces is not None else None
+    x = torch.empty(dshape, dtype=torch.float64, device="cuda")
+    jac = torch.empty(tshape, dtype=torch.float64, device="cuda")
+    active = torch.empty(tshape, dtype=torch.uint8, device="cuda")
+    plastic = torch.empty(tshape, dtype=torch.uint8, device="cuda") if hardness is not None else None
+
+    P = _lib.CcgParams()
+    P.precision = _lib.PRECISIONS[precision]
+    P.load_control = int(external_force is not None)
+    P.external_force = float(external_force) if external_force is not None else 0.0
+    P.offset = float(offset) if offset is not None else 0.0
+    P.has_hardness = int(hardness is not None)
+    P.hardness = hardness if hardness is not None else 0.0
+    P.pentol = float(pentol) if pentol is not None else -1.0
+    P.forcetol = float(forcetol)
+    P.thermotol = float(thermotol)
+    P.mixfac = float(mixfac)
+    P.mixdecfac = float(mixdecfac)
+    P.minmixsteps = int(minmixsteps)
+    P.maxiter = int(maxiter)
+    P.check_every = int(check_every) if check_every else 0
+    P.timeout_s = float(timeout) if timeout else 0.0
+    res = _lib.CcgResult()
+
+    def ptr(t):
+        return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+    torch.cuda.current_stream().synchronize()
+    code = plan._L.cm_ccg_solve(plan.ptr, ctypes.byref(P), ptr(h_dev), ptr(u0), ptr(f0),
+                                ptr(x), ptr(jac), ptr(active), ptr(plastic), ctypes.byref(res))
+    if code == _lib.CM_ERR_NAN:
+        raise RuntimeError("nan encountered.")
+    if code == _lib.CM_ERR_BISECT:
+        raise ValueError("f(a) and f(b) must have different signs")
+    if code == _lib.CM_ERR_BISECT_CONV:
+        raise RuntimeError("Failed to converge after 100 iterations")
+    _lib.check(code)
+
+    result = optim.OptimizeResult()
+    result.nit = res.nit
+    result.nfev = res.nfev
+    result.nit_fp32 = res.nit_fp32
+    result.success = res.status == _lib.CM_SOLVE_CONVERGED
+    result.message = ("Polonsky converged" if result.success
+                      else "Reached maxiter = {}".format(maxiter))
+    result.maxcv = {"max_pen": res.max_pen, "max_pres": res.max_pres}
+    result.offset = res.offset
+    result.fun = res.fun
+    result.pentol = res.pentol_used
+
+    # active set over the full domain (False on the padding)
+    act_dom = torch.zeros(dshape, dtype=torch.bool, device="cuda")
+    act_dom[:tshape[0], :tshape[1]] = active.bool()
+    if substrate.dim == 1:
+        x, jac, act_dom = x.reshape(dom), jac.reshape(nb), act_dom.reshape(dom)
+        if plastic is not None:
+            plastic = plastic.reshape(nb)
+    if as_torch:
+        result.x, result.jac, result.active_set = x, jac, act_dom
+        if plastic is not None and result.success:
+            result.plastic = plastic.bool()
+    else:
+        result.x = x.cpu().numpy()
+        result.jac = jac.cpu().numpy()
+        result.active_set = act_dom.cpu().numpy()
+        if plastic is not None and result.success:
+            result.plastic = plastic.bool().cpu().numpy()
+
+    log_headers = ["status", "it", "area", "cg area", "total force", "offset"]
+    log_values = ["CONVERGED" if result.success else "NOT CONVERGED", res.nit, res.area,
+                  res.cg_area, res.total_force, res.offset]
+    if verbose:
+        log_headers += ["rms pen.", "max. pen.", "max. force", "max. pad force", "max. du"]
+        log_values += [res.rms_pen, res.max_pen, res.max_pres, res.pad_pres, res.maxdu]
+    logger.pr(f"maxiter = {maxiter}")
+    logger.pr(f"pentol = {res.pentol_used}")
+    logger.st(log_headers, log_values, force_print=True)
+    if callback is not None:
+        callback(res.nit, -result.jac,
+                 dict(area=int(res.area), rms_penetration=res.rms_pen,
+                      max_penetration=res.max_pen, max_pressure=res.max_pres,
+                      pad_pressure=res.pad_pres, penetration_tol=res.pentol_used,
+                      pressure_tol=forcetol))
+    return result

@@ -1,0 +1,2 @@
+"""Optimization algorithms (ContactMechanics/Optimization/__init__.py)."""
+from .ConstrainedConjugateGradients import constrained_conjugate_gradients  # noqa: F401

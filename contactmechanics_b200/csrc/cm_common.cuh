@@ -1,0 +1,78 @@
+// Common device helpers for the contact-mechanics CUDA library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CM_DEVINL __device__ __forceinline__
+
+template <typename R> struct CT;
+template <> struct CT<float> { typedef float2 C; };
+template <> struct CT<double> { typedef double2 C; };
+
+template <typename C> CM_DEVINL C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C> CM_DEVINL C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename C> CM_DEVINL C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+// a * conj(b)
+template <typename C> CM_DEVINL C cmulc(C a, C b) {
+  C r;
+  r.x = a.x * b.x + a.y * b.y;
+  r.y = a.y * b.x - a.x * b.y;
+  return r;
+}
+template <typename C> CM_DEVINL C cconj(C a) { a.y = -a.y; return a; }
+template <typename C, typename R> CM_DEVINL C cscale(C a, R s) { a.x *= s; a.y *= s; return a; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename C> CM_DEVINL C mul_mi(C a) {
+  C r;
+  if (INV) { r.x = -a.y; r.y = a.x; }
+  else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+template <typename C> CM_DEVINL C czero() { C r; r.x = 0; r.y = 0; return r; }
+template <typename C, typename R> CM_DEVINL C cmake(R x, R y) { C r; r.x = x; r.y = y; return r; }
+
+enum { RED_SUM = 0, RED_MAX = 1, RED_MIN = 2 };
+
+CM_DEVINL double red_neutral(int kind) {
+  return kind == RED_SUM ? 0.0 : (kind == RED_MAX ? -INFINITY : INFINITY);
+}
+CM_DEVINL double red_apply(int kind, double a, double b) {
+  return kind == RED_SUM ? a + b : (kind == RED_MAX ? fmax(a, b) : fmin(a, b));
+}
+
+// Reduce NV doubles across the block with a fixed tree (deterministic).
+// kinds[i] selects sum / max / min.  Result valid in thread 0.
+// `sm` must hold 32*NV doubles.  All threads must call.
+template <int NV>
+CM_DEVINL void block_reduce(double (&v)[NV], const int (&kinds)[NV], double* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v[i] = red_apply(kinds[i], v[i], __shfl_xor_sync(0xffffffffu, v[i], o));
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) sm[i * 32 + warp] = v[i];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double x = lane < nw ? sm[i * 32 + lane] : red_neutral(kinds[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+        x = red_apply(kinds[i], x, __shfl_xor_sync(0xffffffffu, x, o));
+      v[i] = x;
+    }
+  }
+  __syncthreads();
+}

@@ -1,0 +1,946 @@
+// Host side of libcm_b200: plans, Green's tables, operator application and
+// the constrained-conjugate-gradient driver behind the C ABI of cm_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cm_b200.h"
+#include "cm_kernels.cuh"
+
+#define CM_MAXE32 32
+#define CM_MAXE64 16
+#define CM_SMEM_BUDGET (64 * 1024)
+#define CM_ELEMS_TARGET 4096
+#define CM_COMP_ELEMS 8192
+#define CM_BISECT_PASSES 21
+#define CM_MAX_PARTIAL_VALS 32
+
+#define CK(...)                               \
+  do {                                        \
+    cudaError_t e_ = (__VA_ARGS__);           \
+    if (e_ != cudaSuccess) {                  \
+      last_cuda_error() = e_;                 \
+      return CM_ERR_CUDA;                     \
+    }                                         \
+  } while (0)
+
+#define CKS(...)                     \
+  do {                               \
+    int s_ = (__VA_ARGS__);          \
+    if (s_ != CM_OK) return s_;      \
+  } while (0)
+
+static cudaError_t& last_cuda_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// FFT descriptors and twiddles
+// ---------------------------------------------------------------------------
+static bool make_fft_desc(int n, FftDesc* d) {
+  memset(d, 0, sizeof(*d));
+  d->n = n;
+  int m = n, k = 0;
+  auto push = [&](int r) {
+    if (k >= CM_MAX_STAGES) return false;
+    d->rad[k++] = r;
+    return true;
+  };
+  while (m % 8 == 0 && m >= 8) { if (!push(8)) return false; m /= 8; }
+  while (m % 4 == 0) { if (!push(4)) return false; m /= 4; }
+  while (m % 2 == 0) { if (!push(2)) return false; m /= 2; }
+  const int small[3] = {3, 5, 7};
+  for (int p : small)
+    while (m % p == 0) { if (!push(p)) return false; m /= p; }
+  for (int p = 11; m > 1; p += 2) {
+    while (m % p == 0) {
+      if (!push(p)) return false;
+      d->generic = 1;
+      m /= p;
+    }
+  }
+  d->nst = k;
+  return true;
+}
+
+template <typename C>
+static std::vector<C> make_twiddles(int n) {
+  std::vector<C> tw(n);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = -two_pi * (long double)m / (long double)n;
+    tw[m].x = (decltype(tw[m].x))cosl(a);
+    tw[m].y = (decltype(tw[m].y))sinl(a);
+  }
+  return tw;
+}
+
+// elements a thread holds in the worst stage of a transform of nseq sequences
+static bool fits_regs(const FftDesc& d, long nseq, int maxe) {
+  for (int s = 0; s < d.nst; ++s) {
+    const int r = d.rad[s];
+    if (r > 8 || r == 6) continue;  // generic stages use no register staging
+    const long B = (long)d.n / r * nseq;
+    const long nb = (B + CM_THREADS - 1) / CM_THREADS;
+    if (nb > (maxe + r - 1) / r) return false;
+  }
+  return true;
+}
+
+struct Tiles {
+  int row_tile, col_tile, comp_rows;
+  size_t smem_row, smem_col;
+};
+
+static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, const FftDesc& fx,
+                        const FftDesc& fy, size_t csize, int maxe, Tiles* t) {
+  const int gy = fy.generic ? 2 : 1, gx = fx.generic ? 2 : 1;
+  // rows: pairs of real rows per block
+  int max_pairs = (nx + 1) / 2;
+  int want = std::max(1, CM_ELEMS_TARGET / ny);
+  int np = std::min(max_pairs, want);
+  while (np > 1 && ((size_t)np * ny * csize * gy > CM_SMEM_BUDGET || !fits_regs(fy, np, maxe))) --np;
+  if ((size_t)np * ny * csize * gy > 200 * 1024 || !fits_regs(fy, np, maxe)) return CM_ERR_SIZE;
+  t->row_tile = 2 * np;
+  t->smem_row = (size_t)np * ny * csize * gy;
+  // columns of the half spectrum per block
+  int w = std::min(nyh, std::max(1, CM_ELEMS_TARGET / nx));
+  while (w > 1 && ((size_t)w * nx * csize * gx > CM_SMEM_BUDGET || !fits_regs(fx, w, maxe))) --w;
+  if ((size_t)w * nx * csize * gx > 200 * 1024 || !fits_regs(fx, w, maxe)) return CM_ERR_SIZE;
+  t->col_tile = w;
+  t->smem_col = (size_t)w * nx * csize * gx;
+  t->comp_rows = std::max(1, std::min(tx, CM_COMP_ELEMS / std::max(1, ty)));
+  return CM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Green's-function tables (FP64 on the device)
+// ---------------------------------------------------------------------------
+__global__ void k_table_periodic(double* G, int nx, int ny, int nyh, double sx, double sy,
+                                 double Es, double young, double poisson, int q0_mode,
+                                 double q0_val, double thick, int dim) {
+  const double pi = 3.14159265358979323846;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nx * nyh;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(idx / nyh), k = (int)(idx % nyh);
+    const double qx = ((x <= nx / 2) ? (double)x : (double)(nx - x)) / sx;
+    const double qy = (double)k / sy;
+    const double q = sqrt(qx * qx + qy * qy);
+    double K = (pi * Es) * q;
+    if (thick > 0 && dim == 2) {
+      const double qq = q * (2 * pi * thick);
+      const double fac = 3 - 4 * poisson;
+      const double off = 4 * poisson * (2 * poisson - 3) + 5;
+      double corr = (fac * cosh(2 * qq) + 2 * (qq * qq) + off) / (fac * sinh(2 * qq) - 2 * qq);
+      if (isnan(corr)) corr = 1.0;
+      K *= corr;
+    }
+    if (x == 0 && k == 0) {
+      if (thick > 0 && dim == 2) {
+        K = young / thick * (1 - poisson) / ((1 - 2 * poisson) * (1 + poisson));
+      } else if (q0_mode == CM_Q0_DEFAULT) {
+        K = (dim == 1) ? (pi * Es) * (1.0 / sx) : ((pi * Es) * (1.0 / sx) + (pi * Es) * (1.0 / sy)) / 2;
+      } else if (q0_mode == CM_Q0_ZERO) {
+        K = 1.0;
+      } else {
+        K = q0_val;
+      }
+    }
+    double g = 1.0 / K;
+    if (x == 0 && k == 0 && q0_mode == CM_Q0_ZERO) g = 0.0;
+    G[idx] = g;
+  }
+}
+
+// Displacement of a uniformly loaded dx x dy pixel (Love / Johnson p.54) on
+// the doubled domain, coordinates wrapped at i > nx.
+__global__ void k_love(double* out, int tx, int ty, int nxd, int nyd, double dx, double dy,
+                       double young) {
+  const double pi = 3.14159265358979323846;
+  const double a = dx * 0.5, b = dy * 0.5;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nxd * nyd;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / nyd), j = (int)(idx % nyd);
+    const double x = (double)(i <= tx ? i : i - 2 * tx) * dx;
+    const double y = (double)(j <= ty ? j : j - 2 * ty) * dy;
+    const double xp = x + a, xm = x - a, yp = y + b, ym = y - b;
+    const double r_pp = sqrt(yp * yp + xp * xp), r_mp = sqrt(ym * ym + xp * xp);
+    const double r_pm = sqrt(yp * yp + xm * xm), r_mm = sqrt(ym * ym + xm * xm);
+    const double v = xp * log((yp + r_pp) / (ym + r_mp)) + yp * log((xp + r_pp) / (xm + r_pm)) +
+                     xm * log((ym + r_mm) / (yp + r_pm)) + ym * log((xm + r_mm) / (xp + r_mp));
+    out[idx] = 1 / (pi * young) * v;
+  }
+}
+
+__global__ void k_real_part(const double2* spec, double* G, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    G[i] = spec[i].x;
+}
+
+// Scaled operator tables: disp = -G/(a N), force = -K a / N with K = 1/G (G != 0).
+__global__ void k_tables_scale(const double* G, long n, double aN_inv, double a_over_N,
+                               double* td, double* tf, float* td32, float* tf32) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double g = G[i];
+    const double k = (g != 0.0) ? 1.0 / g : 0.0;
+    const double d = -g * aN_inv, f = -k * a_over_N;
+    td[i] = d;
+    tf[i] = f;
+    td32[i] = (float)d;
+    tf32[i] = (float)f;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CCG preparation and result kernels
+// ---------------------------------------------------------------------------
+// heights -> working precision; max, min and sum of the heights.
+template <typename R>
+__global__ void __launch_bounds__(CM_THREADS)
+k_h_prep(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>& S = slots[item.x];
+  double mx = -INFINITY, mn = INFINITY, sm = 0;
+  CM_COMP_LOOP(S, item.y) {
+    const size_t ic = (size_t)cx0 * S.ty + e;
+    const double h = h64[ic];
+    const_cast<R*>(S.h)[ic] = (R)h;
+    mx = fmax(mx, h);
+    mn = fmin(mn, h);
+    sm += h;
+  }
+  double v[3] = {mx, mn, sm};
+  const int kinds[3] = {RED_MAX, RED_MIN, RED_SUM};
+  tile_finish<3>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[3]) {
+    S.st->p.max_surface = a[0];
+    S.st->gmin = a[1];  // scratch until the loop starts
+    S.st->sum_cg = a[2];
+  });
+}
+
+// rms height and the reference's default penetration tolerance
+// (ConstrainedConjugateGradients.py:150-162); FP32 phases widen pentol.
+template <typename R>
+__global__ void __launch_bounds__(CM_THREADS)
+k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64,
+        int pentol_auto, double rel_pentol) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>& S = slots[item.x];
+  const double mean = S.st->sum_cg / S.st->p.n_surface;
+  double v2 = 0;
+  CM_COMP_LOOP(S, item.y) {
+    const double d = h64[(size_t)cx0 * S.ty + e] - mean;
+    v2 += d * d;
+  }
+  double v[1] = {v2};
+  const int kinds[1] = {RED_SUM};
+  tile_finish<1>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[1]) {
+    CcgState& s = *S.st;
+    if (pentol_auto) {
+      const double rms = sqrt(a[0] / s.p.n_surface);
+      double pt = rms / (10.0 * (0.5 * ((double)S.tx + (double)S.ty)));
+      if (pt == 0) pt = (s.p.offset0 + s.sum_cg / s.p.n_surface) / 1000;
+      if (pt == 0) pt = 1e-3;
+      s.p.pentol = pt;
+    }
+    if (rel_pentol > 0) s.p.pentol = fmax(s.p.pentol, rel_pentol * (s.p.max_surface - s.gmin));
+    s.gmin = 0;
+    s.sum_cg = 0;
+  });
+}
+
+// initial displacement: given or zero, lifted onto the surface on the
+// topography region (ConstrainedConjugateGradients.py:168-201)
+template <typename R>
+__global__ void k_init_u(Slot<R> S, const double* u0, double offset) {
+  const long n = (long)S.nx * S.ny;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / S.ny), y = (int)(i % S.ny);
+    double u = u0 ? u0[i] : 0.0;
+    if (x < S.tx && y < S.ty) {
+      const double lo = (double)S.h[(size_t)x * S.ty + y] + offset;
+      u = (u < lo) ? lo : u;
+    }
+    S.u[i] = (R)u;
+  }
+}
+
+// copy the topography part of a domain-sized FP64 force field
+template <typename R>
+__global__ void k_init_f(Slot<R> S, const double* f0, int ld) {
+  const long n = (long)S.tx * S.ty;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / S.ty), y = (int)(i % S.ty);
+    S.f[0][i] = (R)f0[(size_t)x * ld + y];
+  }
+}
+
+// result.x, result.jac, active_set, plastic and the elastic energy
+// (ConstrainedConjugateGradients.py:454-475, 494-509)
+template <typename R>
+__global__ void __launch_bounds__(CM_THREADS)
+k_ccg_result(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, double* jac,
+             unsigned char* active, unsigned char* plastic) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>& S = slots[item.x];
+  const CcgState* st = S.st;
+  const int par = st->parity, has_h = st->p.has_h, mixing = (st->branch == 1);
+  const double H = st->p.H;
+  const R* ff = S.f[par];       // final force
+  const R* fa = S.f[par ^ 1];   // force at the start of the last iteration
+  double e_sum = 0, area = 0, cg_area = 0, pl = 0;
+  CM_COMP_LOOP(S, item.y) {
+    const int r = e / S.ty, y = e - r * S.ty;
+    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
+    const R f = ff[ic];
+    const R u = S.u[(size_t)(cx0 + r) * S.ny + y];
+    e_sum += (double)f * (double)u;
+    if (jac) jac[ic] = -(double)f;
+    area += (f < 0);
+    bool act;
+    if (mixing) act = S.gneg[ic] != 0;
+    else {
+      const R a = fa[ic];
+      act = (a < 0) && (!has_h || (double)a > -H);
+    }
+    cg_area += act;
+    if (active) active[ic] = act;
+    if (has_h) {
+      const bool p = S.gneg[ic] != 0;
+      pl += p;
+      if (plastic) plastic[ic] = p;
+    }
+  }
+  double v[4] = {e_sum, area, cg_area, pl};
+  const int kinds[4] = {RED_SUM, RED_SUM, RED_SUM, RED_SUM};
+  tile_finish<4>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[4]) {
+    CcgState& s = *S.st;
+    s.sum_cgt = -a[0] / 2;  // result.fun
+    s.A_contact = (long long)a[1];
+    s.A_cg = (long long)a[2];
+    s.A_fl = (long long)a[3];
+  });
+}
+
+template <typename R>
+__global__ void k_to_f64(const R* src, double* dst, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+// force field of one precision -> FP64 domain-sized field (zero padding)
+template <typename R>
+__global__ void k_force_to_domain(const R* f, int tx, int ty, double* out, int nx, int ny) {
+  const long n = (long)nx * ny;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / ny), y = (int)(i % ny);
+    out[i] = (x < tx && y < ty) ? (double)f[(size_t)x * ty + y] : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+template <typename R>
+struct Work {
+  typedef typename CT<R>::C C;
+  Tiles tiles{};
+  C* twx = nullptr;
+  C* twy = nullptr;
+  C* spec = nullptr;
+  R* tab[2] = {nullptr, nullptr};
+  Slot<R>* d_plain = nullptr;  // slot used by cm_apply
+  Slot<R>* d_ccg = nullptr;    // slot used by the solver
+  // solver fields
+  R* h = nullptr;
+  R* u = nullptr;
+  R* f[2] = {nullptr, nullptr};
+  R* t = nullptr;
+  unsigned char* gneg = nullptr;
+  CcgState* st = nullptr;
+  double* partials = nullptr;
+  unsigned int* counter = nullptr;
+  bool ccg_ready = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
+  int graph_iters[2] = {0, 0};
+  int nt_comp = 0, nt_rowt = 0, nt_rowd = 0, nt_col = 0;
+};
+
+struct cm_plan {
+  cm_plan_desc d;
+  int nx, ny, nyh, tx, ty;
+  FftDesc fx, fy;
+  cudaStream_t stream;
+  bool own_stream;
+  double* G = nullptr;
+  double* tab64[2] = {nullptr, nullptr};
+  float* tab32[2] = {nullptr, nullptr};
+  int2* items = nullptr;
+  int max_items = 0;
+  Work<float> w32;
+  Work<double> w64;
+  CcgState* h_state = nullptr;  // pinned readback
+  std::vector<void*> allocs;
+};
+
+static int dev_alloc(cm_plan* p, void** ptr, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    last_cuda_error() = e;
+    cudaGetLastError();
+    return CM_ERR_OOM;
+  }
+  p->allocs.push_back(*ptr);
+  return CM_OK;
+}
+
+template <typename T>
+static int dalloc(cm_plan* p, T** ptr, size_t count) {
+  return dev_alloc(p, reinterpret_cast<void**>(ptr), count * sizeof(T));
+}
+
+static int grid_for(long n) {
+  long g = (n + 255) / 256;
+  if (g > 148L * 16) g = 148L * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+template <typename R, int MAXE>
+static void set_smem_attrs() {
+  static bool done = false;
+  if (done) return;
+  done = true;
+  const int mx = 200 * 1024;
+  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MAXE, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
+template <typename R>
+static Slot<R> base_slot(cm_plan* p, Work<R>& w) {
+  Slot<R> s;
+  memset(&s, 0, sizeof(s));
+  s.nx = p->nx;
+  s.ny = p->ny;
+  s.nyh = p->nyh;
+  s.tx = p->tx;
+  s.ty = p->ty;
+  s.row_tile = w.tiles.row_tile;
+  s.col_tile = w.tiles.col_tile;
+  s.comp_rows = w.tiles.comp_rows;
+  s.nt_comp = (p->tx + s.comp_rows - 1) / s.comp_rows;
+  s.nt_rowt = (p->tx + s.row_tile - 1) / s.row_tile;
+  s.nt_rowd = (p->nx + s.row_tile - 1) / s.row_tile;
+  s.nt_col = (p->nyh + s.col_tile - 1) / s.col_tile;
+  s.fx = p->fx;
+  s.fy = p->fy;
+  s.twx = w.twx;
+  s.twy = w.twy;
+  s.spec = w.spec;
+  s.tab[0] = w.tab[0];
+  s.tab[1] = w.tab[1];
+  s.h = w.h;
+  s.u = w.u;
+  s.f[0] = w.f[0];
+  s.f[1] = w.f[1];
+  s.t = w.t;
+  s.gneg = w.gneg;
+  s.st = w.st;
+  s.partials = w.partials;
+  s.counter = w.counter;
+  return s;
+}
+
+template <typename R>
+static int init_work(cm_plan* p, Work<R>& w, int maxe) {
+  typedef typename CT<R>::C C;
+  CKS(choose_tiles(p->nx, p->ny, p->nyh, p->tx, p->ty, p->fx, p->fy, sizeof(C), maxe, &w.tiles));
+  std::vector<C> twx = make_twiddles<C>(p->nx), twy = make_twiddles<C>(p->ny);
+  CKS(dalloc(p, &w.twx, p->nx));
+  CKS(dalloc(p, &w.twy, p->ny));
+  CK(cudaMemcpy(w.twx, twx.data(), sizeof(C) * p->nx, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(w.twy, twy.data(), sizeof(C) * p->ny, cudaMemcpyHostToDevice));
+  CKS(dalloc(p, &w.spec, (size_t)p->nx * p->nyh));
+  CKS(dalloc(p, &w.d_plain, 1));
+  CKS(dalloc(p, &w.d_ccg, 1));
+  // reduction scratch is shared by the plain-operator slot and the solver
+  const int nt_max = std::max({(p->tx + w.tiles.comp_rows - 1) / w.tiles.comp_rows,
+                               (p->nx + w.tiles.row_tile - 1) / w.tiles.row_tile,
+                               (p->nyh + w.tiles.col_tile - 1) / w.tiles.col_tile, 1});
+  CKS(dalloc(p, &w.partials, (size_t)nt_max * CM_MAX_PARTIAL_VALS));
+  CKS(dalloc(p, &w.counter, 1));
+  CK(cudaMemset(w.counter, 0, sizeof(unsigned int)));
+  CKS(dalloc(p, &w.st, 1));
+  if (nt_max > p->max_items) p->max_items = nt_max;
+  return CM_OK;
+}
+
+template <typename R>
+static int ensure_ccg(cm_plan* p, Work<R>& w) {
+  if (w.ccg_ready) return CM_OK;
+  const size_t nt = (size_t)p->tx * p->ty, nd = (size_t)p->nx * p->ny;
+  CKS(dalloc(p, &w.h, nt));
+  CKS(dalloc(p, &w.u, nd));
+  CKS(dalloc(p, &w.f[0], nt));
+  CKS(dalloc(p, &w.f[1], nt));
+  CKS(dalloc(p, &w.t, nt));
+  CKS(dalloc(p, &w.gneg, nt));
+  CK(cudaMemsetAsync(w.t, 0, nt * sizeof(R), p->stream));
+  CK(cudaMemsetAsync(w.gneg, 0, nt, p->stream));
+  Slot<R> s = base_slot(p, w);
+  w.nt_comp = s.nt_comp;
+  w.nt_rowt = s.nt_rowt;
+  w.nt_rowd = s.nt_rowd;
+  w.nt_col = s.nt_col;
+  CK(cudaMemcpyAsync(w.d_ccg, &s, sizeof(s), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  w.ccg_ready = true;
+  return CM_OK;
+}
+
+template <typename R, int MAXE>
+static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R* in, int in_rows,
+                        int in_cols, int in_ld, R* out, int out_rows, int out_cols, int out_ld,
+                        cudaStream_t s) {
+  set_smem_attrs<R, MAXE>();
+  Slot<R> hs = base_slot(p, w);
+  hs.in = in;
+  hs.out = out;
+  hs.in_rows = in_rows;
+  hs.in_cols = in_cols;
+  hs.in_ld = in_ld;
+  hs.out_rows = out_rows;
+  hs.out_cols = out_cols;
+  hs.out_ld = out_ld;
+  hs.table_sel = table_sel;
+  CK(cudaMemcpyAsync(w.d_plain, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+  const int nt_in = (in_rows + hs.row_tile - 1) / hs.row_tile;
+  const int nt_out = (out_rows + hs.row_tile - 1) / hs.row_tile;
+  if (mode == MODE_FWD) {
+    k_row_fwd<R, MAXE, MODE_FWD><<<nt_in, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+    k_col<R, MAXE, MODE_FWD><<<hs.nt_col, CM_THREADS, w.tiles.smem_col, s>>>(w.d_plain, p->items);
+  } else {
+    k_row_fwd<R, MAXE, MODE_PLAIN><<<nt_in, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+    k_col<R, MAXE, MODE_PLAIN><<<hs.nt_col, CM_THREADS, w.tiles.smem_col, s>>>(w.d_plain, p->items);
+    k_row_inv<R, MAXE, MODE_PLAIN><<<nt_out, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+  }
+  CK(cudaGetLastError());
+  return CM_OK;
+}
+
+static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int in_rows, int in_cols,
+                          int in_ld, void* out, int out_rows, int out_cols, int out_ld, cudaStream_t s) {
+  if (precision == CM_FP64)
+    return launch_plain<double, CM_MAXE64>(p, p->w64, MODE_PLAIN, op, (const double*)in, in_rows, in_cols,
+                                           in_ld, (double*)out, out_rows, out_cols, out_ld, s);
+  return launch_plain<float, CM_MAXE32>(p, p->w32, MODE_PLAIN, op, (const float*)in, in_rows, in_cols,
+                                        in_ld, (float*)out, out_rows, out_cols, out_ld, s);
+}
+
+// ---------------------------------------------------------------------------
+// solver driver
+// ---------------------------------------------------------------------------
+template <typename R, int MAXE>
+static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s) {
+  const Slot<R>* S = w.d_ccg;
+  const int2* it = p->items;
+  const Tiles& T = w.tiles;
+  k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  if (bisect)
+    for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  k_ccg_gsum<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  k_row_fwd<R, MAXE, MODE_T><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
+  k_col<R, MAXE, MODE_T><<<w.nt_col, CM_THREADS, T.smem_col, s>>>(S, it);
+  k_row_inv<R, MAXE, MODE_T><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
+  k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  k_row_fwd<R, MAXE, MODE_F><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
+  k_col<R, MAXE, MODE_F><<<w.nt_col, CM_THREADS, T.smem_col, s>>>(S, it);
+  k_row_inv<R, MAXE, MODE_F><<<w.nt_rowd, CM_THREADS, T.smem_row, s>>>(S, it);
+}
+
+template <typename R, int MAXE>
+static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphExec_t* out) {
+  const int gi = bisect ? 1 : 0;
+  if (w.graph[gi] && w.graph_iters[gi] == iters) {
+    *out = w.graph[gi];
+    return CM_OK;
+  }
+  if (w.graph[gi]) {
+    cudaGraphExecDestroy(w.graph[gi]);
+    w.graph[gi] = nullptr;
+  }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed));
+  for (int i = 0; i < iters; ++i) launch_iteration<R, MAXE>(p, w, bisect, p->stream);
+  cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+  CK(e);
+  e = cudaGraphInstantiate(&w.graph[gi], g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
+  w.graph_iters[gi] = iters;
+  *out = w.graph[gi];
+  return CM_OK;
+}
+
+struct SolveInput {
+  const double* h64;
+  const double* u0;
+  const double* f0;
+  int f0_ld;
+};
+
+template <typename R, int MAXE>
+static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
+                   double rel_pentol, int maxiter, CcgState* fin) {
+  cudaStream_t s = p->stream;
+  set_smem_attrs<R, MAXE>();
+  CKS(ensure_ccg(p, w));
+  CcgState st;
+  memset(&st, 0, sizeof(st));
+  CcgParams& P = st.p;
+  P.F = prm->external_force;
+  P.offset0 = prm->load_control ? 0.0 : prm->offset;
+  P.H = prm->hardness;
+  P.has_h = prm->has_hardness;
+  P.pentol = prm->pentol;
+  P.forcetol = prm->forcetol;
+  P.thermotol = prm->thermotol;
+  P.mixfac = prm->mixfac;
+  P.mixdecfac = prm->mixdecfac;
+  P.minmixsteps = prm->minmixsteps;
+  P.maxiter = maxiter;
+  P.load_control = prm->load_control;
+  P.n_surface = (double)p->tx * (double)p->ty;
+  st.it = 1;
+  st.mode = CMM_RESET;
+  st.G_old = 1.0;
+  st.offset = P.offset0;
+  st.cur_mixfac = P.mixfac;
+  st.nfev = 1;
+  st.scale = 1.0;
+  CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+  k_h_prep<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64);
+  k_h_var<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64, prm->pentol <= 0, rel_pentol);
+  Slot<R> hs = base_slot(p, w);
+  const int gd = grid_for((long)p->nx * p->ny);
+  if (in.f0) {
+    k_init_f<R><<<gd, 256, 0, s>>>(hs, in.f0, in.f0_ld);
+    CKS(launch_plain<R, MAXE>(p, w, MODE_PLAIN, CM_OP_DISP, w.f[0], p->tx, p->ty, p->ty, w.u, p->nx,
+                              p->ny, p->ny, s));
+  } else {
+    k_init_u<R><<<gd, 256, 0, s>>>(hs, in.u0, P.offset0);
+    CKS(launch_plain<R, MAXE>(p, w, MODE_PLAIN, CM_OP_FORCE, w.u, p->nx, p->ny, p->ny, w.f[0], p->tx,
+                              p->ty, p->ty, s));
+  }
+  CK(cudaGetLastError());
+  const bool bisect = prm->has_hardness && prm->load_control;
+  int every = prm->check_every;
+  if (every <= 0) {
+    const long work = (long)p->nx * p->ny;
+    every = work >= (1L << 20) ? 4 : (work >= (1L << 16) ? 8 : 16);
+  }
+  cudaGraphExec_t g;
+  CKS(get_graph<R, MAXE>(p, w, bisect, every, &g));
+  auto t0 = std::chrono::steady_clock::now();
+  for (int done_iters = 0;; done_iters += every) {
+    CK(cudaGraphLaunch(g, s));
+    CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (p->h_state->done) break;
+    if (prm->timeout_s > 0) {
+      const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (el > prm->timeout_s) return CM_ERR_TIMEOUT;
+    }
+    if (done_iters > maxiter + 2 * every) return CM_ERR_CUDA;  // state machine failed to stop
+  }
+  *fin = *p->h_state;
+  if (fin->status == CMS_NAN) return CM_ERR_NAN;
+  if (fin->status == CMS_BISECT_SIGN) return CM_ERR_BISECT;
+  if (fin->status == CMS_BISECT_SIGN + 1) return CM_ERR_BISECT_CONV;
+  return CM_OK;
+}
+
+template <typename R>
+static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned char* active,
+                      unsigned char* plastic, CcgState* fin) {
+  cudaStream_t s = p->stream;
+  k_ccg_result<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, jac, active, plastic);
+  if (x) k_to_f64<R><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(w.u, x, (long)p->nx * p->ny);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *fin = *p->h_state;
+  return CM_OK;
+}
+
+static void fill_result(const CcgState& st, cm_ccg_result* r) {
+  r->status = st.status == CMS_CONVERGED ? CM_SOLVE_CONVERGED : CM_SOLVE_MAXITER;
+  r->nit = st.it;
+  r->nfev = st.nfev;
+  r->last_step_mix = st.branch == 1;
+  r->offset = st.offset;
+  r->fun = st.sum_cgt;
+  r->rms_pen = st.rms_pen;
+  r->max_pen = st.max_pen;
+  r->max_pres = st.max_pres;
+  r->pad_pres = st.pad_pres;
+  r->maxdu = st.maxdu;
+  r->total_force = st.total_force;
+  r->pentol_used = st.p.pentol;
+  r->area = st.A_contact;
+  r->cg_area = st.A_cg;
+  r->plastic_area = st.A_fl;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* cm_version(void) { return "cm_b200 0.1 (sm_100a)"; }
+
+const char* cm_status_string(int status) {
+  switch (status) {
+    case CM_OK: return "ok";
+    case CM_ERR_ARG: return "invalid argument";
+    case CM_ERR_SHAPE: return "array shape mismatch";
+    case CM_ERR_SIZE: return "grid too large for the single-pass transforms";
+    case CM_ERR_CUDA: {
+      static thread_local char buf[256];
+      snprintf(buf, sizeof(buf), "CUDA error: %s", cudaGetErrorString(last_cuda_error()));
+      return buf;
+    }
+    case CM_ERR_OOM: return "device allocation failed";
+    case CM_ERR_NAN: return "nan encountered.";
+    case CM_ERR_BISECT: return "f(a) and f(b) must have different signs";
+    case CM_ERR_BISECT_CONV: return "Failed to converge after 100 iterations";
+    case CM_ERR_TIMEOUT: return "solve exceeded its time budget";
+    default: return "unknown status";
+  }
+}
+
+int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
+  if (!desc || !out) return CM_ERR_ARG;
+  *out = nullptr;
+  if (desc->kind != CM_PERIODIC && desc->kind != CM_FREE) return CM_ERR_ARG;
+  if (desc->dim != 1 && desc->dim != 2) return CM_ERR_ARG;
+  if (desc->nx < 1 || desc->ny < 1 || (desc->dim == 1 && desc->ny != 1)) return CM_ERR_ARG;
+  if (desc->kind == CM_FREE && desc->dim != 2) return CM_ERR_ARG;
+  if (!(desc->sx > 0) || !(desc->sy > 0)) return CM_ERR_ARG;
+  cm_plan* p = new (std::nothrow) cm_plan();
+  if (!p) return CM_ERR_OOM;
+  p->d = *desc;
+  p->tx = desc->nx;
+  p->ty = desc->ny;
+  const int f = desc->kind == CM_FREE ? 2 : 1;
+  p->nx = f * desc->nx;
+  p->ny = f * desc->ny;
+  p->nyh = p->ny / 2 + 1;
+  int rc = CM_OK;
+  auto fail = [&](int code) {
+    cm_plan_destroy(p);
+    return code;
+  };
+  if (!make_fft_desc(p->nx, &p->fx) || !make_fft_desc(p->ny, &p->fy)) return fail(CM_ERR_SIZE);
+  if (stream) {
+    p->stream = (cudaStream_t)stream;
+    p->own_stream = false;
+  } else {
+    if (cudaStreamCreate(&p->stream) != cudaSuccess) return fail(CM_ERR_CUDA);
+    p->own_stream = true;
+  }
+  if (cudaMallocHost(&p->h_state, sizeof(CcgState)) != cudaSuccess) {
+    p->h_state = nullptr;
+    return fail(CM_ERR_OOM);
+  }
+  if ((rc = init_work<double>(p, p->w64, CM_MAXE64)) != CM_OK) return fail(rc);
+  if ((rc = init_work<float>(p, p->w32, CM_MAXE32)) != CM_OK) return fail(rc);
+  // work items (0, i): every launch on this plan covers tiles 0..n-1 of slot 0
+  {
+    std::vector<int2> it(p->max_items);
+    for (int i = 0; i < p->max_items; ++i) it[i] = make_int2(0, i);
+    if ((rc = dalloc(p, &p->items, it.size())) != CM_OK) return fail(rc);
+    if (cudaMemcpy(p->items, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(CM_ERR_CUDA);
+  }
+  const long nh = (long)p->nx * p->nyh;
+  if ((rc = dalloc(p, &p->G, nh)) != CM_OK) return fail(rc);
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = dalloc(p, &p->tab64[i], nh)) != CM_OK) return fail(rc);
+    if ((rc = dalloc(p, &p->tab32[i], nh)) != CM_OK) return fail(rc);
+  }
+  p->w64.tab[0] = p->tab64[0];
+  p->w64.tab[1] = p->tab64[1];
+  p->w32.tab[0] = p->tab32[0];
+  p->w32.tab[1] = p->tab32[1];
+  cudaStream_t s = p->stream;
+  if (desc->kind == CM_PERIODIC) {
+    const double Es = desc->young / (1 - desc->poisson * desc->poisson);
+    k_table_periodic<<<grid_for(nh), 256, 0, s>>>(p->G, p->nx, p->ny, p->nyh, desc->sx, desc->sy, Es,
+                                                   desc->young, desc->poisson, desc->q0_mode,
+                                                   desc->stiffness_q0, desc->thickness, desc->dim);
+  } else {
+    double* love = nullptr;
+    if ((rc = dalloc(p, &love, (long)p->nx * p->ny)) != CM_OK) return fail(rc);
+    k_love<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, p->tx, p->ty, p->nx, p->ny,
+                                                          desc->sx / p->tx, desc->sy / p->ty, desc->young);
+    rc = launch_plain<double, CM_MAXE64>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
+                                         0, 0, s);
+    if (rc != CM_OK) return fail(rc);
+    k_real_part<<<grid_for(nh), 256, 0, s>>>(p->w64.spec, p->G, nh);
+  }
+  const double area = (desc->sx / p->tx) * (desc->sy / p->ty);
+  const double N = (double)p->nx * (double)p->ny;
+  k_tables_scale<<<grid_for(nh), 256, 0, s>>>(p->G, nh, 1.0 / (area * N), area / N, p->tab64[0],
+                                               p->tab64[1], p->tab32[0], p->tab32[1]);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+    return fail(CM_ERR_CUDA);
+  *out = p;
+  return CM_OK;
+}
+
+int cm_plan_destroy(cm_plan* p) {
+  if (!p) return CM_OK;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  for (int i = 0; i < 2; ++i) {
+    if (p->w32.graph[i]) cudaGraphExecDestroy(p->w32.graph[i]);
+    if (p->w64.graph[i]) cudaGraphExecDestroy(p->w64.graph[i]);
+  }
+  for (void* a : p->allocs) cudaFree(a);
+  if (p->h_state) cudaFreeHost(p->h_state);
+  if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return CM_OK;
+}
+
+int cm_plan_shape(const cm_plan* p, int* nxd, int* nyd, int* nyh) {
+  if (!p) return CM_ERR_ARG;
+  if (nxd) *nxd = p->nx;
+  if (nyd) *nyd = p->ny;
+  if (nyh) *nyh = p->nyh;
+  return CM_OK;
+}
+
+int cm_plan_greens_host(cm_plan* p, double* out) {
+  if (!p || !out) return CM_ERR_ARG;
+  CK(cudaMemcpyAsync(out, p->G, sizeof(double) * (size_t)p->nx * p->nyh, cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return CM_OK;
+}
+
+int cm_apply(cm_plan* p, int op, int precision, const void* in, int in_rows, int in_cols, int in_ld,
+             void* out, int out_rows, int out_cols, int out_ld, void* stream) {
+  if (!p || !in || !out) return CM_ERR_ARG;
+  if (op != CM_OP_DISP && op != CM_OP_FORCE) return CM_ERR_ARG;
+  if (precision != CM_FP64 && precision != CM_FP32) return CM_ERR_ARG;
+  if (in_rows < 1 || in_rows > p->nx || in_cols < 1 || in_cols > p->ny || in_ld < in_cols) return CM_ERR_SHAPE;
+  if (out_rows < 1 || out_rows > p->nx || out_cols < 1 || out_cols > p->ny || out_ld < out_cols)
+    return CM_ERR_SHAPE;
+  cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
+  return apply_dispatch(p, op, precision, in, in_rows, in_cols, in_ld, out, out_rows, out_cols, out_ld, s);
+}
+
+int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const double* u0,
+                 const double* f0, double* x, double* jac, unsigned char* active,
+                 unsigned char* plastic, cm_ccg_result* res) {
+  if (!p || !prm || !h || !res) return CM_ERR_ARG;
+  if (prm->precision != CM_FP64 && prm->precision != CM_FP32 && prm->precision != CM_MIXED) return CM_ERR_ARG;
+  if (prm->maxiter < 1) return CM_ERR_ARG;
+  if (prm->has_hardness && !(prm->hardness > 0)) return CM_ERR_ARG;
+  memset(res, 0, sizeof(*res));
+  SolveInput in{h, u0, f0, p->ny};
+  CcgState fin;
+  if (prm->precision == CM_FP64) {
+    CKS(run_ccg<double, CM_MAXE64>(p, p->w64, prm, in, 0.0, prm->maxiter, &fin));
+    CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
+    fill_result(fin, res);
+    return CM_OK;
+  }
+  const double rp = prm->precision == CM_MIXED ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
+  CKS(run_ccg<float, CM_MAXE32>(p, p->w32, prm, in, rp, prm->maxiter, &fin));
+  if (prm->precision == CM_FP32) {
+    CKS(finish_ccg<float>(p, p->w32, x, jac, active, plastic, &fin));
+    fill_result(fin, res);
+    res->nit_fp32 = fin.it;
+    return CM_OK;
+  }
+  // FP64 refinement warm-started from the FP32 forces (initial_forces semantics)
+  const int nit32 = fin.it, nfev32 = fin.nfev;
+  double* f64 = nullptr;
+  {
+    // the FP64 solver's f[1] buffer is free before the refinement starts
+    CKS(ensure_ccg(p, p->w64));
+    f64 = p->w64.u;  // borrow: overwritten by the refinement's own initialisation
+  }
+  const int fpar = fin.parity;
+  k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, p->stream>>>(
+      p->w32.f[fpar], p->tx, p->ty, f64, p->nx, p->ny);
+  CK(cudaGetLastError());
+  // k_init_f reads f64 before the operator overwrites u, so the borrow is safe
+  SolveInput in2{h, nullptr, f64, p->ny};
+  const int rem = std::max(1, prm->maxiter - nit32);
+  CKS(run_ccg<double, CM_MAXE64>(p, p->w64, prm, in2, 0.0, rem, &fin));
+  CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
+  fill_result(fin, res);
+  res->nit += nit32;
+  res->nfev += nfev32;
+  res->nit_fp32 = nit32;
+  return CM_OK;
+}
+
+int cm_ccg_solve_host(cm_plan* p, const cm_ccg_params* prm, const double* h, const double* u0,
+                      const double* f0, double* x, double* jac, unsigned char* active,
+                      unsigned char* plastic, cm_ccg_result* res) {
+  if (!p || !prm || !h || !res) return CM_ERR_ARG;
+  const size_t nt = (size_t)p->tx * p->ty, nd = (size_t)p->nx * p->ny;
+  double *dh = nullptr, *du = nullptr, *df = nullptr, *dx = nullptr, *dj = nullptr;
+  unsigned char *da = nullptr, *dp = nullptr;
+  int rc = CM_OK;
+  cudaStream_t s = p->stream;
+  auto cleanup = [&]() {
+    cudaFree(dh); cudaFree(du); cudaFree(df); cudaFree(dx); cudaFree(dj); cudaFree(da); cudaFree(dp);
+  };
+  if (cudaMalloc(&dh, nt * 8) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (u0 && cudaMalloc(&du, nd * 8) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (f0 && cudaMalloc(&df, nd * 8) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (x && cudaMalloc(&dx, nd * 8) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (jac && cudaMalloc(&dj, nt * 8) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (active && cudaMalloc(&da, nt) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (plastic && cudaMalloc(&dp, nt) != cudaSuccess) { cleanup(); return CM_ERR_OOM; }
+  if (cudaMemcpyAsync(dh, h, nt * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (u0 && cudaMemcpyAsync(du, u0, nd * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+      (f0 && cudaMemcpyAsync(df, f0, nd * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)) {
+    cleanup();
+    return CM_ERR_CUDA;
+  }
+  rc = cm_ccg_solve(p, prm, dh, du, df, dx, dj, da, dp, res);
+  if (rc == CM_OK) {
+    if ((x && cudaMemcpyAsync(x, dx, nd * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        (jac && cudaMemcpyAsync(jac, dj, nt * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        (active && cudaMemcpyAsync(active, da, nt, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        (plastic && cudaMemcpyAsync(plastic, dp, nt, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      rc = CM_ERR_CUDA;
+  }
+  cleanup();
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+/*
+ * cm_b200.h -- C ABI of the B200 elastic contact library (libcm_b200.so).
+ *
+ * The library implements, on one NVIDIA B200 (sm_100a), the hot path of
+ * ContactEngineering/ContactMechanics v1.8.3:
+ *   - the FFT Green's-function operators of PeriodicFFTElasticHalfSpace and
+ *     FreeFFTElasticHalfSpace (evaluate_disp / evaluate_force, Hockney
+ *     zero padding for free boundaries), and
+ *   - the Polonsky-Keer constrained_conjugate_gradients loop including the
+ *     plastic hardness cap used by PlasticNonSmoothContactSystem.
+ *
+ * Conventions
+ *   - Real fields are row-major (nx, ny) arrays of double (CM_FP64) or float
+ *     (CM_FP32), exactly the memory layout of a C-ordered numpy array of
+ *     shape (nx, ny).  "Domain" means the computational grid: (nx, ny) for
+ *     periodic substrates, (2nx, 2ny) for free ones.
+ *   - All pointers named *_dev are device pointers on the current device.
+ *     Pointers named *_host are host pointers.
+ *   - Every entry point returns an int status: CM_OK (0) or a CM_ERR_*
+ *     code; cm_status_string() describes it.  Solver outcomes that the
+ *     reference reports without raising (not converged) come back in
+ *     cm_ccg_result.status, not as an error.
+ *   - A plan is not re-entrant: calls on one plan must be serialised by the
+ *     caller (the reference substrate shares its FFT buffers the same way).
+ *   - stream arguments are cudaStream_t passed as void*; NULL means the
+ *     plan's own stream.
+ */
+#ifndef CM_B200_H
+#define CM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CM_OK 0
+#define CM_ERR_ARG 1          /* invalid argument (mirrors ValueError) */
+#define CM_ERR_SHAPE 2        /* array shape mismatch (mirrors Substrate.Error) */
+#define CM_ERR_SIZE 3         /* grid too large for the single-pass transforms */
+#define CM_ERR_CUDA 4         /* CUDA runtime error */
+#define CM_ERR_OOM 5          /* device allocation failed */
+#define CM_ERR_NAN 6          /* NaN encountered in the solve (RuntimeError) */
+#define CM_ERR_BISECT 7       /* offset bisection sign error (ValueError) */
+#define CM_ERR_BISECT_CONV 8  /* offset bisection did not converge (RuntimeError) */
+#define CM_ERR_TIMEOUT 9      /* a solve exceeded its host-side time budget */
+
+/* substrate kinds */
+#define CM_PERIODIC 0
+#define CM_FREE 1
+
+/* precisions */
+#define CM_FP64 0   /* everything in FP64 */
+#define CM_FP32 1   /* FP32 fields and FFTs, FP64 reductions and scalars */
+#define CM_MIXED 2  /* FP32 solve, then FP64 refinement of the same solve */
+
+/* stiffness at q = 0 for periodic substrates */
+#define CM_Q0_DEFAULT 0  /* mean of the two lowest non-zero stiffnesses */
+#define CM_Q0_ZERO 1     /* stiffness_q0 == 0: G(0) = 0 */
+#define CM_Q0_VALUE 2    /* stiffness_q0 given */
+
+/* operators */
+#define CM_OP_DISP 0   /* evaluate_disp: displacement from forces */
+#define CM_OP_FORCE 1  /* evaluate_force: forces from displacement */
+
+/* solver outcome (cm_ccg_result.status) */
+#define CM_SOLVE_CONVERGED 1
+#define CM_SOLVE_MAXITER 2
+
+typedef struct cm_plan cm_plan;
+
+typedef struct {
+  int kind;            /* CM_PERIODIC or CM_FREE */
+  int dim;             /* 1 or 2; a 1D periodic substrate uses ny = 1 */
+  int nx, ny;          /* topography grid (nb_grid_pts) */
+  double sx, sy;       /* physical_sizes */
+  double young;        /* Young's modulus (contact modulus if poisson = 0) */
+  double poisson;      /* periodic only */
+  int q0_mode;         /* CM_Q0_* (periodic only) */
+  double stiffness_q0; /* used when q0_mode == CM_Q0_VALUE */
+  double thickness;    /* <= 0: infinitely deep half-space (periodic only) */
+} cm_plan_desc;
+
+typedef struct {
+  int precision;         /* CM_FP64, CM_FP32 or CM_MIXED */
+  int load_control;      /* 1: external_force given; 0: offset given */
+  double external_force;
+  double offset;
+  int has_hardness;
+  double hardness;       /* in force units (hardness * area_per_pt) */
+  double pentol;         /* <= 0: the reference's default heuristic */
+  double forcetol, thermotol, mixfac, mixdecfac;
+  int minmixsteps, maxiter;
+  int check_every;       /* iterations per host convergence poll; <= 0: auto */
+  double fp32_pentol_rel;  /* CM_MIXED: FP32 phase pentol = max(pentol, rel * height range);
+                             <= 0: 2e-6 */
+  double timeout_s;      /* host-side wall-clock budget; <= 0: none */
+} cm_ccg_params;
+
+typedef struct {
+  int status;            /* CM_SOLVE_CONVERGED or CM_SOLVE_MAXITER */
+  int nit, nfev;         /* iterations / operator calls (all phases) */
+  int nit_fp32;          /* iterations run in FP32 (CM_MIXED / CM_FP32) */
+  int last_step_mix;     /* 1 if the last iteration was a mixing step */
+  double offset, fun;
+  double rms_pen, max_pen, max_pres, pad_pres, maxdu, total_force;
+  double pentol_used;
+  long long area, cg_area, plastic_area;
+} cm_ccg_result;
+
+/* Returns the message for a status code. */
+const char* cm_status_string(int status);
+
+/* Library version string. */
+const char* cm_version(void);
+
+/*
+ * Create a substrate plan: domain geometry, FFT twiddles and the
+ * Green's-function tables built on the device in FP64 (with an FP32 copy).
+ * Replaces PeriodicFFTElasticHalfSpace.__init__ (FFTElasticHalfSpace.py:169-306,
+ * tables :445-571) and FreeFFTElasticHalfSpace.__init__ (:912-964, table
+ * :1033-1139).  stream: the stream all work of this plan runs on (NULL: a new
+ * non-blocking stream owned by the plan).
+ */
+int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out);
+
+/* Release a plan and every device buffer it owns. */
+int cm_plan_destroy(cm_plan* plan);
+
+/* Domain and half-spectrum shapes: domain (nxd, nyd); half spectrum (nxd, nyh). */
+int cm_plan_shape(const cm_plan* plan, int* nxd, int* nyd, int* nyh);
+
+/*
+ * Copy the unscaled FP64 Green's table G(q) (surface displacement per unit
+ * pressure in Fourier space) to host memory, layout (nxd, nyh) with the half
+ * spectrum along y.  The reference stores the same real values halved along
+ * x (FFTElasticHalfSpace.py:445-561, 1033-1139).
+ */
+int cm_plan_greens_host(cm_plan* plan, double* out_host);
+
+/*
+ * Apply the operator to a device field (FFTElasticHalfSpace.py:573-611,
+ * free :1141-1197).  The input occupies rows [0,in_rows) x cols [0,in_cols)
+ * of the domain (leading dimension in_ld) and is zero elsewhere -- this is
+ * the Hockney zero padding; the output region [0,out_rows) x [0,out_cols) is
+ * written with leading dimension out_ld.  precision selects float or double
+ * buffers (CM_FP64 / CM_FP32).
+ */
+int cm_apply(cm_plan* plan, int op, int precision, const void* in_dev, int in_rows,
+             int in_cols, int in_ld, void* out_dev, int out_rows, int out_cols, int out_ld,
+             void* stream);
+
+/*
+ * Polonsky-Keer constrained conjugate gradients
+ * (ConstrainedConjugateGradients.py:47-509) on one substrate.
+ *   heights_dev      (nx, ny) FP64 topography heights
+ *   init_disp_dev    domain-sized FP64 initial displacements or NULL
+ *   init_force_dev   domain-sized FP64 initial forces or NULL (takes precedence)
+ * Outputs (any may be NULL):
+ *   x_dev            domain-sized FP64 displacements (result.x)
+ *   jac_dev          (nx, ny) FP64 result.jac = -forces on the topography
+ *   active_dev       (nx, ny) uint8 result.active_set on the topography
+ *   plastic_dev      (nx, ny) uint8 result.plastic (hardness runs)
+ * Returns CM_ERR_NAN / CM_ERR_BISECT* for the cases where the reference
+ * raises; otherwise CM_OK with res->status telling converged or maxiter.
+ */
+int cm_ccg_solve(cm_plan* plan, const cm_ccg_params* params, const double* heights_dev,
+                 const double* init_disp_dev, const double* init_force_dev, double* x_dev,
+                 double* jac_dev, unsigned char* active_dev, unsigned char* plastic_dev,
+                 cm_ccg_result* res);
+
+/*
+ * Same as cm_ccg_solve with every array in host memory; the host<->device
+ * copies are part of the call.
+ */
+int cm_ccg_solve_host(cm_plan* plan, const cm_ccg_params* params, const double* heights_host,
+                      const double* init_disp_host, const double* init_force_host,
+                      double* x_host, double* jac_host, unsigned char* active_host,
+                      unsigned char* plastic_host, cm_ccg_result* res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CM_B200_H */

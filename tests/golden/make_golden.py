@@ -1,0 +1,172 @@
+"""Generate golden vectors by running the reference's own code.
+
+Run in a container that has the reference checkout (read-only) at
+``/root/reference``::
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+It imports ContactMechanics unmodified over the serial stand-ins of
+``refstubs.py`` and writes ``tests/golden/*.npz``.  The fixtures are small
+(grids of at most 64x64) so that the CPU test-suite stays fast.  The GPU box
+never runs this script; tests only read the committed ``.npz`` files.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+
+import refstubs  # noqa: E402
+
+
+def _sphere(nb, sizes, radius):
+    nx, ny = nb
+    sx, sy = sizes
+    x = ((np.arange(nx) - nx / 2) * sx / nx).reshape(-1, 1)
+    y = ((np.arange(ny) - ny / 2) * sy / ny).reshape(1, -1)
+    return -(x * x + y * y) / (2 * radius)
+
+
+def main(ref_root):
+    refstubs.install(ref_root)
+    from ContactMechanics import (PeriodicFFTElasticHalfSpace,
+                                  FreeFFTElasticHalfSpace)
+    from ContactMechanics.Systems import NonSmoothContactSystem
+    from ContactMechanics.PlasticSystemSpecialisations import \
+        PlasticNonSmoothContactSystem
+    from oracle.contact_oracle import self_affine
+
+    rng = np.random.default_rng(20261203)
+    out = {}
+
+    # ---- operators --------------------------------------------------------
+    periodic_cases = [
+        ("p8x15", (8, 15), (2.45, 1.0), {}),
+        ("p9x4", (9, 4), (2.45, 1.0), {}),
+        ("p16x16_q0zero", (16, 16), (1.0, 1.0), dict(stiffness_q0=0.0)),
+        ("p16x12_q0val", (16, 12), (3.0, 2.0), dict(stiffness_q0=2.5)),
+        ("p32x24_thick", (32, 24), (1.0, 1.5), dict(thickness=0.2, poisson=0.3)),
+        ("p33x64_poisson", (33, 64), (1.0, 1.0), dict(poisson=0.25)),
+        ("p17", (17,), (3.0,), {}),
+    ]
+    for name, nb, sizes, kw in periodic_cases:
+        s = PeriodicFFTElasticHalfSpace(nb, 1.7, sizes, **kw)
+        out[f"op_{name}_config"] = np.array(json.dumps(dict(
+            kind="periodic", nb_grid_pts=list(nb), physical_sizes=list(sizes),
+            young=1.7, kwargs=kw)))
+        f = rng.standard_normal(nb)
+        u = rng.standard_normal(nb)
+        out[f"op_{name}_G"] = s.greens_function
+        out[f"op_{name}_f"] = f
+        out[f"op_{name}_u"] = u
+        out[f"op_{name}_disp"] = s.evaluate_disp(f)
+        out[f"op_{name}_force"] = s.evaluate_force(u)
+    free_cases = [("f8x8", (8, 8), (1.0, 1.0)),
+                  ("f7x9", (7, 9), (2.0, 1.0)),
+                  ("f12x5", (12, 5), (1.0, 3.0))]
+    for name, nb, sizes in free_cases:
+        s = FreeFFTElasticHalfSpace(nb, 2.3, sizes)
+        out[f"op_{name}_config"] = np.array(json.dumps(dict(
+            kind="free", nb_grid_pts=list(nb), physical_sizes=list(sizes),
+            young=2.3, kwargs={})))
+        fpad = np.zeros(s.nb_domain_grid_pts)
+        fpad[:nb[0], :nb[1]] = rng.standard_normal(nb)
+        out[f"op_{name}_G"] = s.greens_function
+        out[f"op_{name}_f"] = fpad
+        out[f"op_{name}_disp"] = s.evaluate_disp(fpad)
+        out[f"op_{name}_disp_unpadded"] = s.evaluate_disp(fpad[:nb[0], :nb[1]])
+        upad = rng.standard_normal(s.nb_domain_grid_pts)
+        out[f"op_{name}_u"] = upad
+        out[f"op_{name}_force"] = s.evaluate_force(upad)
+
+    # ---- solves -----------------------------------------------------------
+    from refstubs import Topography, PlasticTopography
+
+    def record(name, res, extra=None):
+        out[f"ccg_{name}_x"] = res.x
+        out[f"ccg_{name}_jac"] = res.jac
+        out[f"ccg_{name}_active_set"] = res.active_set
+        out[f"ccg_{name}_scalars"] = np.array(
+            [res.offset, res.fun, res.nit, res.nfev, float(res.success)])
+        if hasattr(res, "plastic"):
+            out[f"ccg_{name}_plastic"] = res.plastic
+        for k, v in (extra or {}).items():
+            out[f"ccg_{name}_{k}"] = v
+
+    def solve(name, substrate, heights, sizes, inputs, plastic_h=None, **kw):
+        cfg = dict(kind="free" if isinstance(substrate, FreeFFTElasticHalfSpace)
+                   else "periodic", nb_grid_pts=list(substrate.nb_grid_pts),
+                   physical_sizes=list(sizes), young=substrate.young,
+                   hardness=plastic_h, solver_kwargs=kw)
+        out[f"ccg_{name}_config"] = np.array(json.dumps(cfg))
+        topo = Topography(heights, sizes)
+        if plastic_h is not None:
+            topo = PlasticTopography(topo, plastic_h)
+            system = PlasticNonSmoothContactSystem(substrate, topo)
+        else:
+            system = NonSmoothContactSystem(substrate, topo)
+        res = system.minimize_proxy(**kw)
+        extra = dict(heights=heights)
+        if plastic_h is not None:
+            extra["plastic_displ"] = topo.plastic_displ.copy()
+        record(name, res, extra)
+        out[f"ccg_{name}_inputs"] = np.array(inputs, dtype=float)
+
+    # periodic Hertz, load control
+    nb, sizes = (32, 32), (1.0, 1.0)
+    h = _sphere(nb, sizes, 1.0)
+    solve("hertz_periodic_load", PeriodicFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [np.nan, 1e-3, np.nan, 1e-12, 1e-14],
+          external_force=1e-3, pentol=1e-12, forcetol=1e-14)
+    # free sphere, offset control
+    nb, sizes = (32, 28), (1.0, 1.0)
+    h = _sphere(nb, sizes, 2.0)
+    solve("sphere_free_offset", FreeFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [0.03, np.nan, np.nan, 1e-12, 1e-14],
+          offset=0.03, pentol=1e-12, forcetol=1e-14)
+    # a coarse free sphere that stalls: exercises the maxiter exit
+    nb, sizes = (24, 20), (1.0, 1.0)
+    h = _sphere(nb, sizes, 1.0)
+    solve("stall_free_offset", FreeFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [0.01, np.nan, np.nan, 1e-9, 1e-14, 60],
+          offset=0.01, pentol=1e-9, forcetol=1e-14, maxiter=60)
+    # free sphere, load control
+    nb, sizes = (16, 18), (2.0, 2.0)
+    h = _sphere(nb, sizes, 2.0)
+    solve("sphere_free_load", FreeFFTElasticHalfSpace(nb, 3.0, sizes),
+          h, sizes, [np.nan, 0.05, np.nan, 1e-11, 1e-13],
+          external_force=0.05, pentol=1e-11, forcetol=1e-13)
+    # periodic rough, load control
+    nb, sizes = (32, 32), (1.0, 1.0)
+    h = self_affine(nb, sizes, 0.8, 0.1, seed=7)
+    solve("rough_periodic_load", PeriodicFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [np.nan, 2e-3, np.nan, 1e-12, 1e-14],
+          external_force=2e-3, pentol=1e-12, forcetol=1e-14)
+    # periodic rough, plastic, load control (exercises the mixing branch)
+    h = self_affine(nb, sizes, 0.7, 0.2, seed=11)
+    solve("plastic_periodic_load", PeriodicFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [np.nan, 5e-3, 0.05, 1e-11, 1e-10], plastic_h=0.05,
+          external_force=5e-3, pentol=1e-11, forcetol=1e-10, maxiter=2000)
+    # periodic rough, plastic, offset control
+    h = self_affine(nb, sizes, 0.7, 0.2, seed=12)
+    off = float(np.max(h) - 0.3 * (np.max(h) - np.min(h)))
+    solve("plastic_periodic_offset", PeriodicFFTElasticHalfSpace(nb, 1.0, sizes),
+          h, sizes, [-off, np.nan, 0.05, 1e-11, 1e-10], plastic_h=0.05,
+          offset=-off, pentol=1e-11, forcetol=1e-10, maxiter=2000)
+    # Westergaard-like wavy profile, offset control
+    nb, sizes = (64, 8), (30.0, 1.0)
+    h = np.resize(np.cos(2 * np.pi * np.arange(nb[0]) / nb[0]), (nb[1], nb[0])).T.copy()
+    solve("wavy_periodic_offset", PeriodicFFTElasticHalfSpace(nb, 3.56, sizes),
+          h, sizes, [-0.5, np.nan, np.nan, 1e-9, 1e-5], offset=-0.5, pentol=1e-9)
+
+    path = os.path.join(HERE, "reference_vectors.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
