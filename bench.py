@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the elastic contact solve on B200.
+
+Workload (the single-solve non-periodic configuration): FreeFFTElasticHalfSpace
+with a 1024 x 1024 topography, Hockney-padded to a 2048 x 2048 domain; seeded
+self-affine Gaussian rough surface (Hurst 0.8, short-wavelength cutoff 4 px,
+rolloff below 2 pi / (L/8), rms slope 0.1, L = 1, E* = 1); load sweep of 10
+mean pressures log-spaced 1e-4 .. 1e-2 E*, each solve warm-started from the
+previous displacement.  One step = one full sweep (10 solves).  Tolerances:
+pentol = 1e-9 (max h - min h), forcetol = 1e-12 F, thermotol 1e-6.
+
+Reported: solves/s of the mixed-precision path (FP32 bulk, FP64 reductions,
+FP64 refinement) with inputs resident on the device (`value`); the plain FP64
+path on the same sweep (`fp64_value`); the relative displacement error of the
+mixed result against the FP64 result; p50 / p99 per-solve latency; `e2e`
+through the public API with host (numpy) arrays; a roofline of the dominant
+kernel from live CUDA-event timing; the CPU oracle on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CCG solves/s + p99 latency at 1e-6 rel err, mixed vs plain FP64, one B200"
+N_TOPO = 1024
+PRESSURES = np.logspace(-4, -2, 10)
+SEED = 2026
+WORKLOAD = ("free 1024x1024 topography (Hockney 2048x2048 domain), self-affine H=0.8 "
+            "slope 0.1 cutoff 4px rolloff L/8, seed 2026; sweep of 10 mean pressures "
+            "logspace(-4,-2) E*, warm-started; pentol 1e-9*(max h-min h), forcetol 1e-12*F")
+CPU_BUDGET_S = 20.0
+
+
+def surface():
+    from contactmechanics_b200.Generation import self_affine
+    return self_affine((N_TOPO, N_TOPO), (1.0, 1.0), 0.8, 0.1, seed=SEED,
+                       rolloff_wavelength=1.0 / 8)
+
+
+def tolerances(h, F):
+    return dict(pentol=1e-9 * float(np.max(h) - np.min(h)), forcetol=1e-12 * F)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (numpy / scipy.fft with all host threads)
+# ---------------------------------------------------------------------------
+def cpu_sample(h):
+    from oracle import contact_oracle as oc
+    cores = os.cpu_count() or 1
+    sub = oc.FreeSubstrate((N_TOPO, N_TOPO), 1.0, (1.0, 1.0), workers=cores)
+    t0 = time.perf_counter()
+    done, iters, u0 = 0, 0, None
+    for p in PRESSURES:
+        r = oc.constrained_conjugate_gradients(sub, h, external_force=float(p),
+                                               initial_displacements=u0, **tolerances(h, p))
+        u0 = r["x"]
+        done += 1
+        iters += r["nit"]
+        if time.perf_counter() - t0 > CPU_BUDGET_S:
+            break
+    el = time.perf_counter() - t0
+    return dict(value=done / el, unit="solves/s", cores=cores, kind="port",
+                sample=f"oracle (numpy, scipy.fft workers={cores}) on the first {done} solve(s) "
+                       f"of the sweep in order, {iters} iterations, {el:.1f} s",
+                seconds=el, solves=done, iterations=iters)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.QUERY,
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for i, n in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def kernel_bytes(nx, ny, tx, ty, prec_bytes=4):
+    """Algorithmic bytes one launch of each iteration kernel moves (FP32 bulk)."""
+    p, c = prec_bytes, 2 * prec_bytes
+    N, Nd = tx * ty, nx * ny
+    nyh = ny // 2 + 1
+    nh_t, nh = tx * nyh, nx * nyh
+    return {
+        "k_ccg_begin": 3 * p * N,
+        "k_ccg_gsum": 3 * p * N,
+        "k_row_fwd<T>": 5 * p * N + c * nh_t,
+        "k_col<T>": 2 * c * nh_t + p * nh,
+        "k_row_inv<T>": c * nh_t + p * N,
+        "k_ccg_update": 5 * p * N,
+        "k_row_fwd<F>": 2 * p * N + c * nh_t,
+        "k_col<F>": c * nh_t + p * nh + c * nh,
+        "k_row_inv<F>": c * nh + 2 * p * Nd + 2 * p * N,
+    }
+
+
+def iteration_bytes(nx, ny, tx, ty, p=4, pt=4):
+    """Compulsory bytes of one CCG iteration with state resident:
+    p (5N + 2N_d) + 2 p_t N_h."""
+    return p * (5 * tx * ty + 2 * nx * ny) + 2 * pt * nx * (ny // 2 + 1)
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "c2_kernel_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import contactmechanics_b200 as cm
+    from contactmechanics_b200 import _lib
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    h = surface()
+    hd = torch.from_numpy(h).cuda()
+    sub = cm.FreeFFTElasticHalfSpace((N_TOPO, N_TOPO), 1.0, (1.0, 1.0))
+    L = _lib.load_library()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def sweep(precision, host=False, lat=None):
+        u0 = None
+        out = []
+        for p in PRESSURES:
+            F = float(p)
+            if lat is not None:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+            r = cm.constrained_conjugate_gradients(
+                sub, h if host else hd, external_force=F, precision=precision,
+                initial_displacements=u0, **tolerances(h, F))
+            if lat is not None:
+                e1.record()
+                e1.synchronize()
+                lat.append(e0.elapsed_time(e1))
+            if not r.success:
+                raise RuntimeError(f"solve at p={F} did not converge: {r.message}")
+            u0 = r.x
+            out.append(r)
+        return out
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(precision, steps, host=False, lat=None):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            res = sweep(precision, host=host, lat=lat)
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, res
+
+    for _ in range(args.warmup):
+        sweep("mixed")
+        sweep("fp64")
+    # headline: mixed precision, device-resident inputs
+    lat = []
+    n0 = L.cm_launch_count()
+    with ClockSampler(local_rank) as clocks:
+        ms_mixed, res_mixed = timed("mixed", args.steps, lat=lat)
+    launches = int(L.cm_launch_count() - n0)
+    ms_fp64, res_fp64 = timed("fp64", args.steps)
+    # end to end through the public API with host arrays
+    sweep("mixed", host=True)
+    ms_e2e, _ = timed("mixed", args.steps, host=True)
+
+    solves = len(PRESSURES) * args.steps
+    value = solves * world / (ms_mixed / 1e3)
+    fp64_value = solves * world / (ms_fp64 / 1e3)
+    e2e_value = solves * world / (ms_e2e / 1e3)
+    n = N_TOPO
+    errs, area_errs = [], []
+    for a, b in zip(res_mixed, res_fp64):
+        ua, ub = a.x[:n, :n], b.x[:n, :n]
+        errs.append(float(torch.linalg.norm(ua - ub) / torch.linalg.norm(ub)))
+        aa, ab = int((a.jac > 0).sum()), int((b.jac > 0).sum())
+        area_errs.append(abs(aa - ab) / max(ab, 1))
+    iters = [r.nit for r in res_mixed]
+    iters32 = [r.nit_fp32 for r in res_mixed]
+    iters64 = [r.nit for r in res_fp64]
+
+    # live per-kernel timing of the FP32 iteration (first load, cold start)
+    P = _lib.CcgParams()
+    P.precision = _lib.CM_FP32
+    P.load_control = 1
+    P.external_force = float(PRESSURES[0])
+    tol = tolerances(h, float(PRESSURES[0]))
+    P.pentol, P.forcetol, P.thermotol = tol["pentol"], tol["forcetol"], 1e-6
+    P.mixfac, P.mixdecfac, P.minmixsteps, P.maxiter = 0.1, 0.95, 10, 100000
+    ms_k = (ctypes.c_float * 16)()
+    nk = ctypes.c_int()
+    names = (ctypes.c_char_p * 16)()
+    torch.cuda.synchronize()
+    _lib.check(L.cm_ccg_profile(sub._plan.ptr, ctypes.byref(P), ctypes.c_void_p(hd.data_ptr()),
+                                20, ms_k, ctypes.byref(nk), names))
+    nxd, nyd = sub.nb_domain_grid_pts
+    kb = kernel_bytes(nxd, nyd, n, n)
+    per_kernel = {}
+    for i in range(nk.value):
+        name = names[i].decode()
+        per_kernel[name] = {"ms": float(ms_k[i]), "bytes": kb.get(name)}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["ms"])
+    peak, peak_kind = peaks()
+    t_dom = per_kernel[dom]["ms"] / 1e3
+    achieved = per_kernel[dom]["bytes"] / t_dom / 1e9
+    traffic = load_traffic().get(dom)
+    t_iter = sum(v["ms"] for v in per_kernel.values()) / 1e3
+    b_iter = iteration_bytes(nxd, nyd, n, n)
+    return dict(
+        value=value, ms_mixed=ms_mixed, fp64_value=fp64_value, ms_fp64=ms_fp64,
+        e2e_value=e2e_value, ms_e2e=ms_e2e, lat=lat, launches=launches,
+        clocks=clocks.summary(), rel_err=max(errs), area_err=max(area_errs),
+        iters=iters, iters32=iters32, iters64=iters64,
+        roofline={"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                  "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                  "traffic": traffic, "bytes_per_launch": per_kernel[dom]["bytes"],
+                  "ms_per_launch": per_kernel[dom]["ms"]},
+        iteration_roofline={"bytes": b_iter, "ms": t_iter * 1e3,
+                            "achieved": b_iter / t_iter / 1e9, "frac": b_iter / t_iter / 1e9 / peak},
+        per_kernel=per_kernel,
+        h2d=h.nbytes + nxd * nyd * 8, d2h=nxd * nyd * 8 + h.nbytes + nxd * nyd)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        s = cpu_sample(surface())
+        line = {"metric": METRIC, "value": s["value"], "unit": "solves/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "arm": "CPU oracle, bounded sample"},
+                "cpu_baseline": {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": s["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    r = run_gpu(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        s = cpu_sample(surface())
+        cpu = {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    lat = np.array(r["lat"])
+    solves_per_step = len(PRESSURES)
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_mixed"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solves_per_step": solves_per_step,
+                   "l2": "256 MB buffer written between steps (> 126 MB L2)",
+                   "parallelism": f"replicas x{world}", "precision": "mixed (FP32 bulk, FP64 "
+                   "reductions, FP64 refinement)"},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "fp64_value": r["fp64_value"], "speedup_vs_fp64": r["value"] / r["fp64_value"],
+        "rel_err_vs_fp64": r["rel_err"], "area_rel_err_vs_fp64": r["area_err"],
+        "iterations": {"mixed": r["iters"], "mixed_fp32_part": r["iters32"], "fp64": r["iters64"]},
+        "e2e": {"value": r["e2e_value"], "unit": "solves/s",
+                "h2d_bytes_per_step": r["h2d"] * solves_per_step,
+                "d2h_bytes_per_step": r["d2h"] * solves_per_step},
+        "gpu_launches": r["launches"],
+        "roofline": r["roofline"],
+        "iteration_roofline": r["iteration_roofline"],
+        "per_kernel_ms": {k: v["ms"] for k, v in r["per_kernel"].items()},
+        "clocks": r["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -85,6 +85,10 @@ SIGNATURES = {
                           ctypes.POINTER(CcgResult)]),
     "cm_ccg_solve_host": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp, ctypes.POINTER(CcgResult)]),
+    "cm_launch_count": (ctypes.c_ulonglong, []),
+    "cm_ccg_profile": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _i,
+                            ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i),
+                            ctypes.POINTER(ctypes.c_char_p)]),
 }
 
 _lock = threading.Lock()

@@ -76,3 +76,25 @@ CM_DEVINL void block_reduce(double (&v)[NV], const int (&kinds)[NV], double* sm)
   }
   __syncthreads();
 }
+
+// Loop over e in [0, n) with the block's threads, U indices per thread per
+// round: all U loads are issued before any use, so U global loads are in
+// flight per thread instead of one.
+template <int U, typename LoadF, typename UseF>
+CM_DEVINL void batched_loop(int n, LoadF load, UseF use) {
+  typedef decltype(load(0)) V;
+  const int T = blockDim.x;
+  for (int e0 = threadIdx.x; e0 < n; e0 += U * T) {
+    V v[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = e0 + i * T;
+      if (e < n) v[i] = load(e);
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = e0 + i * T;
+      if (e < n) use(e, v[i]);
+    }
+  }
+}

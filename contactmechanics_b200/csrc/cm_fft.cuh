@@ -3,14 +3,13 @@
 // A block transforms `nseq` complex sequences of length n held in shared
 // memory.  Element i of sequence s lives at buf[s*sstride + i*estride], so
 // the same engine serves row tiles (sequences contiguous) and column tiles
-// (sequences interleaved).  Radices 2,3,4,5,7,8 run in place with register
-// staging: every thread loads its butterflies' inputs, the block
-// synchronises, then every thread stores its outputs.  Any other prime
-// factor runs as an O(r^2) direct DFT stage out of place through `scratch`.
+// (sequences interleaved).  Stages ping-pong between two shared buffers
+// (out-of-place Stockham, self-sorting); radices 2,3,4,5,7,8 have unrolled
+// butterflies, any other prime factor runs as an O(r^2) direct DFT stage.
 //
 // Twiddles come from a per-length table tw[m] = exp(-2 pi i m / n), built on
-// the host in long double and rounded once, so FP64 transforms keep full
-// accuracy.
+// the host in long double and rounded once (so FP64 transforms keep full
+// accuracy) and staged in shared memory by each kernel.
 #pragma once
 #include "cm_common.cuh"
 
@@ -23,14 +22,15 @@ struct FftDesc {
   int rad[CM_MAX_STAGES];
 };
 
+// twiddle lookup (the table is staged in shared memory by the caller)
 template <typename C>
-CM_DEVINL C tw_get(const C* __restrict__ tw, int m) { return __ldg(tw + m); }
+CM_DEVINL C tw_get(const C* tw, int m) { return tw[m]; }
 
 // Length-RR DFT on registers.  Forward uses W = exp(-2 pi i / RR).
 template <bool INV, int RR, typename C>
 struct Dft {
   // generic small radix (3, 5, 7): direct sum with twiddles from the table
-  static CM_DEVINL void run(C (&v)[RR], const C* __restrict__ tw, int n) {
+  static CM_DEVINL void run(C (&v)[RR], const C* tw, int n) {
     C w[RR];
     const int ws = n / RR;
     w[0] = cmake<C>(1, 0);
@@ -105,54 +105,43 @@ struct Dft<INV, 8, C> {
   }
 };
 
-// One in-place Stockham stage of radix RR; each thread owns up to NB butterflies.
-template <typename C, bool INV, int RR, int NB>
-CM_DEVINL void fft_stage(C* buf, int n, int Ns, int nseq, int sstride, int estride,
-                         bool seq_fastest, const C* __restrict__ tw) {
+// One Stockham stage of radix RR from src to dst (out of place); every
+// thread walks its butterflies one at a time, so only RR values are live.
+template <typename C, bool INV, int RR>
+CM_DEVINL void fft_stage(const C* src, C* dst, int n, int Ns, int nseq, int sstride, int estride,
+                         bool seq_fastest, const C* tw) {
   const int m = n / RR;
   const int B = m * nseq;
   const int step = n / (Ns * RR);
-  C v[NB][RR];
-  int obase[NB];
+  for (int bi = threadIdx.x; bi < B; bi += blockDim.x) {
+    int s, j;
+    if (seq_fastest) { s = bi % nseq; j = bi / nseq; }
+    else { j = bi % m; s = bi / m; }
+    const C* in = src + s * sstride;
+    const int k = j % Ns;
+    C v[RR];
 #pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int bi = threadIdx.x + b * blockDim.x;
-    if (bi < B) {
-      int s, j;
-      if (seq_fastest) { s = bi % nseq; j = bi / nseq; }
-      else { j = bi % m; s = bi / m; }
-      const C* src = buf + s * sstride;
-      const int k = j % Ns;
+    for (int q = 0; q < RR; ++q) v[q] = in[(j + q * m) * estride];
+    if (Ns > 1) {
 #pragma unroll
-      for (int q = 0; q < RR; ++q) v[b][q] = src[(j + q * m) * estride];
-      if (Ns > 1) {
-#pragma unroll
-        for (int q = 1; q < RR; ++q) {
-          const C w = tw_get(tw, q * k * step);
-          v[b][q] = INV ? cmulc(v[b][q], w) : cmul(v[b][q], w);
-        }
+      for (int q = 1; q < RR; ++q) {
+        const C w = tw_get(tw, q * k * step);
+        v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
       }
-      Dft<INV, RR, C>::run(v[b], tw, n);
-      obase[b] = s * sstride + ((j - k) * RR + k) * estride;
     }
-  }
-  __syncthreads();
+    Dft<INV, RR, C>::run(v, tw, n);
+    C* out = dst + s * sstride + ((j - k) * RR + k) * estride;
 #pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int bi = threadIdx.x + b * blockDim.x;
-    if (bi < B) {
-#pragma unroll
-      for (int q = 0; q < RR; ++q) buf[obase[b] + q * Ns * estride] = v[b][q];
-    }
+    for (int q = 0; q < RR; ++q) out[q * Ns * estride] = v[q];
   }
   __syncthreads();
 }
 
-// Direct DFT stage for an arbitrary radix r, out of place through scratch.
+// Direct DFT stage for an arbitrary radix r (prime factors above 7).
 template <typename C, bool INV>
-CM_DEVINL void fft_stage_generic(C* buf, C* scratch, int n, int r, int Ns, int nseq,
+CM_DEVINL void fft_stage_generic(const C* src, C* dst, int n, int r, int Ns, int nseq,
                                  int sstride, int estride, bool seq_fastest,
-                                 const C* __restrict__ tw) {
+                                 const C* tw) {
   const int m = n / r;
   const int B = m * nseq;
   const int step = n / (Ns * r);
@@ -161,14 +150,14 @@ CM_DEVINL void fft_stage_generic(C* buf, C* scratch, int n, int r, int Ns, int n
     int s, j;
     if (seq_fastest) { s = bi % nseq; j = bi / nseq; }
     else { j = bi % m; s = bi / m; }
-    const C* src = buf + s * sstride;
-    C* dst = scratch + s * sstride;
+    const C* in = src + s * sstride;
+    C* out = dst + s * sstride;
     const int k = j % Ns;
     const int ob = (j - k) * r + k;
     for (int q = 0; q < r; ++q) {
       C acc = czero<C>();
       for (int p = 0; p < r; ++p) {
-        C x = src[(j + p * m) * estride];
+        C x = in[(j + p * m) * estride];
         if (Ns > 1 && p > 0) {
           const C w = tw_get(tw, p * k * step);
           x = INV ? cmulc(x, w) : cmul(x, w);
@@ -176,38 +165,33 @@ CM_DEVINL void fft_stage_generic(C* buf, C* scratch, int n, int r, int Ns, int n
         const C w = tw_get(tw, ((p * q) % r) * ws);
         acc = cadd(acc, INV ? cmulc(x, w) : cmul(x, w));
       }
-      dst[(ob + q * Ns) * estride] = acc;
+      out[(ob + q * Ns) * estride] = acc;
     }
-  }
-  __syncthreads();
-  const int total = n * nseq;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    int s, i;
-    if (seq_fastest) { s = e % nseq; i = e / nseq; }
-    else { i = e % n; s = e / n; }
-    const int off = s * sstride + i * estride;
-    buf[off] = scratch[off];
   }
   __syncthreads();
 }
 
-// Transform all sequences in place.  MAXE bounds the elements a thread holds
-// per stage; the host guarantees ceil(n*nseq/(r*blockDim)) <= ceil(MAXE/r).
-template <typename C, bool INV, int MAXE>
-CM_DEVINL void fft_smem(C* buf, C* scratch, const FftDesc& d, int nseq, int sstride,
-                        int estride, bool seq_fastest, const C* __restrict__ tw) {
+// Transform all sequences; data starts in `a`, `b` is a buffer of the same
+// size.  Returns the buffer that holds the result.
+template <typename C, bool INV>
+CM_DEVINL C* fft_smem(C* a, C* b, const FftDesc& d, int nseq, int sstride, int estride,
+                      bool seq_fastest, const C* tw) {
   int Ns = 1;
   for (int st = 0; st < d.nst; ++st) {
     const int r = d.rad[st];
     switch (r) {
-      case 8: fft_stage<C, INV, 8, (MAXE + 7) / 8>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      case 4: fft_stage<C, INV, 4, (MAXE + 3) / 4>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      case 2: fft_stage<C, INV, 2, (MAXE + 1) / 2>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      case 3: fft_stage<C, INV, 3, (MAXE + 2) / 3>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      case 5: fft_stage<C, INV, 5, (MAXE + 4) / 5>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      case 7: fft_stage<C, INV, 7, (MAXE + 6) / 7>(buf, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
-      default: fft_stage_generic<C, INV>(buf, scratch, d.n, r, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 8: fft_stage<C, INV, 8>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 4: fft_stage<C, INV, 4>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 2: fft_stage<C, INV, 2>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 3: fft_stage<C, INV, 3>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 5: fft_stage<C, INV, 5>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      case 7: fft_stage<C, INV, 7>(a, b, d.n, Ns, nseq, sstride, estride, seq_fastest, tw); break;
+      default: fft_stage_generic<C, INV>(a, b, d.n, r, Ns, nseq, sstride, estride, seq_fastest, tw); break;
     }
+    C* t = a;
+    a = b;
+    b = t;
     Ns *= r;
   }
+  return a;
 }

@@ -5,7 +5,7 @@
 //               rows are packed into one complex FFT and separated after.
 //               In a contact solve the prologue computes the field on the
 //               fly (search direction t, or the final force f).
-//   k_col     : per column block: FFT along x, multiply by the real Green's
+//   k_col     : per column tile: FFT along x, multiply by the real Green's
 //               table, inverse FFT along x.  Rows of the free (Hockney)
 //               domain beyond the topography are zero-filled, not read.
 //   k_row_inv : half spectrum -> real rows.  In a contact solve the epilogue
@@ -14,12 +14,18 @@
 //               writing an extra field.
 // CCG element-wise kernels (k_ccg_*) run over the topography region.
 //
+// Layout of the half spectrum and of the Green's tables in HBM: column tiles
+// of width W = 2^lw.  Element (x, k) lives at ((k >> lw) * nx + x) * W +
+// (k & (W-1)), so a column tile is one contiguous block (read and written
+// whole by k_col) and a row tile of R rows touches contiguous R*W runs.
+//
 // Every reduction is deterministic: per-tile partials in a fixed tile
 // order, reduced by the last tile of the slot (atomic ticket, no waiting).
 #pragma once
 #include "cm_slot.cuh"
 
-#define CM_THREADS 256
+#define CM_THREADS 256      // element-wise kernels
+#define CM_FFT_THREADS 512  // upper bound for the transform kernels
 
 enum {
   MODE_PLAIN = 0,  // operator on caller buffers
@@ -28,21 +34,25 @@ enum {
   MODE_FWD = 3,    // forward transform only (Green's table construction)
 };
 
+CM_DEVINL size_t spec_at(int x, int k, int nx, int lw) {
+  return (((size_t)(k >> lw) * nx + x) << lw) + (k & ((1 << lw) - 1));
+}
+
 // ---------------------------------------------------------------------------
 // last-tile reduction
 // ---------------------------------------------------------------------------
-template <int NV, typename R, typename Fin>
-CM_DEVINL void tile_finish(const Slot<R>& S, int tile, int ntiles, double (&v)[NV],
-                           const int (&kinds)[NV], Fin fin) {
+template <int NV, typename Fin>
+CM_DEVINL void tile_finish(double* __restrict__ partials, unsigned int* counter, int tile,
+                           int ntiles, double (&v)[NV], const int (&kinds)[NV], Fin fin) {
   __shared__ double red_sm[32 * NV];
   __shared__ int am_last;
   block_reduce<NV>(v, kinds, red_sm);
   if (threadIdx.x == 0) {
-    double* P = S.partials + (size_t)tile * NV;
+    double* P = partials + (size_t)tile * NV;
 #pragma unroll
     for (int i = 0; i < NV; ++i) P[i] = v[i];
     __threadfence();
-    const unsigned prev = atomicAdd(S.counter, 1u);
+    const unsigned prev = atomicAdd(counter, 1u);
     am_last = (prev == (unsigned)(ntiles - 1));
   }
   __syncthreads();
@@ -54,237 +64,364 @@ CM_DEVINL void tile_finish(const Slot<R>& S, int tile, int ntiles, double (&v)[N
   for (int tt = threadIdx.x; tt < ntiles; tt += blockDim.x) {
 #pragma unroll
     for (int i = 0; i < NV; ++i)
-      acc[i] = red_apply(kinds[i], acc[i], __ldcg(S.partials + (size_t)tt * NV + i));
+      acc[i] = red_apply(kinds[i], acc[i], __ldcg(partials + (size_t)tt * NV + i));
   }
   block_reduce<NV>(acc, kinds, red_sm);
   if (threadIdx.x == 0) {
     fin(acc);
-    *S.counter = 0;
+    *counter = 0;
   }
+}
+
+// stage the FFT descriptor and twiddle table of length n in shared memory
+template <typename C>
+CM_DEVINL void stage_fft(FftDesc& fd, const FftDesc& src, C* tws, const C* __restrict__ tw, int n) {
+  const int nint = (int)(sizeof(FftDesc) / sizeof(int));
+  for (int i = threadIdx.x; i < nint; i += blockDim.x)
+    reinterpret_cast<int*>(&fd)[i] = reinterpret_cast<const int*>(&src)[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tws[i] = __ldg(tw + i);
+}
+
+// scalar state of a contact solve that the operator prologues/epilogues use
+struct CcgView {
+  int par, has_h, uniform, apply_nc, branch;
+  double beta, offset, H, scale, tau, funif;
+};
+
+CM_DEVINL void load_view(const CcgState* st, CcgView& v) {
+  v.par = st->parity;
+  v.has_h = st->p.has_h;
+  v.uniform = st->uniform;
+  v.apply_nc = st->apply_nc;
+  v.branch = st->branch;
+  v.beta = st->beta;
+  v.offset = st->offset;
+  v.H = st->p.H;
+  v.scale = st->scale;
+  v.tau = st->tau;
+  v.funif = -st->p.F / st->p.n_surface;
 }
 
 // ---------------------------------------------------------------------------
 // operator passes
 // ---------------------------------------------------------------------------
-template <typename R, int MAXE, int MODE>
-__global__ void __launch_bounds__(CM_THREADS)
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
 k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   typedef typename CT<R>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
-  int par = 0, has_h = 0, uniform = 0, apply_nc = 0;
-  double beta = 0, offset = 0, H = 0, scale = 1, tau = 0, funif = 0;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  CcgView cv{};
   if (MODE == MODE_T || MODE == MODE_F) {
     if (st->done) return;
     if (MODE == MODE_T && st->branch != 0) return;
-    par = st->parity;
-    has_h = st->p.has_h;
-    H = st->p.H;
-    offset = st->offset;
-    beta = st->beta;
-    scale = st->scale;
-    tau = st->tau;
-    uniform = st->uniform;
-    apply_nc = st->apply_nc;
-    funif = -st->p.F / st->p.n_surface;
+    load_view(st, cv);
   }
-  const int ny = S.ny, nyh = S.nyh, ty = S.ty;
-  const int rows_total = (MODE == MODE_PLAIN || MODE == MODE_FWD) ? S.in_rows : S.tx;
-  const int x0 = item.y * S.row_tile;
-  const int nrows = min(S.row_tile, rows_total - x0);
+  const int nx = Sp->nx, ny = Sp->ny, nyh = Sp->nyh, ty = Sp->ty, lw = Sp->lw;
+  const int rows_total = (MODE == MODE_PLAIN || MODE == MODE_FWD) ? Sp->in_rows : Sp->tx;
+  const int row_tile = Sp->row_tile;
+  const int x0 = item.y * row_tile;
+  const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  C* scratch = buf + npairs * ny;
-  double acc = 0.0;
-  const R* fin = (MODE == MODE_T) ? S.f[par] : S.f[par ^ 1];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + ny;
+  C* scratch = buf + (row_tile >> 1) * ny;
+  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
+  C* __restrict__ spec = Sp->spec;
+  double acc = 0.0, amax = 0.0;
 
-  for (int e = threadIdx.x; e < npairs * ny; e += blockDim.x) {
-    const int p = e / ny, y = e - p * ny;
-    R vv[2] = {0, 0};
+  if (MODE == MODE_PLAIN || MODE == MODE_FWD) {
+    const R* __restrict__ in = Sp->in;
+    const int in_cols = Sp->in_cols, in_ld = Sp->in_ld;
+    batched_loop<4>(npairs * ny, [&](int e) {
+      const int p = e / ny, y = e - p * ny;
+      const int xa = x0 + 2 * p;
+      R va = 0, vb = 0;
+      if (y < in_cols) {
+        va = in[(size_t)xa * in_ld + y];
+        if (xa + 1 < x0 + nrows) vb = in[(size_t)(xa + 1) * in_ld + y];
+      }
+      return cmake<C>(va, vb);
+    }, [&](int e, C v) { buf[e] = v; });
+  } else {
+    const R* __restrict__ u = Sp->u;
+    const R* __restrict__ h = Sp->h;
+    R* __restrict__ fio = Sp->f[MODE == MODE_T ? cv.par : (cv.par ^ 1)];
+    R* __restrict__ t = Sp->t;
+    const R off = (R)cv.offset;
+    struct In { R f[2], u[2], h[2], t[2]; };
+    batched_loop<2>(npairs * ny, [&](int e) {
+      const int p = e / ny, y = e - p * ny;
+      In v;
 #pragma unroll
-    for (int w = 0; w < 2; ++w) {
-      const int x = x0 + 2 * p + w;
-      if (x >= x0 + nrows) continue;
-      if (MODE == MODE_PLAIN || MODE == MODE_FWD) {
-        if (y < S.in_cols) vv[w] = S.in[(size_t)x * S.in_ld + y];
-      } else if (y < ty) {
-        const size_t ic = (size_t)x * ty + y;
-        const size_t iu = (size_t)x * ny + y;
-        if (MODE == MODE_T) {
-          const R fa = fin[ic];
-          const bool c = (fa < 0) && (!has_h || (double)fa > -H);
-          const R g = (S.u[iu] - S.h[ic]) - (R)offset;
-          const R tn = c ? (R)(g + (R)beta * S.t[ic]) : (R)0;
-          S.t[ic] = tn;
-          if (c) acc += (double)g * (double)tn;
-          vv[w] = tn;
-        } else {  // MODE_F
-          const R fp = fin[ic];
-          double v = uniform ? funif : scale * (double)fp;
-          const bool flowing = has_h && (double)fp <= -H;
-          if (flowing) v = -H;
-          if (apply_nc) {
-            const R g = (S.u[iu] - S.h[ic]) - (R)offset;
-            const bool nc = ((fp == (R)0) && g < 0) || (flowing && g > 0);
-            if (nc) v += tau * (double)g;
+      for (int w = 0; w < 2; ++w) {
+        const int x = x0 + 2 * p + w;
+        v.f[w] = 0; v.u[w] = 0; v.h[w] = 0; v.t[w] = 0;
+        if (x < x0 + nrows && y < ty) {
+          const size_t ic = (size_t)x * ty + y;
+          v.f[w] = fio[ic];
+          if (MODE == MODE_T || cv.apply_nc) {
+            v.u[w] = u[(size_t)x * ny + y];
+            v.h[w] = h[ic];
           }
-          const R vr = (R)v;
-          S.f[par ^ 1][ic] = vr;
-          acc += (double)vr;
-          vv[w] = vr;
+          if (MODE == MODE_T) v.t[w] = t[ic];
         }
       }
-    }
-    buf[e] = cmake<C>(vv[0], vv[1]);
+      return v;
+    }, [&](int e, const In& v) {
+      const int p = e / ny, y = e - p * ny;
+      R vv[2] = {0, 0};
+      if (y < ty) {
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+          const int x = x0 + 2 * p + w;
+          if (x >= x0 + nrows) continue;
+          const size_t ic = (size_t)x * ty + y;
+          if (MODE == MODE_T) {
+            // search direction (ConstrainedConjugateGradients.py:276-279)
+            const R fa = v.f[w];
+            const bool c = (fa < 0) && (!cv.has_h || (double)fa > -cv.H);
+            const R g = (v.u[w] - v.h[w]) - off;
+            const R tn = c ? (R)(g + (R)cv.beta * v.t[w]) : (R)0;
+            t[ic] = tn;
+            if (c) acc += (double)g * (double)tn;
+            vv[w] = tn;
+          } else {
+            // final force of the iteration (:362-389)
+            const R fp = v.f[w];
+            double fv = cv.uniform ? cv.funif : cv.scale * (double)fp;
+            const bool flowing = cv.has_h && (double)fp <= -cv.H;
+            if (flowing) fv = -cv.H;
+            if (cv.apply_nc) {
+              const R g = (v.u[w] - v.h[w]) - off;
+              const bool nc = ((fp == (R)0) && g < 0) || (flowing && g > 0);
+              if (nc) fv += cv.tau * (double)g;
+            }
+            const R vr = (R)fv;
+            fio[ic] = vr;
+            acc += (double)vr;
+            amax = fmax(amax, fabs((double)vr));
+            vv[w] = vr;
+          }
+        }
+      }
+      buf[e] = cmake<C>(vv[0], vv[1]);
+    });
   }
   __syncthreads();
-  fft_smem<C, false, MAXE>(buf, scratch, S.fy, npairs, ny, 1, false, S.twy);
+  const C* res = fft_smem<C, false>(buf, scratch, fd, npairs, ny, 1, false, tws);
   for (int e = threadIdx.x; e < npairs * nyh; e += blockDim.x) {
     const int p = e / nyh, k = e - p * nyh;
-    const C z = buf[p * ny + k];
-    const C zm = buf[p * ny + (k == 0 ? 0 : ny - k)];
+    const C z = res[p * ny + k];
+    const C zm = res[p * ny + (k == 0 ? 0 : ny - k)];
     const int xa = x0 + 2 * p;
-    S.spec[(size_t)xa * nyh + k] = cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
+    spec[spec_at(xa, k, nx, lw)] = cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
     if (xa + 1 < x0 + nrows)
-      S.spec[(size_t)(xa + 1) * nyh + k] = cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5);
+      spec[spec_at(xa + 1, k, nx, lw)] = cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5);
   }
-  if (MODE == MODE_T || MODE == MODE_F) {
+  if (MODE == MODE_T) {
     double v[1] = {acc};
     const int kinds[1] = {RED_SUM};
-    tile_finish<1>(S, item.y, S.nt_rowt, v, kinds, [&](double (&a)[1]) {
-      if (MODE == MODE_T) st->sum_cgt = a[0];
-      else st->total_force = -a[0];
+    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds,
+                   [&](double (&a)[1]) { st->sum_cgt = a[0]; });
+  } else if (MODE == MODE_F) {
+    double v[2] = {acc, amax};
+    const int kinds[2] = {RED_SUM, RED_MAX};
+    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds, [&](double (&a)[2]) {
+      st->total_force = -a[0];
+      st->fmax = a[1];
     });
   }
 }
 
-template <typename R, int MAXE, int MODE>
-__global__ void __launch_bounds__(CM_THREADS)
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
 k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   typedef typename CT<R>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
   if (MODE == MODE_T || MODE == MODE_F) {
-    if (S.st->done) return;
-    if (MODE == MODE_T && S.st->branch != 0) return;
+    const CcgState* st = Sp->st;
+    if (st->done) return;
+    if (MODE == MODE_T && st->branch != 0) return;
   }
-  const int nx = S.nx, nyh = S.nyh;
-  const int k0 = item.y * S.col_tile;
-  const int wc = min(S.col_tile, nyh - k0);
+  const int nx = Sp->nx, nyh = Sp->nyh, lw = Sp->lw;
+  const int W = 1 << lw;
+  const int k0 = item.y * W;
+  const int wc = min(W, nyh - k0);
   int nx_in, nx_out;
-  const R* tab;
+  const R* __restrict__ tab;
   if (MODE == MODE_PLAIN || MODE == MODE_FWD) {
-    nx_in = S.in_rows;
-    nx_out = (MODE == MODE_FWD) ? nx : S.out_rows;
-    tab = S.tab[S.table_sel];
+    nx_in = Sp->in_rows;
+    nx_out = (MODE == MODE_FWD) ? nx : Sp->out_rows;
+    tab = Sp->tab[Sp->table_sel];
   } else {
-    nx_in = S.tx;
-    nx_out = (MODE == MODE_T) ? S.tx : nx;
-    tab = S.tab[0];
+    nx_in = Sp->tx;
+    nx_out = (MODE == MODE_T) ? Sp->tx : nx;
+    tab = Sp->tab[0];
   }
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  C* scratch = buf + nx * wc;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + nx;
+  C* scratch = buf + nx * W;
+  stage_fft(fd, Sp->fx, tws, Sp->twx, nx);
+  // the tile is one contiguous block of nx * W elements in HBM
+  C* __restrict__ blk = Sp->spec + (size_t)item.y * nx * W;
+  const R* __restrict__ tblk = tab + (size_t)item.y * nx * W;
   const int total = nx * wc;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int x = e / wc, c = e - x * wc;
-    buf[e] = (x < nx_in) ? S.spec[(size_t)x * nyh + k0 + c] : czero<C>();
+  if (wc == W) {
+    batched_loop<8>(nx_in * W, [&](int e) { return blk[e]; }, [&](int e, C v) { buf[e] = v; });
+    for (int e = nx_in * W + threadIdx.x; e < total; e += blockDim.x) buf[e] = czero<C>();
+  } else {
+    batched_loop<8>(total, [&](int e) {
+      const int x = e / wc, c = e - x * wc;
+      return (x < nx_in) ? blk[x * W + c] : czero<C>();
+    }, [&](int e, C v) { buf[e] = v; });
   }
   __syncthreads();
-  fft_smem<C, false, MAXE>(buf, scratch, S.fx, wc, 1, wc, true, S.twx);
+  C* res = fft_smem<C, false>(buf, scratch, fd, wc, 1, wc, true, tws);
   if (MODE != MODE_FWD) {
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    batched_loop<8>(total, [&](int e) {
       const int x = e / wc, c = e - x * wc;
-      buf[e] = cscale(buf[e], __ldg(tab + (size_t)x * nyh + k0 + c));
-    }
+      return __ldg(tblk + x * W + c);
+    }, [&](int e, R g) { res[e] = cscale(res[e], g); });
     __syncthreads();
-    fft_smem<C, true, MAXE>(buf, scratch, S.fx, wc, 1, wc, true, S.twx);
+    res = fft_smem<C, true>(res, res == buf ? scratch : buf, fd, wc, 1, wc, true, tws);
   }
-  for (int e = threadIdx.x; e < nx_out * wc; e += blockDim.x) {
-    const int x = e / wc, c = e - x * wc;
-    S.spec[(size_t)x * nyh + k0 + c] = buf[e];
+  if (wc == W) {
+    for (int e = threadIdx.x; e < nx_out * W; e += blockDim.x) blk[e] = res[e];
+  } else {
+    for (int e = threadIdx.x; e < nx_out * wc; e += blockDim.x) {
+      const int x = e / wc, c = e - x * wc;
+      blk[x * W + c] = res[e];
+    }
   }
 }
 
-template <typename R, int MAXE, int MODE>
-__global__ void __launch_bounds__(CM_THREADS)
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
 k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   typedef typename CT<R>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
-  int par = 0, has_h = 0, branch = 0;
-  double offset = 0, H = 0;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  CcgView cv{};
   if (MODE == MODE_T || MODE == MODE_F) {
     if (st->done) return;
-    branch = st->branch;
-    if (MODE == MODE_T && branch != 0) return;
-    par = st->parity;
-    has_h = st->p.has_h;
-    H = st->p.H;
-    offset = st->offset;
+    if (MODE == MODE_T && st->branch != 0) return;
+    load_view(st, cv);
   }
-  const int ny = S.ny, nyh = S.nyh, ty = S.ty, tx = S.tx;
-  const int rows_total = (MODE == MODE_PLAIN) ? S.out_rows : (MODE == MODE_T ? tx : S.nx);
-  const int x0 = item.y * S.row_tile;
-  const int nrows = min(S.row_tile, rows_total - x0);
+  const int nx = Sp->nx, ny = Sp->ny, nyh = Sp->nyh, ty = Sp->ty, tx = Sp->tx, lw = Sp->lw;
+  const int rows_total = (MODE == MODE_PLAIN) ? Sp->out_rows : (MODE == MODE_T ? tx : nx);
+  const int row_tile = Sp->row_tile;
+  const int x0 = item.y * row_tile;
+  const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  C* scratch = buf + npairs * ny;
-  for (int e = threadIdx.x; e < npairs * nyh; e += blockDim.x) {
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + ny;
+  C* scratch = buf + (row_tile >> 1) * ny;
+  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
+  const C* __restrict__ spec = Sp->spec;
+  struct XY { C X, Y; };
+  batched_loop<4>(npairs * nyh, [&](int e) {
     const int p = e / nyh, k = e - p * nyh;
     const int xa = x0 + 2 * p;
-    C X = S.spec[(size_t)xa * nyh + k];
-    C Y = (xa + 1 < x0 + nrows) ? S.spec[(size_t)(xa + 1) * nyh + k] : czero<C>();
+    XY v;
+    v.X = spec[spec_at(xa, k, nx, lw)];
+    v.Y = (xa + 1 < x0 + nrows) ? spec[spec_at(xa + 1, k, nx, lw)] : czero<C>();
+    return v;
+  }, [&](int e, XY v) {
+    const int p = e / nyh, k = e - p * nyh;
+    C X = v.X, Y = v.Y;
     const bool selfconj = (k == 0) || (2 * k == ny);
     if (selfconj) { X.y = 0; Y.y = 0; }
     buf[p * ny + k] = cmake<C>(X.x - Y.y, X.y + Y.x);
     if (!selfconj) buf[p * ny + ny - k] = cmake<C>(X.x + Y.y, Y.x - X.y);
-  }
+  });
   __syncthreads();
-  fft_smem<C, true, MAXE>(buf, scratch, S.fy, npairs, ny, 1, false, S.twy);
-  double a0 = 0.0, a1 = 0.0;  // MODE_T: sum r t ; MODE_F: max|du|, max penetration
-  if (MODE == MODE_F) { a0 = 0.0; a1 = -INFINITY; }
-  const R* fa_buf = S.f[par];
-  for (int e = threadIdx.x; e < npairs * ny; e += blockDim.x) {
-    const int p = e / ny, y = e - p * ny;
-    const C z = buf[e];
+  const C* res = fft_smem<C, true>(buf, scratch, fd, npairs, ny, 1, false, tws);
+  double a0 = 0.0, a1 = -INFINITY;  // MODE_T: sum r t ; MODE_F: max|du|, max penetration
+  if (MODE == MODE_PLAIN) {
+    R* __restrict__ out = Sp->out;
+    const int out_cols = Sp->out_cols, out_ld = Sp->out_ld;
+    for (int e = threadIdx.x; e < npairs * ny; e += blockDim.x) {
+      const int p = e / ny, y = e - p * ny;
+      if (y >= out_cols) continue;
+      const C z = res[e];
+      const int xa = x0 + 2 * p;
+      out[(size_t)xa * out_ld + y] = z.x;
+      if (xa + 1 < x0 + nrows) out[(size_t)(xa + 1) * out_ld + y] = z.y;
+    }
+  } else if (MODE == MODE_T) {
+    const R* __restrict__ t = Sp->t;
+    struct T2 { R a, b; };
+    batched_loop<4>(npairs * ny, [&](int e) {
+      const int p = e / ny, y = e - p * ny;
+      const int xa = x0 + 2 * p;
+      T2 v{0, 0};
+      if (y < ty) {
+        v.a = t[(size_t)xa * ty + y];
+        if (xa + 1 < x0 + nrows) v.b = t[(size_t)(xa + 1) * ty + y];
+      }
+      return v;
+    }, [&](int e, T2 v) {
+      const C z = res[e];
+      a0 += (double)z.x * (double)v.a + (double)z.y * (double)v.b;
+    });
+  } else {
+    R* __restrict__ u = Sp->u;
+    const R* __restrict__ h = Sp->h;
+    const R* __restrict__ fa_buf = Sp->f[cv.par];
+    const unsigned char* __restrict__ gneg = Sp->gneg;
+    const R off = (R)cv.offset;
+    struct UF { R uo[2], fa[2], h[2]; unsigned char gn[2]; };
+    batched_loop<2>(npairs * ny, [&](int e) {
+      const int p = e / ny, y = e - p * ny;
+      UF v;
 #pragma unroll
-    for (int w = 0; w < 2; ++w) {
-      const int x = x0 + 2 * p + w;
-      if (x >= x0 + nrows) continue;
-      const R val = w ? z.y : z.x;
-      if (MODE == MODE_PLAIN) {
-        if (y < S.out_cols) S.out[(size_t)x * S.out_ld + y] = val;
-      } else if (MODE == MODE_T) {
-        if (y < ty) a0 += (double)val * (double)S.t[(size_t)x * ty + y];
-      } else {  // MODE_F: displacement update
-        const size_t iu = (size_t)x * ny + y;
-        const R uo = S.u[iu];
-        a0 = fmax(a0, (double)fabs(val - uo));
-        S.u[iu] = val;
+      for (int w = 0; w < 2; ++w) {
+        const int x = x0 + 2 * p + w;
+        v.uo[w] = 0; v.fa[w] = 0; v.h[w] = 0; v.gn[w] = 0;
+        if (x >= x0 + nrows) continue;
+        v.uo[w] = u[(size_t)x * ny + y];
         if (x < tx && y < ty) {
           const size_t ic = (size_t)x * ty + y;
+          v.h[w] = h[ic];
+          if (cv.branch == 0) v.fa[w] = fa_buf[ic];
+          else v.gn[w] = gneg[ic];
+        }
+      }
+      return v;
+    }, [&](int e, const UF& v) {
+      const int p = e / ny, y = e - p * ny;
+      const C z = res[e];
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = x0 + 2 * p + w;
+        if (x >= x0 + nrows) continue;
+        const R val = w ? z.y : z.x;
+        a0 = fmax(a0, (double)fabs(val - v.uo[w]));
+        u[(size_t)x * ny + y] = val;
+        if (x < tx && y < ty) {
           bool c;
-          if (branch == 0) {
-            const R fa = fa_buf[ic];
-            c = (fa < 0) && (!has_h || (double)fa > -H);
-          } else {
-            c = S.gneg[ic] != 0;
-          }
-          const R pen = (S.h[ic] + (R)offset) - val;
+          if (cv.branch == 0) c = (v.fa[w] < 0) && (!cv.has_h || (double)v.fa[w] > -cv.H);
+          else c = v.gn[w] != 0;
+          const R pen = (v.h[w] + off) - val;
           a1 = fmax(a1, c ? (double)pen : 0.0);
         }
       }
-    }
+    });
   }
   if (MODE == MODE_T) {
     double v[1] = {a0};
     const int kinds[1] = {RED_SUM};
-    tile_finish<1>(S, item.y, S.nt_rowt, v, kinds, [&](double (&a)[1]) {
+    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds, [&](double (&a)[1]) {
       // step length (ConstrainedConjugateGradients.py:287-294)
       double tau = 0.0;
       if (st->A_cg > 0) {
@@ -298,7 +435,7 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   } else if (MODE == MODE_F) {
     double v[2] = {a0, a1};
     const int kinds[2] = {RED_MAX, RED_MAX};
-    tile_finish<2>(S, item.y, S.nt_rowd, v, kinds, [&](double (&a)[2]) {
+    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowd, v, kinds, [&](double (&a)[2]) {
       // convergence test (ConstrainedConjugateGradients.py:391-434, 491-492)
       CcgState& s = *st;
       const CcgParams& P = s.p;
@@ -317,11 +454,12 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
       if (P.load_control && s.have_last_mh) conv = conv && fabs((mh - s.last_mh) / mh) < P.thermotol;
       s.last_mh = mh;
       s.have_last_mh = 1;
+      const double ftol = fmax(P.forcetol, P.rel_forcetol * s.fmax);
       if (s.mode == CMM_MIX)
-        conv = conv && s.maxdu < P.pentol && s.max_pres < P.forcetol && s.pad_pres < P.forcetol;
+        conv = conv && s.maxdu < P.pentol && s.max_pres < ftol && s.pad_pres < ftol;
       else
         conv = conv && s.rms_pen < P.pentol && s.max_pen < P.pentol && s.maxdu < P.pentol &&
-               s.max_pres < P.forcetol && s.pad_pres < P.forcetol;
+               s.max_pres < ftol && s.pad_pres < ftol;
       s.parity ^= 1;
       if (conv) {
         s.status = CMS_CONVERGED;
@@ -342,11 +480,27 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
 // ---------------------------------------------------------------------------
 // CCG element-wise kernels over the topography region
 // ---------------------------------------------------------------------------
-#define CM_COMP_LOOP(S, tile)                                              \
-  const int cx0 = (tile) * (S).comp_rows;                                  \
-  const int crows = min((S).comp_rows, (S).tx - cx0);                      \
-  const int cn = crows * (S).ty;                                           \
-  for (int e = threadIdx.x; e < cn; e += blockDim.x)
+// Fields of one comp tile (rows [cx0, cx0+crows) of the topography) in registers.
+template <typename R>
+struct CompTile {
+  int cx0, cn, ty, ny;
+  const R* __restrict__ u;
+  const R* __restrict__ h;
+  CM_DEVINL CompTile(const Slot<R>* Sp, int tile) {
+    ty = Sp->ty;
+    ny = Sp->ny;
+    cx0 = tile * Sp->comp_rows;
+    cn = min(Sp->comp_rows, Sp->tx - cx0) * ty;
+    u = Sp->u;
+    h = Sp->h;
+  }
+  // topography index and displacement index of element e of the tile
+  CM_DEVINL void at(int e, size_t& ic, size_t& iu) const {
+    const int r = e / ty, y = e - r * ty;
+    ic = (size_t)cx0 * ty + e;
+    iu = (size_t)(cx0 + r) * ny + y;
+  }
+};
 
 // Start of an iteration: contact areas, raw-gap sums, step kind and offset
 // (ConstrainedConjugateGradients.py:239-270, 300-318).
@@ -354,29 +508,32 @@ template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
   if (st->done) return;
-  const int par = st->parity, has_h = st->p.has_h;
+  const int has_h = st->p.has_h;
   const double H = st->p.H;
-  const R* f = S.f[par];
+  const R* __restrict__ f = Sp->f[st->parity];
+  const CompTile<R> T(Sp, item.y);
   double a_c = 0, a_cg = 0, s_cg = 0, gmax = -INFINITY, gmin = INFINITY;
-  CM_COMP_LOOP(S, item.y) {
-    const int r = e / S.ty, y = e - r * S.ty;
-    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
-    const R fa = f[ic];
-    const bool c0 = fa < 0;
-    const bool c = c0 && (!has_h || (double)fa > -H);
-    const R g = S.u[(size_t)(cx0 + r) * S.ny + y] - S.h[ic];
+  struct V3 { R f, u, h; };
+  batched_loop<4>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V3{f[ic], T.u[iu], T.h[ic]};
+  }, [&](int, V3 v) {
+    const bool c0 = v.f < 0;
+    const bool c = c0 && (!has_h || (double)v.f > -H);
+    const R g = v.u - v.h;
     a_c += c0;
     a_cg += c;
     if (c) s_cg += (double)g;
     gmax = fmax(gmax, (double)g);
     gmin = fmin(gmin, (double)g);
-  }
+  });
   double v[5] = {a_c, a_cg, s_cg, gmax, gmin};
   const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-  tile_finish<5>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[5]) {
+  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[5]) {
     CcgState& s = *st;
     const CcgParams& P = s.p;
     s.A_contact = (long long)a[0];
@@ -414,25 +571,28 @@ template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
   if (st->done || st->branch != 0) return;
-  const int par = st->parity, has_h = st->p.has_h;
+  const int has_h = st->p.has_h;
   const double H = st->p.H;
   const R off = (R)st->offset;
-  const R* f = S.f[par];
+  const R* __restrict__ f = Sp->f[st->parity];
+  const CompTile<R> T(Sp, item.y);
   double G = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const int r = e / S.ty, y = e - r * S.ty;
-    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
-    const R fa = f[ic];
-    const bool c = (fa < 0) && (!has_h || (double)fa > -H);
-    const R g = (S.u[(size_t)(cx0 + r) * S.ny + y] - S.h[ic]) - off;
+  struct V3 { R f, u, h; };
+  batched_loop<4>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V3{f[ic], T.u[iu], T.h[ic]};
+  }, [&](int, V3 v) {
+    const bool c = (v.f < 0) && (!has_h || (double)v.f > -H);
+    const R g = (v.u - v.h) - off;
     if (c) G += (double)g * (double)g;
-  }
+  });
   double v[1] = {G};
   const int kinds[1] = {RED_SUM};
-  tile_finish<1>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[1]) {
+  tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[1]) {
     CcgState& s = *st;
     s.G = a[0];
     s.beta = (s.delta > 0 && s.G_old > 0) ? (double)s.delta * (s.G / s.G_old) : 0.0;
@@ -447,28 +607,33 @@ template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
   if (st->done || st->branch != 1 || !st->bs_active) return;
   __shared__ double cand[CM_BIS_CAND];
   const int ncand = (st->bs_iter < 0) ? 1 : CM_BIS_CAND;
   if (threadIdx.x < ncand) cand[threadIdx.x] = st->bs_cand[threadIdx.x];
   __syncthreads();
+  const CompTile<R> T(Sp, item.y);
   double cnt[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const int r = e / S.ty, y = e - r * S.ty;
-    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
-    const double g = (double)(S.u[(size_t)(cx0 + r) * S.ny + y] - S.h[ic]);
+  struct V2 { R u, h; };
+  batched_loop<4>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V2{T.u[iu], T.h[ic]};
+  }, [&](int, V2 v) {
+    const double g = (double)(v.u - v.h);
 #pragma unroll
     for (int i = 0; i < CM_BIS_CAND; ++i)
       if (i < ncand) cnt[i] += (g - cand[i] < 0.0) ? 1.0 : 0.0;
-  }
+  });
   int kinds[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
-  tile_finish<CM_BIS_CAND>(S, item.y, S.nt_comp, cnt, kinds, [&](double (&a)[CM_BIS_CAND]) {
+  tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, cnt, kinds,
+                           [&](double (&a)[CM_BIS_CAND]) {
     CcgState& s = *st;
     const double H = s.p.H, F = s.p.F;
     const double xtol = 2e-12, rtol = 8.881784197001252e-16;
@@ -533,26 +698,33 @@ template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  CcgState* st = S.st;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
   if (st->done) return;
   const int par = st->parity, has_h = st->p.has_h, branch = st->branch;
   const double H = st->p.H;
   const R off = (R)st->offset;
   const R tau = (R)st->tau;
   const double mix = st->cur_mixfac;
-  const R* f = S.f[par];
-  R* fo = S.f[par ^ 1];
+  const R* __restrict__ f = Sp->f[par];
+  R* __restrict__ fo = Sp->f[par ^ 1];
+  const R* __restrict__ t = Sp->t;
+  unsigned char* __restrict__ gneg = Sp->gneg;
+  const CompTile<R> T(Sp, item.y);
   double a_fl = 0, min_fl = INFINITY, max_t = 0, s_fp = 0, n_nc = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const int r = e / S.ty, y = e - r * S.ty;
-    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
-    const R fa = f[ic];
-    const R g = (S.u[(size_t)(cx0 + r) * S.ny + y] - S.h[ic]) - off;
+  struct V4 { R f, u, h, t; };
+  batched_loop<4>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V4{f[ic], T.u[iu], T.h[ic], branch == 0 ? t[ic] : (R)0};
+  }, [&](int e, V4 v) {
+    const size_t ic = (size_t)T.cx0 * T.ty + e;
+    const R fa = v.f;
+    const R g = (v.u - v.h) - off;
     R fn;
     if (branch == 0) {
       const bool c = (fa < 0) && (!has_h || (double)fa > -H);
-      fn = c ? (R)(fa + tau * S.t[ic]) : fa;
+      fn = c ? (R)(fa + tau * v.t) : fa;
     } else {
       fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
     }
@@ -565,11 +737,11 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     s_fp += (double)fp;
     n_nc += nc;
     fo[ic] = fp;
-    if (has_h) S.gneg[ic] = g < 0;
-  }
+    if (has_h) gneg[ic] = g < 0;
+  });
   double v[5] = {a_fl, min_fl, max_t, s_fp, n_nc};
   const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
-  tile_finish<5>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[5]) {
+  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[5]) {
     CcgState& s = *st;
     const CcgParams& P = s.p;
     s.A_fl = (long long)a[0];

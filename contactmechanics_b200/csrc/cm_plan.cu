@@ -13,13 +13,12 @@
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
 
-#define CM_MAXE32 32
-#define CM_MAXE64 16
-#define CM_SMEM_BUDGET (64 * 1024)
-#define CM_ELEMS_TARGET 4096
-#define CM_COMP_ELEMS 8192
+#define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
+#define CM_SMEM_COL_MAX (160 * 1024)
+#define CM_COMP_ELEMS 2048
 #define CM_BISECT_PASSES 21
 #define CM_MAX_PARTIAL_VALS 32
+#define CM_FP32_ITER_CAP 2000
 
 #define CK(...)                               \
   do {                                        \
@@ -35,6 +34,8 @@
     int s_ = (__VA_ARGS__);          \
     if (s_ != CM_OK) return s_;      \
   } while (0)
+
+static unsigned long long g_launches = 0;  // kernels launched by this library
 
 static cudaError_t& last_cuda_error() {
   static thread_local cudaError_t e = cudaSuccess;
@@ -82,40 +83,41 @@ static std::vector<C> make_twiddles(int n) {
   return tw;
 }
 
-// elements a thread holds in the worst stage of a transform of nseq sequences
-static bool fits_regs(const FftDesc& d, long nseq, int maxe) {
-  for (int s = 0; s < d.nst; ++s) {
-    const int r = d.rad[s];
-    if (r > 8 || r == 6) continue;  // generic stages use no register staging
-    const long B = (long)d.n / r * nseq;
-    const long nb = (B + CM_THREADS - 1) / CM_THREADS;
-    if (nb > (maxe + r - 1) / r) return false;
-  }
-  return true;
-}
-
 struct Tiles {
-  int row_tile, col_tile, comp_rows;
+  int row_tile, col_tile, lw, comp_rows;
+  int threads_row, threads_col;
   size_t smem_row, smem_col;
+  int ntile_cols;  // number of spectrum column tiles
 };
 
-static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, const FftDesc& fx,
-                        const FftDesc& fy, size_t csize, int maxe, Tiles* t) {
-  const int gy = fy.generic ? 2 : 1, gx = fx.generic ? 2 : 1;
-  // rows: pairs of real rows per block
-  int max_pairs = (nx + 1) / 2;
-  int want = std::max(1, CM_ELEMS_TARGET / ny);
-  int np = std::min(max_pairs, want);
-  while (np > 1 && ((size_t)np * ny * csize * gy > CM_SMEM_BUDGET || !fits_regs(fy, np, maxe))) --np;
-  if ((size_t)np * ny * csize * gy > 200 * 1024 || !fits_regs(fy, np, maxe)) return CM_ERR_SIZE;
+static int pow2_threads(size_t work) {
+  // about sixteen transform elements per thread, 128..256 threads
+  size_t t = 128;
+  while (t < 256 && t * 16 < work) t *= 2;
+  return (int)t;
+}
+
+// Tile shapes: a row tile holds `row_tile` real rows (packed in pairs), a
+// column tile `col_tile` = 2^lw half-spectrum columns.  Shared memory holds
+// the twiddles of the transform plus two ping-pong buffers.
+static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, Tiles* t) {
+  const size_t elems = CM_SMEM_ROW / (2 * csize);
+  int np = (int)std::max<size_t>(1, elems / (size_t)ny);
+  np = std::min(np, (nx + 1) / 2);
+  const size_t srow = (2 * (size_t)np * ny + ny) * csize;
+  if (srow > CM_SMEM_COL_MAX) return CM_ERR_SIZE;
   t->row_tile = 2 * np;
-  t->smem_row = (size_t)np * ny * csize * gy;
-  // columns of the half spectrum per block
-  int w = std::min(nyh, std::max(1, CM_ELEMS_TARGET / nx));
-  while (w > 1 && ((size_t)w * nx * csize * gx > CM_SMEM_BUDGET || !fits_regs(fx, w, maxe))) --w;
-  if ((size_t)w * nx * csize * gx > 200 * 1024 || !fits_regs(fx, w, maxe)) return CM_ERR_SIZE;
-  t->col_tile = w;
-  t->smem_col = (size_t)w * nx * csize * gx;
+  t->smem_row = srow;
+  t->threads_row = pow2_threads((size_t)np * ny);
+  int lw = 0;
+  while ((2ul << lw) * (size_t)nx <= elems && (1 << (lw + 1)) <= nyh) ++lw;
+  const size_t scol = (2 * ((size_t)1 << lw) * nx + nx) * csize;
+  if (scol > CM_SMEM_COL_MAX) return CM_ERR_SIZE;
+  t->lw = lw;
+  t->col_tile = 1 << lw;
+  t->smem_col = scol;
+  t->threads_col = pow2_threads(((size_t)1 << lw) * nx);
+  t->ntile_cols = (nyh + t->col_tile - 1) / t->col_tile;
   t->comp_rows = std::max(1, std::min(tx, CM_COMP_ELEMS / std::max(1, ty)));
   return CM_OK;
 }
@@ -179,22 +181,30 @@ __global__ void k_love(double* out, int tx, int ty, int nxd, int nyd, double dx,
   }
 }
 
-__global__ void k_real_part(const double2* spec, double* G, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    G[i] = spec[i].x;
+// real part of a spectrum stored in column tiles of width 2^lw -> natural (nx, nyh)
+__global__ void k_real_part(const double2* spec, double* G, int nx, int nyh, int lw) {
+  const long n = (long)nx * nyh;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / nyh), k = (int)(i % nyh);
+    G[i] = spec[spec_at(x, k, nx, lw)].x;
+  }
 }
 
-// Scaled operator tables: disp = -G/(a N), force = -K a / N with K = 1/G (G != 0).
-__global__ void k_tables_scale(const double* G, long n, double aN_inv, double a_over_N,
-                               double* td, double* tf, float* td32, float* tf32) {
+// Scaled operator tables in the tiled spectrum layout of each precision:
+// disp = -G/(a N), force = -K a / N with K = 1/G (G != 0).
+__global__ void k_tables_scale(const double* G, int nx, int nyh, double aN_inv, double a_over_N,
+                               double* td, double* tf, int lw64, float* td32, float* tf32, int lw32) {
+  const long n = (long)nx * nyh;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / nyh), k = (int)(i % nyh);
     const double g = G[i];
-    const double k = (g != 0.0) ? 1.0 / g : 0.0;
-    const double d = -g * aN_inv, f = -k * a_over_N;
-    td[i] = d;
-    tf[i] = f;
-    td32[i] = (float)d;
-    tf32[i] = (float)f;
+    const double kk = (g != 0.0) ? 1.0 / g : 0.0;
+    const double d = -g * aN_inv, f = -kk * a_over_N;
+    const size_t j64 = spec_at(x, k, nx, lw64), j32 = spec_at(x, k, nx, lw32);
+    td[j64] = d;
+    tf[j64] = f;
+    td32[j32] = (float)d;
+    tf32[j32] = (float)f;
   }
 }
 
@@ -206,22 +216,25 @@ template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_h_prep(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  const CompTile<R> T(Sp, item.y);
+  R* __restrict__ h = const_cast<R*>(Sp->h);
+  const size_t base = (size_t)T.cx0 * T.ty;
   double mx = -INFINITY, mn = INFINITY, sm = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const size_t ic = (size_t)cx0 * S.ty + e;
-    const double h = h64[ic];
-    const_cast<R*>(S.h)[ic] = (R)h;
-    mx = fmax(mx, h);
-    mn = fmin(mn, h);
-    sm += h;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    const double hv = h64[base + e];
+    h[base + e] = (R)hv;
+    mx = fmax(mx, hv);
+    mn = fmin(mn, hv);
+    sm += hv;
   }
   double v[3] = {mx, mn, sm};
   const int kinds[3] = {RED_MAX, RED_MIN, RED_SUM};
-  tile_finish<3>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[3]) {
-    S.st->p.max_surface = a[0];
-    S.st->gmin = a[1];  // scratch until the loop starts
-    S.st->sum_cg = a[2];
+  CcgState* st = Sp->st;
+  tile_finish<3>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[3]) {
+    st->p.max_surface = a[0];
+    st->gmin = a[1];  // scratch until the loop starts
+    st->sum_cg = a[2];
   });
 }
 
@@ -232,20 +245,24 @@ __global__ void __launch_bounds__(CM_THREADS)
 k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64,
         int pentol_auto, double rel_pentol) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  const double mean = S.st->sum_cg / S.st->p.n_surface;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  const CompTile<R> T(Sp, item.y);
+  const size_t base = (size_t)T.cx0 * T.ty;
+  const double mean = st->sum_cg / st->p.n_surface;
   double v2 = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const double d = h64[(size_t)cx0 * S.ty + e] - mean;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    const double d = h64[base + e] - mean;
     v2 += d * d;
   }
   double v[1] = {v2};
   const int kinds[1] = {RED_SUM};
-  tile_finish<1>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[1]) {
-    CcgState& s = *S.st;
+  const int tx = Sp->tx, ty = Sp->ty;
+  tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[1]) {
+    CcgState& s = *st;
     if (pentol_auto) {
       const double rms = sqrt(a[0] / s.p.n_surface);
-      double pt = rms / (10.0 * (0.5 * ((double)S.tx + (double)S.ty)));
+      double pt = rms / (10.0 * (0.5 * ((double)tx + (double)ty)));
       if (pt == 0) pt = (s.p.offset0 + s.sum_cg / s.p.n_surface) / 1000;
       if (pt == 0) pt = 1e-3;
       s.p.pentol = pt;
@@ -289,23 +306,25 @@ __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_result(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, double* jac,
              unsigned char* active, unsigned char* plastic) {
   const int2 item = items[blockIdx.x];
-  const Slot<R>& S = slots[item.x];
-  const CcgState* st = S.st;
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
   const int par = st->parity, has_h = st->p.has_h, mixing = (st->branch == 1);
   const double H = st->p.H;
-  const R* ff = S.f[par];       // final force
-  const R* fa = S.f[par ^ 1];   // force at the start of the last iteration
+  const R* __restrict__ ff = Sp->f[par];       // final force
+  const R* __restrict__ fa = Sp->f[par ^ 1];   // force at the start of the last iteration
+  const unsigned char* __restrict__ gneg = Sp->gneg;
+  const CompTile<R> T(Sp, item.y);
   double e_sum = 0, area = 0, cg_area = 0, pl = 0;
-  CM_COMP_LOOP(S, item.y) {
-    const int r = e / S.ty, y = e - r * S.ty;
-    const size_t ic = (size_t)(cx0 + r) * S.ty + y;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
     const R f = ff[ic];
-    const R u = S.u[(size_t)(cx0 + r) * S.ny + y];
+    const R u = T.u[iu];
     e_sum += (double)f * (double)u;
     if (jac) jac[ic] = -(double)f;
     area += (f < 0);
     bool act;
-    if (mixing) act = S.gneg[ic] != 0;
+    if (mixing) act = gneg[ic] != 0;
     else {
       const R a = fa[ic];
       act = (a < 0) && (!has_h || (double)a > -H);
@@ -313,15 +332,15 @@ k_ccg_result(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, 
     cg_area += act;
     if (active) active[ic] = act;
     if (has_h) {
-      const bool p = S.gneg[ic] != 0;
+      const bool p = gneg[ic] != 0;
       pl += p;
       if (plastic) plastic[ic] = p;
     }
   }
   double v[4] = {e_sum, area, cg_area, pl};
   const int kinds[4] = {RED_SUM, RED_SUM, RED_SUM, RED_SUM};
-  tile_finish<4>(S, item.y, S.nt_comp, v, kinds, [&](double (&a)[4]) {
-    CcgState& s = *S.st;
+  tile_finish<4>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[4]) {
+    CcgState& s = *st;
     s.sum_cgt = -a[0] / 2;  // result.fun
     s.A_contact = (long long)a[1];
     s.A_cg = (long long)a[2];
@@ -414,23 +433,30 @@ static int grid_for(long n) {
   return (int)g;
 }
 
-template <typename R, int MAXE>
+template <typename R>
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
   done = true;
   const int mx = 200 * 1024;
-  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_fwd<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col<R, MAXE, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_row_inv<R, MAXE, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  const int carve = cudaSharedmemCarveoutMaxShared;
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_F>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_col<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_col<R, MODE_F>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_row_inv<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_row_inv<R, MODE_F>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_fwd<R, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col<R, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MODE_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MODE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_inv<R, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 template <typename R>
@@ -444,11 +470,12 @@ static Slot<R> base_slot(cm_plan* p, Work<R>& w) {
   s.ty = p->ty;
   s.row_tile = w.tiles.row_tile;
   s.col_tile = w.tiles.col_tile;
+  s.lw = w.tiles.lw;
   s.comp_rows = w.tiles.comp_rows;
   s.nt_comp = (p->tx + s.comp_rows - 1) / s.comp_rows;
   s.nt_rowt = (p->tx + s.row_tile - 1) / s.row_tile;
   s.nt_rowd = (p->nx + s.row_tile - 1) / s.row_tile;
-  s.nt_col = (p->nyh + s.col_tile - 1) / s.col_tile;
+  s.nt_col = w.tiles.ntile_cols;
   s.fx = p->fx;
   s.fy = p->fy;
   s.twx = w.twx;
@@ -469,21 +496,21 @@ static Slot<R> base_slot(cm_plan* p, Work<R>& w) {
 }
 
 template <typename R>
-static int init_work(cm_plan* p, Work<R>& w, int maxe) {
+static int init_work(cm_plan* p, Work<R>& w) {
   typedef typename CT<R>::C C;
-  CKS(choose_tiles(p->nx, p->ny, p->nyh, p->tx, p->ty, p->fx, p->fy, sizeof(C), maxe, &w.tiles));
+  CKS(choose_tiles(p->nx, p->ny, p->nyh, p->tx, p->ty, sizeof(C), &w.tiles));
   std::vector<C> twx = make_twiddles<C>(p->nx), twy = make_twiddles<C>(p->ny);
   CKS(dalloc(p, &w.twx, p->nx));
   CKS(dalloc(p, &w.twy, p->ny));
   CK(cudaMemcpy(w.twx, twx.data(), sizeof(C) * p->nx, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(w.twy, twy.data(), sizeof(C) * p->ny, cudaMemcpyHostToDevice));
-  CKS(dalloc(p, &w.spec, (size_t)p->nx * p->nyh));
+  CKS(dalloc(p, &w.spec, (size_t)p->nx * w.tiles.ntile_cols * w.tiles.col_tile));
   CKS(dalloc(p, &w.d_plain, 1));
   CKS(dalloc(p, &w.d_ccg, 1));
   // reduction scratch is shared by the plain-operator slot and the solver
   const int nt_max = std::max({(p->tx + w.tiles.comp_rows - 1) / w.tiles.comp_rows,
                                (p->nx + w.tiles.row_tile - 1) / w.tiles.row_tile,
-                               (p->nyh + w.tiles.col_tile - 1) / w.tiles.col_tile, 1});
+                               w.tiles.ntile_cols, 1});
   CKS(dalloc(p, &w.partials, (size_t)nt_max * CM_MAX_PARTIAL_VALS));
   CKS(dalloc(p, &w.counter, 1));
   CK(cudaMemset(w.counter, 0, sizeof(unsigned int)));
@@ -515,11 +542,11 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
   return CM_OK;
 }
 
-template <typename R, int MAXE>
+template <typename R>
 static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R* in, int in_rows,
                         int in_cols, int in_ld, R* out, int out_rows, int out_cols, int out_ld,
                         cudaStream_t s) {
-  set_smem_attrs<R, MAXE>();
+  set_smem_attrs<R>();
   Slot<R> hs = base_slot(p, w);
   hs.in = in;
   hs.out = out;
@@ -533,13 +560,14 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
   CK(cudaMemcpyAsync(w.d_plain, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
   const int nt_in = (in_rows + hs.row_tile - 1) / hs.row_tile;
   const int nt_out = (out_rows + hs.row_tile - 1) / hs.row_tile;
+  g_launches += (mode == MODE_FWD) ? 2 : 3;
   if (mode == MODE_FWD) {
-    k_row_fwd<R, MAXE, MODE_FWD><<<nt_in, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
-    k_col<R, MAXE, MODE_FWD><<<hs.nt_col, CM_THREADS, w.tiles.smem_col, s>>>(w.d_plain, p->items);
+    k_row_fwd<R, MODE_FWD><<<nt_in, w.tiles.threads_row, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+    k_col<R, MODE_FWD><<<hs.nt_col, w.tiles.threads_col, w.tiles.smem_col, s>>>(w.d_plain, p->items);
   } else {
-    k_row_fwd<R, MAXE, MODE_PLAIN><<<nt_in, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
-    k_col<R, MAXE, MODE_PLAIN><<<hs.nt_col, CM_THREADS, w.tiles.smem_col, s>>>(w.d_plain, p->items);
-    k_row_inv<R, MAXE, MODE_PLAIN><<<nt_out, CM_THREADS, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+    k_row_fwd<R, MODE_PLAIN><<<nt_in, w.tiles.threads_row, w.tiles.smem_row, s>>>(w.d_plain, p->items);
+    k_col<R, MODE_PLAIN><<<hs.nt_col, w.tiles.threads_col, w.tiles.smem_col, s>>>(w.d_plain, p->items);
+    k_row_inv<R, MODE_PLAIN><<<nt_out, w.tiles.threads_row, w.tiles.smem_row, s>>>(w.d_plain, p->items);
   }
   CK(cudaGetLastError());
   return CM_OK;
@@ -548,34 +576,59 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
 static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int in_rows, int in_cols,
                           int in_ld, void* out, int out_rows, int out_cols, int out_ld, cudaStream_t s) {
   if (precision == CM_FP64)
-    return launch_plain<double, CM_MAXE64>(p, p->w64, MODE_PLAIN, op, (const double*)in, in_rows, in_cols,
+    return launch_plain<double>(p, p->w64, MODE_PLAIN, op, (const double*)in, in_rows, in_cols,
                                            in_ld, (double*)out, out_rows, out_cols, out_ld, s);
-  return launch_plain<float, CM_MAXE32>(p, p->w32, MODE_PLAIN, op, (const float*)in, in_rows, in_cols,
+  return launch_plain<float>(p, p->w32, MODE_PLAIN, op, (const float*)in, in_rows, in_cols,
                                         in_ld, (float*)out, out_rows, out_cols, out_ld, s);
 }
 
 // ---------------------------------------------------------------------------
 // solver driver
 // ---------------------------------------------------------------------------
-template <typename R, int MAXE>
-static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s) {
+// kernels of one iteration, in launch order (bisection passes excluded)
+#define CM_ITER_KERNELS 10
+static const char* const k_iter_names[CM_ITER_KERNELS] = {
+    "k_ccg_begin", "k_ccg_gsum", "k_row_fwd<T>", "k_col<T>", "k_row_inv<T>",
+    "k_ccg_update", "k_row_fwd<F>", "k_col<F>", "k_row_inv<F>", "k_ccg_bisect"};
+
+static int iteration_launches(bool bisect) {
+  return CM_ITER_KERNELS - 1 + (bisect ? CM_BISECT_PASSES : 0);
+}
+
+// One CCG iteration.  With `ev` (CM_ITER_KERNELS + 1 events) an event is
+// recorded before the first and after every kernel, for the profiler.
+template <typename R>
+static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s,
+                             cudaEvent_t* ev = nullptr) {
   const Slot<R>* S = w.d_ccg;
   const int2* it = p->items;
   const Tiles& T = w.tiles;
+  int k = 0;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], s); };
+  mark();
   k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
   if (bisect)
     for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  mark();
   k_ccg_gsum<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
-  k_row_fwd<R, MAXE, MODE_T><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
-  k_col<R, MAXE, MODE_T><<<w.nt_col, CM_THREADS, T.smem_col, s>>>(S, it);
-  k_row_inv<R, MAXE, MODE_T><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
+  mark();
+  k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  mark();
+  k_col<R, MODE_T><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  mark();
+  k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  mark();
   k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
-  k_row_fwd<R, MAXE, MODE_F><<<w.nt_rowt, CM_THREADS, T.smem_row, s>>>(S, it);
-  k_col<R, MAXE, MODE_F><<<w.nt_col, CM_THREADS, T.smem_col, s>>>(S, it);
-  k_row_inv<R, MAXE, MODE_F><<<w.nt_rowd, CM_THREADS, T.smem_row, s>>>(S, it);
+  mark();
+  k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  mark();
+  k_col<R, MODE_F><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  mark();
+  k_row_inv<R, MODE_F><<<w.nt_rowd, T.threads_row, T.smem_row, s>>>(S, it);
+  mark();
 }
 
-template <typename R, int MAXE>
+template <typename R>
 static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphExec_t* out) {
   const int gi = bisect ? 1 : 0;
   if (w.graph[gi] && w.graph_iters[gi] == iters) {
@@ -588,7 +641,7 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
   }
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed));
-  for (int i = 0; i < iters; ++i) launch_iteration<R, MAXE>(p, w, bisect, p->stream);
+  for (int i = 0; i < iters; ++i) launch_iteration<R>(p, w, bisect, p->stream);
   cudaError_t e = cudaStreamEndCapture(p->stream, &g);
   CK(e);
   e = cudaGraphInstantiate(&w.graph[gi], g, 0);
@@ -606,11 +659,12 @@ struct SolveInput {
   int f0_ld;
 };
 
-template <typename R, int MAXE>
+template <typename R>
 static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
-                   double rel_pentol, int maxiter, CcgState* fin) {
+                   double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
+                   int prof_iters = 0, float* prof_ms = nullptr) {
   cudaStream_t s = p->stream;
-  set_smem_attrs<R, MAXE>();
+  set_smem_attrs<R>();
   CKS(ensure_ccg(p, w));
   CcgState st;
   memset(&st, 0, sizeof(st));
@@ -624,6 +678,7 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   P.thermotol = prm->thermotol;
   P.mixfac = prm->mixfac;
   P.mixdecfac = prm->mixdecfac;
+  P.rel_forcetol = rel_forcetol;
   P.minmixsteps = prm->minmixsteps;
   P.maxiter = maxiter;
   P.load_control = prm->load_control;
@@ -636,31 +691,53 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   st.nfev = 1;
   st.scale = 1.0;
   CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+  g_launches += 3;  // heights statistics (2) and the initial field
   k_h_prep<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64);
   k_h_var<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64, prm->pentol <= 0, rel_pentol);
   Slot<R> hs = base_slot(p, w);
   const int gd = grid_for((long)p->nx * p->ny);
   if (in.f0) {
     k_init_f<R><<<gd, 256, 0, s>>>(hs, in.f0, in.f0_ld);
-    CKS(launch_plain<R, MAXE>(p, w, MODE_PLAIN, CM_OP_DISP, w.f[0], p->tx, p->ty, p->ty, w.u, p->nx,
+    CKS(launch_plain<R>(p, w, MODE_PLAIN, CM_OP_DISP, w.f[0], p->tx, p->ty, p->ty, w.u, p->nx,
                               p->ny, p->ny, s));
   } else {
     k_init_u<R><<<gd, 256, 0, s>>>(hs, in.u0, P.offset0);
-    CKS(launch_plain<R, MAXE>(p, w, MODE_PLAIN, CM_OP_FORCE, w.u, p->nx, p->ny, p->ny, w.f[0], p->tx,
+    CKS(launch_plain<R>(p, w, MODE_PLAIN, CM_OP_FORCE, w.u, p->nx, p->ny, p->ny, w.f[0], p->tx,
                               p->ty, p->ty, s));
   }
   CK(cudaGetLastError());
   const bool bisect = prm->has_hardness && prm->load_control;
+  if (prof_iters > 0) {
+    // profiler: eager launches with an event between kernels
+    std::vector<cudaEvent_t> ev(CM_ITER_KERNELS + 1);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int k = 0; k < CM_ITER_KERNELS; ++k) prof_ms[k] = 0;
+    for (int i = 0; i < prof_iters; ++i) {
+      launch_iteration<R>(p, w, bisect, s, ev.data());
+      CK(cudaEventSynchronize(ev[CM_ITER_KERNELS - 1]));
+      for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        prof_ms[k] += ms / prof_iters;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *fin = *p->h_state;
+    return CM_OK;
+  }
   int every = prm->check_every;
   if (every <= 0) {
     const long work = (long)p->nx * p->ny;
     every = work >= (1L << 20) ? 4 : (work >= (1L << 16) ? 8 : 16);
   }
   cudaGraphExec_t g;
-  CKS(get_graph<R, MAXE>(p, w, bisect, every, &g));
+  CKS(get_graph<R>(p, w, bisect, every, &g));
   auto t0 = std::chrono::steady_clock::now();
   for (int done_iters = 0;; done_iters += every) {
     CK(cudaGraphLaunch(g, s));
+    g_launches += (unsigned long long)every * iteration_launches(bisect);
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (p->h_state->done) break;
@@ -682,7 +759,11 @@ static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned c
                       unsigned char* plastic, CcgState* fin) {
   cudaStream_t s = p->stream;
   k_ccg_result<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, jac, active, plastic);
-  if (x) k_to_f64<R><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(w.u, x, (long)p->nx * p->ny);
+  g_launches += 1;
+  if (x) {
+    k_to_f64<R><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(w.u, x, (long)p->nx * p->ny);
+    g_launches += 1;
+  }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -770,8 +851,8 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
     p->h_state = nullptr;
     return fail(CM_ERR_OOM);
   }
-  if ((rc = init_work<double>(p, p->w64, CM_MAXE64)) != CM_OK) return fail(rc);
-  if ((rc = init_work<float>(p, p->w32, CM_MAXE32)) != CM_OK) return fail(rc);
+  if ((rc = init_work<double>(p, p->w64)) != CM_OK) return fail(rc);
+  if ((rc = init_work<float>(p, p->w32)) != CM_OK) return fail(rc);
   // work items (0, i): every launch on this plan covers tiles 0..n-1 of slot 0
   {
     std::vector<int2> it(p->max_items);
@@ -781,10 +862,14 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
       return fail(CM_ERR_CUDA);
   }
   const long nh = (long)p->nx * p->nyh;
+  const long nh64 = (long)p->nx * p->w64.tiles.ntile_cols * p->w64.tiles.col_tile;
+  const long nh32 = (long)p->nx * p->w32.tiles.ntile_cols * p->w32.tiles.col_tile;
   if ((rc = dalloc(p, &p->G, nh)) != CM_OK) return fail(rc);
   for (int i = 0; i < 2; ++i) {
-    if ((rc = dalloc(p, &p->tab64[i], nh)) != CM_OK) return fail(rc);
-    if ((rc = dalloc(p, &p->tab32[i], nh)) != CM_OK) return fail(rc);
+    if ((rc = dalloc(p, &p->tab64[i], nh64)) != CM_OK) return fail(rc);
+    if ((rc = dalloc(p, &p->tab32[i], nh32)) != CM_OK) return fail(rc);
+    cudaMemset(p->tab64[i], 0, nh64 * sizeof(double));
+    cudaMemset(p->tab32[i], 0, nh32 * sizeof(float));
   }
   p->w64.tab[0] = p->tab64[0];
   p->w64.tab[1] = p->tab64[1];
@@ -801,15 +886,16 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
     if ((rc = dalloc(p, &love, (long)p->nx * p->ny)) != CM_OK) return fail(rc);
     k_love<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, p->tx, p->ty, p->nx, p->ny,
                                                           desc->sx / p->tx, desc->sy / p->ty, desc->young);
-    rc = launch_plain<double, CM_MAXE64>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
+    rc = launch_plain<double>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
                                          0, 0, s);
     if (rc != CM_OK) return fail(rc);
-    k_real_part<<<grid_for(nh), 256, 0, s>>>(p->w64.spec, p->G, nh);
+    k_real_part<<<grid_for(nh), 256, 0, s>>>(p->w64.spec, p->G, p->nx, p->nyh, p->w64.tiles.lw);
   }
   const double area = (desc->sx / p->tx) * (desc->sy / p->ty);
   const double N = (double)p->nx * (double)p->ny;
-  k_tables_scale<<<grid_for(nh), 256, 0, s>>>(p->G, nh, 1.0 / (area * N), area / N, p->tab64[0],
-                                               p->tab64[1], p->tab32[0], p->tab32[1]);
+  k_tables_scale<<<grid_for(nh), 256, 0, s>>>(p->G, p->nx, p->nyh, 1.0 / (area * N), area / N,
+                                               p->tab64[0], p->tab64[1], p->w64.tiles.lw, p->tab32[0],
+                                               p->tab32[1], p->w32.tiles.lw);
   if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
     return fail(CM_ERR_CUDA);
   *out = p;
@@ -868,13 +954,17 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   SolveInput in{h, u0, f0, p->ny};
   CcgState fin;
   if (prm->precision == CM_FP64) {
-    CKS(run_ccg<double, CM_MAXE64>(p, p->w64, prm, in, 0.0, prm->maxiter, &fin));
+    CKS(run_ccg<double>(p, p->w64, prm, in, 0.0, 0.0, prm->maxiter, &fin));
     CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
     fill_result(fin, res);
     return CM_OK;
   }
   const double rp = prm->precision == CM_MIXED ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
-  CKS(run_ccg<float, CM_MAXE32>(p, p->w32, prm, in, rp, prm->maxiter, &fin));
+  const double rf = prm->precision == CM_MIXED ? 1e-5 : 0.0;
+  // FP32 phase: tolerances widened to FP32 resolution; a phase that cannot
+  // reach them within its iteration cap hands over to the FP64 refinement
+  const int cap32 = prm->precision == CM_MIXED ? std::min(prm->maxiter, CM_FP32_ITER_CAP) : prm->maxiter;
+  CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin));
   if (prm->precision == CM_FP32) {
     CKS(finish_ccg<float>(p, p->w32, x, jac, active, plastic, &fin));
     fill_result(fin, res);
@@ -896,13 +986,32 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   // k_init_f reads f64 before the operator overwrites u, so the borrow is safe
   SolveInput in2{h, nullptr, f64, p->ny};
   const int rem = std::max(1, prm->maxiter - nit32);
-  CKS(run_ccg<double, CM_MAXE64>(p, p->w64, prm, in2, 0.0, rem, &fin));
+  CKS(run_ccg<double>(p, p->w64, prm, in2, 0.0, 0.0, rem, &fin));
   CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
   fill_result(fin, res);
   res->nit += nit32;
   res->nfev += nfev32;
   res->nit_fp32 = nit32;
   return CM_OK;
+}
+
+unsigned long long cm_launch_count(void) { return g_launches; }
+
+int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int iters,
+                   float* ms_per_kernel, int* n_kernels, const char** names) {
+  if (!p || !prm || !h || iters < 1 || !ms_per_kernel) return CM_ERR_ARG;
+  SolveInput in{h, nullptr, nullptr, p->ny};
+  CcgState fin;
+  cm_ccg_params q = *prm;
+  q.maxiter = std::max(prm->maxiter, iters + 1);
+  if (prm->precision == CM_FP64)
+    CKS(run_ccg<double>(p, p->w64, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
+  else
+    CKS(run_ccg<float>(p, p->w32, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
+  if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
+  if (names)
+    for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) names[k] = k_iter_names[k];
+  return fin.done && fin.it < iters ? CM_ERR_ARG : CM_OK;
 }
 
 int cm_ccg_solve_host(cm_plan* p, const cm_ccg_params* prm, const double* h, const double* u0,

@@ -26,6 +26,7 @@ struct CcgParams {
   double offset0;    // rigid-body offset (offset control)
   double H;          // hardness in force units
   double pentol, forcetol, thermotol, mixfac, mixdecfac;
+  double rel_forcetol;  // FP32 phases: forcetol >= rel_forcetol * max|f|
   double n_surface;  // number of topography points
   double max_surface;
   int load_control;
@@ -53,7 +54,7 @@ struct CcgState {
   double G_old, G, beta, tau, offset, cur_mixfac, scale;
   double last_tf, last_mh;
   double sum_cg, sum_cgt, gmax, gmin;
-  double max_pres, pad_pres, total_force, maxdu, max_pen, rms_pen;
+  double max_pres, pad_pres, total_force, maxdu, max_pen, rms_pen, fmax;
   // scipy-compatible bisection state (offset of the mixing step)
   double bs_xa, bs_dm, bs_fa;
   double bs_cand[CM_BIS_CAND + 1];
@@ -64,7 +65,8 @@ struct Slot {
   typedef typename CT<R>::C C;
   // geometry: domain (nx, ny), half spectrum (nx, nyh), topography (tx, ty)
   int nx, ny, nyh, tx, ty;
-  int row_tile, col_tile, comp_rows;       // tile shapes
+  int row_tile, col_tile, comp_rows;       // tile shapes (col_tile = 2^lw)
+  int lw;                                  // log2 of the spectrum column-tile width
   int nt_comp, nt_rowt, nt_rowd, nt_col;   // tiles over comp rows, rows<tx, rows<nx, columns
   FftDesc fx, fy;
   const C* twx;

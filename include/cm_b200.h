@@ -177,6 +177,24 @@ int cm_ccg_solve_host(cm_plan* plan, const cm_ccg_params* params, const double* 
                       double* x_host, double* jac_host, unsigned char* active_host,
                       unsigned char* plastic_host, cm_ccg_result* res);
 
+/*
+ * Number of kernels this library has launched in the process (graph nodes
+ * count once per replay).  Instrumentation; no reference counterpart.
+ */
+unsigned long long cm_launch_count(void);
+
+/*
+ * Per-kernel timing of the solver's iteration: initialises a solve like
+ * cm_ccg_solve (precision CM_FP64 or CM_FP32) and runs `iters` iterations
+ * eagerly with a CUDA event between kernels on the plan's stream.  Writes
+ * the average milliseconds of each of the *n_kernels kernels (launch order)
+ * to ms_per_kernel (capacity >= 16) and, if names is not NULL, their names.
+ * Returns CM_ERR_ARG if the solve stopped before `iters` iterations.
+ * Instrumentation; no reference counterpart.
+ */
+int cm_ccg_profile(cm_plan* plan, const cm_ccg_params* params, const double* heights_dev,
+                   int iters, float* ms_per_kernel, int* n_kernels, const char** names);
+
 #ifdef __cplusplus
 }
 #endif
