@@ -178,6 +178,7 @@ def run_gpu(args, rank, world, local_rank):
     import torch
     import contactmechanics_b200 as cm
     from contactmechanics_b200 import _lib
+    from contactmechanics_b200.replicas import max_over_ranks
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -226,11 +227,7 @@ def run_gpu(args, rank, world, local_rank):
             res = sweep(precision, host=host, lat=lat)
         e1.record()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dist=dist, device="cuda")
         return ms, res
 
     for _ in range(args.warmup):
@@ -311,7 +308,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", choices=["mixed", "fp64", "fp32"], default=None,
+                    help="run the first solve of the sweep once and exit (for profilers)")
     args = ap.parse_args()
+    if args.profile_solve:
+        import torch
+        import contactmechanics_b200 as cm
+        h = surface()
+        sub = cm.FreeFFTElasticHalfSpace((N_TOPO, N_TOPO), 1.0, (1.0, 1.0))
+        F = float(PRESSURES[0])
+        r = cm.constrained_conjugate_gradients(sub, torch.from_numpy(h).cuda(), external_force=F,
+                                               precision=args.profile_solve, **tolerances(h, F))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_solve": args.profile_solve, "nit": r.nit, "success": bool(r.success)}))
+        return 0
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
