@@ -302,6 +302,47 @@ k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   }
 }
 
+// Convergence test at the end of an iteration (ConstrainedConjugateGradients.py
+// :391-434, 491-492); run by the last tile of the displacement update.
+CM_DEVINL void ccg_converge(CcgState& s, double maxdu_in, double maxpen_in) {
+  // convergence test (ConstrainedConjugateGradients.py:391-434, 491-492)
+  const CcgParams& P = s.p;
+  s.maxdu = maxdu_in;
+  s.nfev += (s.branch == 0) ? 2 : 1;
+  s.G_old = s.G;
+  s.rms_pen = (s.A_cg > 0) ? sqrt(s.G / (double)s.A_cg) : sqrt(s.G);
+  s.max_pen = fmax(0.0, maxpen_in);
+  const double tf = s.total_force;
+  bool conv = true;
+  if (P.load_control) conv = conv && fabs((tf - P.F) / tf) < P.thermotol;
+  else if (s.have_last_tf) conv = conv && fabs((tf - s.last_tf) / tf) < P.thermotol;
+  s.last_tf = tf;
+  s.have_last_tf = 1;
+  const double mh = P.max_surface + s.offset;
+  if (P.load_control && s.have_last_mh) conv = conv && fabs((mh - s.last_mh) / mh) < P.thermotol;
+  s.last_mh = mh;
+  s.have_last_mh = 1;
+  const double ftol = fmax(P.forcetol, P.rel_forcetol * s.fmax);
+  if (s.mode == CMM_MIX)
+    conv = conv && s.maxdu < P.pentol && s.max_pres < ftol && s.pad_pres < ftol;
+  else
+    conv = conv && s.rms_pen < P.pentol && s.max_pen < P.pentol && s.maxdu < P.pentol &&
+           s.max_pres < ftol && s.pad_pres < ftol;
+  s.parity ^= 1;
+  if (conv) {
+    s.status = CMS_CONVERGED;
+    s.done = 1;
+  } else if (isnan(s.G) || isnan(s.rms_pen)) {
+    s.status = CMS_NAN;
+    s.done = 1;
+  } else if (s.it >= P.maxiter) {
+    s.status = CMS_MAXITER;
+    s.done = 1;
+  } else {
+    s.it += 1;
+  }
+}
+
 template <typename R, int MODE>
 __global__ void __launch_bounds__(CM_FFT_THREADS)
 k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
@@ -435,45 +476,8 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   } else if (MODE == MODE_F) {
     double v[2] = {a0, a1};
     const int kinds[2] = {RED_MAX, RED_MAX};
-    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowd, v, kinds, [&](double (&a)[2]) {
-      // convergence test (ConstrainedConjugateGradients.py:391-434, 491-492)
-      CcgState& s = *st;
-      const CcgParams& P = s.p;
-      s.maxdu = a[0];
-      s.nfev += (s.branch == 0) ? 2 : 1;
-      s.G_old = s.G;
-      s.rms_pen = (s.A_cg > 0) ? sqrt(s.G / (double)s.A_cg) : sqrt(s.G);
-      s.max_pen = fmax(0.0, a[1]);
-      const double tf = s.total_force;
-      bool conv = true;
-      if (P.load_control) conv = conv && fabs((tf - P.F) / tf) < P.thermotol;
-      else if (s.have_last_tf) conv = conv && fabs((tf - s.last_tf) / tf) < P.thermotol;
-      s.last_tf = tf;
-      s.have_last_tf = 1;
-      const double mh = P.max_surface + s.offset;
-      if (P.load_control && s.have_last_mh) conv = conv && fabs((mh - s.last_mh) / mh) < P.thermotol;
-      s.last_mh = mh;
-      s.have_last_mh = 1;
-      const double ftol = fmax(P.forcetol, P.rel_forcetol * s.fmax);
-      if (s.mode == CMM_MIX)
-        conv = conv && s.maxdu < P.pentol && s.max_pres < ftol && s.pad_pres < ftol;
-      else
-        conv = conv && s.rms_pen < P.pentol && s.max_pen < P.pentol && s.maxdu < P.pentol &&
-               s.max_pres < ftol && s.pad_pres < ftol;
-      s.parity ^= 1;
-      if (conv) {
-        s.status = CMS_CONVERGED;
-        s.done = 1;
-      } else if (isnan(s.G) || isnan(s.rms_pen)) {
-        s.status = CMS_NAN;
-        s.done = 1;
-      } else if (s.it >= P.maxiter) {
-        s.status = CMS_MAXITER;
-        s.done = 1;
-      } else {
-        s.it += 1;
-      }
-    });
+    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowd, v, kinds,
+                   [&](double (&a)[2]) { ccg_converge(*st, a[0], a[1]); });
   }
 }
 

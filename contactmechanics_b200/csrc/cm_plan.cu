@@ -12,6 +12,7 @@
 
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
+#include "cm_kernels_p2.cuh"
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
 #define CM_SMEM_COL_MAX (160 * 1024)
@@ -86,6 +87,8 @@ static std::vector<C> make_twiddles(int n) {
 struct Tiles {
   int row_tile, col_tile, lw, comp_rows;
   int threads_row, threads_col;
+  bool p2;                          // both sides 2^6..2^12: specialised transforms
+  int p2_threads_row, p2_threads_col;
   size_t smem_row, smem_col;
   int ntile_cols;  // number of spectrum column tiles
 };
@@ -119,6 +122,12 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   t->threads_col = pow2_threads(((size_t)1 << lw) * nx);
   t->ntile_cols = (nyh + t->col_tile - 1) / t->col_tile;
   t->comp_rows = std::max(1, std::min(tx, CM_COMP_ELEMS / std::max(1, ty)));
+  // register-resident power-of-two transforms: one thread per 8 elements
+  t->p2_threads_row = np * (ny / 8);
+  t->p2_threads_col = (1 << lw) * (nx / 8);
+  auto is_p2 = [](int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; };
+  t->p2 = is_p2(nx) && is_p2(ny) && t->p2_threads_row >= 32 && t->p2_threads_row <= CM_FFT_THREADS &&
+          t->p2_threads_col >= 32 && t->p2_threads_col <= CM_FFT_THREADS;
   return CM_OK;
 }
 
@@ -434,10 +443,14 @@ static int grid_for(long n) {
 }
 
 template <typename R>
+static void set_p2_attrs();
+
+template <typename R>
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
   done = true;
+  set_p2_attrs<R>();
   const int mx = 200 * 1024;
   const int carve = cudaSharedmemCarveoutMaxShared;
   cudaFuncSetAttribute(k_row_fwd<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
@@ -585,6 +598,70 @@ static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int
 // ---------------------------------------------------------------------------
 // solver driver
 // ---------------------------------------------------------------------------
+// ---- power-of-two specialisations -------------------------------------------
+static int log2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return (1 << l) == n ? l : -1;
+}
+
+#define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+
+template <typename R, int MODE>
+static bool p2_row_fwd(int logn, int grid, int threads, size_t smem, cudaStream_t s,
+                       const Slot<R>* S, const int2* it) {
+  switch (logn) {
+#define CM_CASE(L) case L: k_row_fwd_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return false;
+  }
+}
+
+template <typename R, int MODE>
+static bool p2_col(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
+                   const int2* it) {
+  switch (logn) {
+#define CM_CASE(L) case L: k_col_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return false;
+  }
+}
+
+template <typename R, int MODE>
+static bool p2_row_inv(int logn, int grid, int threads, size_t smem, cudaStream_t s,
+                       const Slot<R>* S, const int2* it) {
+  switch (logn) {
+#define CM_CASE(L) case L: k_row_inv_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return false;
+  }
+}
+
+template <typename R>
+static void set_p2_attrs() {
+  static bool done = false;
+  if (done) return;
+  done = true;
+  const int mx = 200 * 1024;
+  const int carve = cudaSharedmemCarveoutMaxShared;
+#define CM_ATTR(K)                                                                  \
+  cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);         \
+  cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+#define CM_CASE(L)                           \
+  CM_ATTR((k_row_fwd_p2<R, MODE_T, L>))      \
+  CM_ATTR((k_row_fwd_p2<R, MODE_F, L>))      \
+  CM_ATTR((k_col_p2<R, MODE_T, L>))          \
+  CM_ATTR((k_col_p2<R, MODE_F, L>))          \
+  CM_ATTR((k_row_inv_p2<R, MODE_T, L>))      \
+  CM_ATTR((k_row_inv_p2<R, MODE_F, L>))
+  CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+#undef CM_ATTR
+}
+
 // kernels of one iteration, in launch order (bisection passes excluded)
 #define CM_ITER_KERNELS 10
 static const char* const k_iter_names[CM_ITER_KERNELS] = {
@@ -612,19 +689,28 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   mark();
   k_ccg_gsum<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
   mark();
-  k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  const bool p2 = T.p2;
+  const int ly = p->fy.n, lx = p->fx.n;
+  const int ry = log2_exact(ly), rx = log2_exact(lx);
+  if (!(p2 && p2_row_fwd<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
+    k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
-  k_col<R, MODE_T><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  if (!(p2 && p2_col<R, MODE_T>(rx, w.nt_col, T.p2_threads_col, T.smem_col, s, S, it)))
+    k_col<R, MODE_T><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
   mark();
-  k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  if (!(p2 && p2_row_inv<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
+    k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
   k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
   mark();
-  k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  if (!(p2 && p2_row_fwd<R, MODE_F>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
+    k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
-  k_col<R, MODE_F><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  if (!(p2 && p2_col<R, MODE_F>(rx, w.nt_col, T.p2_threads_col, T.smem_col, s, S, it)))
+    k_col<R, MODE_F><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
   mark();
-  k_row_inv<R, MODE_F><<<w.nt_rowd, T.threads_row, T.smem_row, s>>>(S, it);
+  if (!(p2 && p2_row_inv<R, MODE_F>(ry, w.nt_rowd, T.p2_threads_row, T.smem_row, s, S, it)))
+    k_row_inv<R, MODE_F><<<w.nt_rowd, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
 }
 

@@ -165,3 +165,56 @@ def test_solve_mixed_vs_reference(cm, golden, name):
     a = np.count_nonzero(res.jac > 0)
     a_ref = np.count_nonzero(golden[f"ccg_{name}_jac"] > 0)
     assert abs(a - a_ref) <= 1e-3 * a_ref
+
+
+P2_CASES = [
+    # (kind, nb, hardness(pressure) or None, load F or None, offset or None)
+    ("periodic", (64, 64), None, 2e-3, None),
+    ("periodic", (128, 256), None, 5e-3, None),
+    ("free", (64, 64), None, None, 0.02),
+    ("free", (32, 64), None, 1e-3, None),
+    ("periodic", (64, 64), 0.05, 4e-3, None),
+]
+
+
+def _oracle_case(kind, nb, hardness, F, offset, seed=21):
+    sizes = (1.0, 1.0)
+    if kind == "free":
+        h = oc.sphere(nb, sizes, 2.0)
+        o = oc.FreeSubstrate(nb, 1.0, sizes)
+    else:
+        h = oc.self_affine(nb, sizes, 0.7, 0.2 if hardness else 0.1, seed=seed)
+        o = oc.PeriodicSubstrate(nb, 1.0, sizes)
+    kw = dict(pentol=1e-11 * (h.max() - h.min()), forcetol=1e-13, maxiter=5000)
+    if F is not None:
+        kw["external_force"] = F
+    if offset is not None:
+        kw["offset"] = offset
+    if hardness is not None:
+        kw["hardness"] = hardness * o.area_per_pt
+        kw["forcetol"] = 1e-10
+    return h, o, kw
+
+
+@pytest.mark.parametrize("case", P2_CASES, ids=lambda c: f"{c[0]}{c[1][0]}x{c[1][1]}{'_plastic' if c[2] else ''}")
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_pow2_transforms_vs_oracle(cm, case, precision):
+    """Sizes 64..256 run the register-resident power-of-two transforms."""
+    kind, nb, hardness, F, offset = case
+    h, o, kw = _oracle_case(*case)
+    ref = oc.constrained_conjugate_gradients(o, h, **kw)
+    if kind == "free":
+        s = cm.FreeFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0))
+    else:
+        s = cm.PeriodicFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0))
+    res = cm.constrained_conjugate_gradients(s, h, precision=precision, **kw)
+    assert res.success and ref["success"]
+    x, xr = res.x[:nb[0], :nb[1]], ref["x"][:nb[0], :nb[1]]
+    rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
+    tol = 1e-10 if precision == "fp64" else 1e-6
+    assert rel < tol, rel
+    if precision == "fp64":
+        np.testing.assert_array_equal(res.active_set, ref["active_set"])
+        np.testing.assert_allclose(res.offset, ref["offset"], rtol=1e-9)
+    a, ar = np.count_nonzero(res.jac > 0), np.count_nonzero(ref["jac"] > 0)
+    assert abs(a - ar) <= max(1, 1e-3 * ar)
