@@ -145,6 +145,8 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
     result.offset = res.offset
     result.fun = res.fun
     result.pentol = res.pentol_used
+    result.timing = {"ms_fp32": res.ms_fp32, "ms_fp64": res.ms_fp64, "ms_total": res.ms_total,
+                     "polls": res.polls}
 
     # active set over the full domain (False on the padding)
     act_dom = torch.zeros(dshape, dtype=torch.bool, device="cuda")

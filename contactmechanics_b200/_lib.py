@@ -67,7 +67,9 @@ class CcgResult(ctypes.Structure):
                 ("maxdu", ctypes.c_double), ("total_force", ctypes.c_double),
                 ("pentol_used", ctypes.c_double),
                 ("area", ctypes.c_longlong), ("cg_area", ctypes.c_longlong),
-                ("plastic_area", ctypes.c_longlong)]
+                ("plastic_area", ctypes.c_longlong), ("ms_fp32", ctypes.c_double),
+                ("ms_fp64", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("polls", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p

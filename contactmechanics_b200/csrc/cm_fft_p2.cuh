@@ -26,6 +26,13 @@ struct P2Plan {
   static constexpr int NST = 1 + (LOGN - (LOGN % 3 == 0 ? 3 : LOGN % 3)) / 3;
 };
 
+// Shared-memory index with one padding slot per 8 elements: the strided
+// Stockham writes (stride 4 or 8 elements across a warp) and the column
+// layouts then hit distinct banks.  A buffer of E elements needs
+// smem_padded(E) slots.
+CM_DEVINL int spad(int e) { return e + (e >> 3); }
+__host__ __device__ inline int smem_padded(int e) { return e + (e >> 3) + 1; }
+
 template <bool INV, int R, typename C>
 CM_DEVINL void dft_r(C* v) {
   if (R == 8) Dft<INV, 8, C>::run(*reinterpret_cast<C(*)[8]>(v), nullptr, 8);
@@ -38,12 +45,12 @@ CM_DEVINL void dft_r(C* v) {
 }
 
 // Transform the thread's 8 elements in place.  Sequence layout in shared
-// memory: element i at base[i * estride]; sA / sB are the two ping-pong
-// buffers (same base offset for this thread's sequence); tw: twiddle table
-// exp(-2 pi i m / N) in shared memory.  Ends with the result in v and no
-// pending shared-memory reads (a barrier is needed before reusing sA/sB).
+// memory: element i of this thread's sequence at buf[spad(base + i*estride)];
+// sA / sB are the two ping-pong buffers; tw: twiddle table exp(-2 pi i m / N)
+// in shared memory.  Ends with the result in v and no pending shared-memory
+// reads (a barrier is needed before reusing sA/sB).
 template <typename C, bool INV, int LOGN>
-CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int estride, int tt, const C* tw) {
+CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int base, int estride, int tt, const C* tw) {
   typedef P2Plan<LOGN> P;
   constexpr int N = P::N;
   // ---- first stage (Ns = 1): radix FIRST, 8/FIRST butterflies per thread
@@ -70,7 +77,7 @@ CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int estride, int tt, const C* tw)
     for (int i = 0; i < B; ++i) {
       const int j = tt + i * P::TPS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) sA[(j * R + q) * estride] = o[i * R + q];
+      for (int q = 0; q < R; ++q) sA[spad(base + (j * R + q) * estride)] = o[i * R + q];
     }
   }
   __syncthreads();
@@ -83,7 +90,7 @@ CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int estride, int tt, const C* tw)
     const int k = tt & (Ns - 1);
     C g[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) g[q] = src[(tt + q * P::TPS) * estride];
+    for (int q = 0; q < 8; ++q) g[q] = src[spad(base + (tt + q * P::TPS) * estride)];
     const int step = N / (Ns * 8);
 #pragma unroll
     for (int q = 1; q < 8; ++q) {
@@ -98,7 +105,7 @@ CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int estride, int tt, const C* tw)
     } else {
       const int ob = (tt - k) * 8 + k;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) dst[(ob + q * Ns) * estride] = g[q];
+      for (int q = 0; q < 8; ++q) dst[spad(base + (ob + q * Ns) * estride)] = g[q];
       __syncthreads();
       C* t = src;
       src = dst;

@@ -103,6 +103,163 @@ CM_DEVINL void load_view(const CcgState* st, CcgView& v) {
 }
 
 // ---------------------------------------------------------------------------
+// scalar steps between the field passes (shared by every execution path)
+// ---------------------------------------------------------------------------
+// Step kind and offset (ConstrainedConjugateGradients.py:239-270, 300-318).
+CM_DEVINL void fin_begin(CcgState& s, double (&a)[5]) {
+  const CcgParams& P = s.p;
+  s.A_contact = (long long)a[0];
+  s.A_cg = (long long)a[1];
+  s.sum_cg = a[2];
+  s.gmax = a[3];
+  s.gmin = a[4];
+  const bool cg = !P.has_h || (s.A_contact > 0 && (double)s.A_cg / (double)s.A_contact > 0.01 &&
+                               s.mixsteps <= 0);
+  s.bs_active = 0;
+  if (cg) {
+    s.branch = 0;
+    if (s.mode == CMM_MIX) s.mode = CMM_SD;
+    if (P.load_control) s.offset = (s.A_cg > 0) ? s.sum_cg / (double)s.A_cg : 0.0;
+  } else {
+    s.branch = 1;
+    if (s.mode != CMM_MIX) {
+      s.mixsteps = P.minmixsteps;
+      s.mode = CMM_MIX;
+    }
+    if (P.load_control) {
+      // scipy.optimize.bisect(f, a=max g, b=min g); first pass evaluates f(a)
+      s.bs_active = 1;
+      s.bs_iter = -1;
+      s.bs_xa = s.gmax;
+      s.bs_dm = s.gmin - s.gmax;
+      s.bs_cand[0] = s.gmax;
+    }
+  }
+
+}
+
+// G and the conjugation factor (:273-279).
+CM_DEVINL void fin_gsum(CcgState& s, double (&a)[1]) {
+  s.G = a[0];
+  s.beta = (s.delta > 0 && s.G_old > 0) ? (double)s.delta * (s.G / s.G_old) : 0.0;
+
+}
+
+// Replays five levels of scipy's bisection on the counts of one pass (:316-318).
+CM_DEVINL void fin_bisect(CcgState& s, double (&a)[CM_BIS_CAND]) {
+  const double H = s.p.H, F = s.p.F;
+  const double xtol = 2e-12, rtol = 8.881784197001252e-16;
+  const int maxit = 100;
+  if (s.bs_iter < 0) {
+    const double fa = a[0] * H - F;
+    const double fb = 0.0 * H - F;  // nothing lies below min g
+    s.bs_fa = fa;
+    if (fa * fb > 0) {
+      s.status = CMS_BISECT_SIGN;
+      s.done = 1;
+      s.bs_active = 0;
+      return;
+    }
+    if (fa == 0) { s.offset = s.bs_xa; s.bs_active = 0; return; }
+    if (fb == 0) { s.offset = s.gmin; s.bs_active = 0; return; }
+    s.bs_iter = 0;
+  } else {
+    int node = 1;
+    double xa = s.bs_xa, dm = s.bs_dm;
+    for (int lev = 0; lev < 5; ++lev) {
+      dm *= 0.5;
+      const double xm = xa + dm;
+      const double fm = a[node - 1] * H - F;
+      s.bs_iter += 1;
+      if (fm * s.bs_fa >= 0) { xa = xm; node = 2 * node + 1; }
+      else node = 2 * node;
+      if (fm == 0 || fabs(dm) < xtol + rtol * fabs(xm)) {
+        s.offset = xm;
+        s.bs_active = 0;
+        return;
+      }
+      if (s.bs_iter >= maxit) {
+        s.status = CMS_BISECT_SIGN + 1;  // bisection did not converge
+        s.done = 1;
+        s.bs_active = 0;
+        return;
+      }
+    }
+    s.bs_xa = xa;
+    s.bs_dm = dm;
+  }
+  // candidate midpoints of the next five levels, heap-indexed from 1
+  double xa_n[CM_BIS_CAND + 1], xm_n[CM_BIS_CAND + 1];
+  double dml = s.bs_dm;
+  int lev_start = 1;
+  for (int lev = 0; lev < 5; ++lev) {
+    dml *= 0.5;
+    for (int i = lev_start; i < 2 * lev_start; ++i) {
+      xa_n[i] = (i == 1) ? s.bs_xa : ((i & 1) ? xm_n[i >> 1] : xa_n[i >> 1]);
+      xm_n[i] = xa_n[i] + dml;
+      s.bs_cand[i - 1] = xm_n[i];
+    }
+    lev_start *= 2;
+  }
+
+}
+
+// Step length (:287-294).
+CM_DEVINL void fin_tau(CcgState& s, double (&a)[1]) {
+  // step length (ConstrainedConjugateGradients.py:287-294)
+  double tau = 0.0;
+  if (s.A_cg > 0) {
+    const double xx = -a[0];
+    if (xx > 0.0) tau = s.sum_cgt / xx;
+    else s.G = 0.0;
+  }
+  s.tau = tau;
+  s.cur_mixfac = s.p.mixfac;
+
+}
+
+// Load scaling, hardness cap and restart bookkeeping after the projection (:334-389).
+CM_DEVINL void fin_update(CcgState& s, double (&a)[5]) {
+  const CcgParams& P = s.p;
+  s.A_fl = (long long)a[0];
+  s.n_nc = (long long)a[4];
+  double mp = a[2];
+  if (P.has_h && s.A_fl > 0) mp = fmax(mp, -a[1]);
+  s.max_pres = mp;
+  s.pad_pres = 0.0;  // the force is structurally zero on the padding
+  s.uniform = 0;
+  s.scale = 1.0;
+  if (P.load_control) {
+    const double total = -a[3];
+    if (total != 0) s.scale = P.F / total;
+    else s.uniform = 1;
+  }
+  if (s.branch == 1) {
+    s.cur_mixfac *= P.mixdecfac;
+    if (s.mixsteps > 0) s.mixsteps -= 1;
+    s.delta = 0;
+    s.G = 0;
+    s.apply_nc = 0;
+  } else if (s.n_nc > 0) {
+    s.apply_nc = 1;
+    s.delta = 0;
+    s.mode = CMM_SD;
+  } else {
+    s.apply_nc = 0;
+    s.delta = 1;
+    s.mode = CMM_CG;
+  }
+
+}
+
+// Total force of the iteration's final forces and their maximum magnitude.
+CM_DEVINL void fin_force(CcgState& s, double (&a)[2]) {
+  s.total_force = -a[0];
+  s.fmax = a[1];
+
+}
+
+// ---------------------------------------------------------------------------
 // operator passes
 // ---------------------------------------------------------------------------
 template <typename R, int MODE>
@@ -230,10 +387,8 @@ k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   } else if (MODE == MODE_F) {
     double v[2] = {acc, amax};
     const int kinds[2] = {RED_SUM, RED_MAX};
-    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds, [&](double (&a)[2]) {
-      st->total_force = -a[0];
-      st->fmax = a[1];
-    });
+    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds,
+                   [&](double (&a)[2]) { fin_force(*st, a); });
   }
 }
 
@@ -462,17 +617,8 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   if (MODE == MODE_T) {
     double v[1] = {a0};
     const int kinds[1] = {RED_SUM};
-    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds, [&](double (&a)[1]) {
-      // step length (ConstrainedConjugateGradients.py:287-294)
-      double tau = 0.0;
-      if (st->A_cg > 0) {
-        const double xx = -a[0];
-        if (xx > 0.0) tau = st->sum_cgt / xx;
-        else st->G = 0.0;
-      }
-      st->tau = tau;
-      st->cur_mixfac = st->p.mixfac;
-    });
+    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, v, kinds,
+                   [&](double (&a)[1]) { fin_tau(*st, a); });
   } else if (MODE == MODE_F) {
     double v[2] = {a0, a1};
     const int kinds[2] = {RED_MAX, RED_MAX};
@@ -537,37 +683,8 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   });
   double v[5] = {a_c, a_cg, s_cg, gmax, gmin};
   const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[5]) {
-    CcgState& s = *st;
-    const CcgParams& P = s.p;
-    s.A_contact = (long long)a[0];
-    s.A_cg = (long long)a[1];
-    s.sum_cg = a[2];
-    s.gmax = a[3];
-    s.gmin = a[4];
-    const bool cg = !P.has_h || (s.A_contact > 0 && (double)s.A_cg / (double)s.A_contact > 0.01 &&
-                                 s.mixsteps <= 0);
-    s.bs_active = 0;
-    if (cg) {
-      s.branch = 0;
-      if (s.mode == CMM_MIX) s.mode = CMM_SD;
-      if (P.load_control) s.offset = (s.A_cg > 0) ? s.sum_cg / (double)s.A_cg : 0.0;
-    } else {
-      s.branch = 1;
-      if (s.mode != CMM_MIX) {
-        s.mixsteps = P.minmixsteps;
-        s.mode = CMM_MIX;
-      }
-      if (P.load_control) {
-        // scipy.optimize.bisect(f, a=max g, b=min g); first pass evaluates f(a)
-        s.bs_active = 1;
-        s.bs_iter = -1;
-        s.bs_xa = s.gmax;
-        s.bs_dm = s.gmin - s.gmax;
-        s.bs_cand[0] = s.gmax;
-      }
-    }
-  });
+  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[5]) { fin_begin(*st, a); });
 }
 
 // G = sum over the CG area of g^2 and the conjugation factor (:273-279).
@@ -596,11 +713,8 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   });
   double v[1] = {G};
   const int kinds[1] = {RED_SUM};
-  tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[1]) {
-    CcgState& s = *st;
-    s.G = a[0];
-    s.beta = (s.delta > 0 && s.G_old > 0) ? (double)s.delta * (s.G / s.G_old) : 0.0;
-  });
+  tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[1]) { fin_gsum(*st, a); });
 }
 
 // One pass of the load-controlled offset bisection of the mixing step
@@ -637,63 +751,7 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
   tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, cnt, kinds,
-                           [&](double (&a)[CM_BIS_CAND]) {
-    CcgState& s = *st;
-    const double H = s.p.H, F = s.p.F;
-    const double xtol = 2e-12, rtol = 8.881784197001252e-16;
-    const int maxit = 100;
-    if (s.bs_iter < 0) {
-      const double fa = a[0] * H - F;
-      const double fb = 0.0 * H - F;  // nothing lies below min g
-      s.bs_fa = fa;
-      if (fa * fb > 0) {
-        s.status = CMS_BISECT_SIGN;
-        s.done = 1;
-        s.bs_active = 0;
-        return;
-      }
-      if (fa == 0) { s.offset = s.bs_xa; s.bs_active = 0; return; }
-      if (fb == 0) { s.offset = s.gmin; s.bs_active = 0; return; }
-      s.bs_iter = 0;
-    } else {
-      int node = 1;
-      double xa = s.bs_xa, dm = s.bs_dm;
-      for (int lev = 0; lev < 5; ++lev) {
-        dm *= 0.5;
-        const double xm = xa + dm;
-        const double fm = a[node - 1] * H - F;
-        s.bs_iter += 1;
-        if (fm * s.bs_fa >= 0) { xa = xm; node = 2 * node + 1; }
-        else node = 2 * node;
-        if (fm == 0 || fabs(dm) < xtol + rtol * fabs(xm)) {
-          s.offset = xm;
-          s.bs_active = 0;
-          return;
-        }
-        if (s.bs_iter >= maxit) {
-          s.status = CMS_BISECT_SIGN + 1;  // bisection did not converge
-          s.done = 1;
-          s.bs_active = 0;
-          return;
-        }
-      }
-      s.bs_xa = xa;
-      s.bs_dm = dm;
-    }
-    // candidate midpoints of the next five levels, heap-indexed from 1
-    double xa_n[CM_BIS_CAND + 1], xm_n[CM_BIS_CAND + 1];
-    double dml = s.bs_dm;
-    int lev_start = 1;
-    for (int lev = 0; lev < 5; ++lev) {
-      dml *= 0.5;
-      for (int i = lev_start; i < 2 * lev_start; ++i) {
-        xa_n[i] = (i == 1) ? s.bs_xa : ((i & 1) ? xm_n[i >> 1] : xa_n[i >> 1]);
-        xm_n[i] = xa_n[i] + dml;
-        s.bs_cand[i - 1] = xm_n[i];
-      }
-      lev_start *= 2;
-    }
-  });
+                           [&](double (&a)[CM_BIS_CAND]) { fin_bisect(*st, a); });
 }
 
 // Force update, projection onto [0, H], constraint bookkeeping
@@ -745,36 +803,6 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   });
   double v[5] = {a_fl, min_fl, max_t, s_fp, n_nc};
   const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
-  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[5]) {
-    CcgState& s = *st;
-    const CcgParams& P = s.p;
-    s.A_fl = (long long)a[0];
-    s.n_nc = (long long)a[4];
-    double mp = a[2];
-    if (P.has_h && s.A_fl > 0) mp = fmax(mp, -a[1]);
-    s.max_pres = mp;
-    s.pad_pres = 0.0;  // the force is structurally zero on the padding
-    s.uniform = 0;
-    s.scale = 1.0;
-    if (P.load_control) {
-      const double total = -a[3];
-      if (total != 0) s.scale = P.F / total;
-      else s.uniform = 1;
-    }
-    if (s.branch == 1) {
-      s.cur_mixfac *= P.mixdecfac;
-      if (s.mixsteps > 0) s.mixsteps -= 1;
-      s.delta = 0;
-      s.G = 0;
-      s.apply_nc = 0;
-    } else if (s.n_nc > 0) {
-      s.apply_nc = 1;
-      s.delta = 0;
-      s.mode = CMM_SD;
-    } else {
-      s.apply_nc = 0;
-      s.delta = 1;
-      s.mode = CMM_CG;
-    }
-  });
+  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[5]) { fin_update(*st, a); });
 }

@@ -42,7 +42,7 @@ k_row_fwd_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int npairs = (nrows + 1) >> 1;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
-  C* bufB = bufA + (row_tile >> 1) * N;
+  C* bufB = bufA + smem_padded((row_tile >> 1) * N);
   stage_tw(tws, Sp->twy, N);
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int xa = x0 + 2 * s;
@@ -115,16 +115,16 @@ k_row_fwd_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     v[q] = cmake<C>(out[0], out[1]);
   }
   __syncthreads();  // twiddles staged
-  fft_p2<C, false, LOGN>(v, bufA + s * N, bufB + s * N, 1, tt, tws);
+  fft_p2<C, false, LOGN>(v, bufA, bufB, s * N, 1, tt, tws);
   __syncthreads();  // transform reads done before bufA is overwritten
 #pragma unroll
-  for (int q = 0; q < 8; ++q) bufA[s * N + tt + q * P::TPS] = v[q];
+  for (int q = 0; q < 8; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
   __syncthreads();
   C* __restrict__ spec = Sp->spec;
   for (int e = threadIdx.x; e < npairs * nyh; e += blockDim.x) {
     const int p = e / nyh, k = e - p * nyh;
-    const C z = bufA[p * N + k];
-    const C zm = bufA[p * N + ((N - k) & (N - 1))];
+    const C z = bufA[spad(p * N + k)];
+    const C zm = bufA[spad(p * N + ((N - k) & (N - 1)))];
     const int x = x0 + 2 * p;
     spec[spec_at(x, k, nx, lw)] = cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
     if (x + 1 < x0 + nrows)
@@ -138,10 +138,8 @@ k_row_fwd_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   } else {
     double vr[2] = {acc, amax};
     const int kinds[2] = {RED_SUM, RED_MAX};
-    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, vr, kinds, [&](double (&a)[2]) {
-      st->total_force = -a[0];
-      st->fmax = a[1];
-    });
+    tile_finish<2>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, vr, kinds,
+                   [&](double (&a)[2]) { fin_force(*st, a); });
   }
 }
 
@@ -164,7 +162,7 @@ k_col_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int nx_out = (MODE == MODE_T) ? Sp->tx : N;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
-  C* bufB = bufA + N * W;
+  C* bufB = bufA + smem_padded(N * W);
   stage_tw(tws, Sp->twx, N);
   const int c = threadIdx.x & (W - 1), tt = threadIdx.x >> lw;
   C* __restrict__ blk = Sp->spec + (size_t)item.y * N * W;
@@ -179,11 +177,11 @@ k_col_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
     g[q] = col_ok ? __ldg(tblk + x * W + c) : (R)0;
   }
   __syncthreads();  // twiddles staged
-  fft_p2<C, false, LOGN>(v, bufA + c, bufB + c, W, tt, tws);
+  fft_p2<C, false, LOGN>(v, bufA, bufB, c, W, tt, tws);
 #pragma unroll
   for (int q = 0; q < 8; ++q) v[q] = cscale(v[q], g[q]);
   __syncthreads();  // forward reads done before the inverse writes
-  fft_p2<C, true, LOGN>(v, bufA + c, bufB + c, W, tt, tws);
+  fft_p2<C, true, LOGN>(v, bufA, bufB, c, W, tt, tws);
   if (col_ok) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -215,27 +213,33 @@ k_row_inv_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int npairs = (nrows + 1) >> 1;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
-  C* bufB = bufA + (row_tile >> 1) * N;
+  C* bufB = bufA + smem_padded((row_tile >> 1) * N);
   stage_tw(tws, Sp->twy, N);
   const C* __restrict__ spec = Sp->spec;
-  for (int e = threadIdx.x; e < npairs * nyh; e += blockDim.x) {
+  struct XY { C X, Y; };
+  batched_loop<4>(npairs * nyh, [&](int e) {
     const int p = e / nyh, k = e - p * nyh;
     const int x = x0 + 2 * p;
-    C X = spec[spec_at(x, k, nx, lw)];
-    C Y = (x + 1 < x0 + nrows) ? spec[spec_at(x + 1, k, nx, lw)] : czero<C>();
+    XY r;
+    r.X = spec[spec_at(x, k, nx, lw)];
+    r.Y = (x + 1 < x0 + nrows) ? spec[spec_at(x + 1, k, nx, lw)] : czero<C>();
+    return r;
+  }, [&](int e, XY r) {
+    const int p = e / nyh, k = e - p * nyh;
+    C X = r.X, Y = r.Y;
     const bool selfconj = (k == 0) || (2 * k == N);
     if (selfconj) { X.y = 0; Y.y = 0; }
-    bufA[p * N + k] = cmake<C>(X.x - Y.y, X.y + Y.x);
-    if (!selfconj) bufA[p * N + N - k] = cmake<C>(X.x + Y.y, Y.x - X.y);
-  }
+    bufA[spad(p * N + k)] = cmake<C>(X.x - Y.y, X.y + Y.x);
+    if (!selfconj) bufA[spad(p * N + N - k)] = cmake<C>(X.x + Y.y, Y.x - X.y);
+  });
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const bool s_ok = s < npairs;
   C v[8];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) v[q] = s_ok ? bufA[s * N + tt + q * P::TPS] : czero<C>();
+  for (int q = 0; q < 8; ++q) v[q] = s_ok ? bufA[spad(s * N + tt + q * P::TPS)] : czero<C>();
   // the first stage writes bufB while other threads may still read bufA
-  fft_p2<C, true, LOGN>(v, bufB + s * N, bufA + s * N, 1, tt, tws);
+  fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
   const int xa = x0 + 2 * s;
   const bool va_ok = s_ok, vb_ok = s_ok && (xa + 1 < x0 + nrows);
   double a0 = 0.0, a1 = -INFINITY;
@@ -250,17 +254,8 @@ k_row_inv_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     }
     double vr[1] = {a0};
     const int kinds[1] = {RED_SUM};
-    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, vr, kinds, [&](double (&a)[1]) {
-      // step length (ConstrainedConjugateGradients.py:287-294)
-      double tau = 0.0;
-      if (st->A_cg > 0) {
-        const double xx = -a[0];
-        if (xx > 0.0) tau = st->sum_cgt / xx;
-        else st->G = 0.0;
-      }
-      st->tau = tau;
-      st->cur_mixfac = st->p.mixfac;
-    });
+    tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_rowt, vr, kinds,
+                   [&](double (&a)[1]) { fin_tau(*st, a); });
   } else {
     R* __restrict__ u = Sp->u;
     const R* __restrict__ h = Sp->h;

@@ -13,6 +13,7 @@
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
 #include "cm_kernels_p2.cuh"
+#include "cm_persist.cuh"
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
 #define CM_SMEM_COL_MAX (160 * 1024)
@@ -20,6 +21,7 @@
 #define CM_BISECT_PASSES 21
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
+#define CM_PERSIST_ITERS 32   // iterations per cooperative launch
 
 #define CK(...)                               \
   do {                                        \
@@ -37,6 +39,7 @@
   } while (0)
 
 static unsigned long long g_launches = 0;  // kernels launched by this library
+static thread_local int g_polls = 0;        // convergence polls of the current call
 
 static cudaError_t& last_cuda_error() {
   static thread_local cudaError_t e = cudaSuccess;
@@ -104,7 +107,9 @@ static int pow2_threads(size_t work) {
 // column tile `col_tile` = 2^lw half-spectrum columns.  Shared memory holds
 // the twiddles of the transform plus two ping-pong buffers.
 static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, Tiles* t) {
-  const size_t elems = CM_SMEM_ROW / (2 * csize);
+  // 2048 transform elements per tile: 256 threads for the register-resident
+  // transforms, so two blocks share an SM and overlap memory with compute
+  const size_t elems = std::min<size_t>(CM_SMEM_ROW / (2 * csize), 2048);
   int np = (int)std::max<size_t>(1, elems / (size_t)ny);
   np = std::min(np, (nx + 1) / 2);
   const size_t srow = (2 * (size_t)np * ny + ny) * csize;
@@ -122,9 +127,12 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   t->threads_col = pow2_threads(((size_t)1 << lw) * nx);
   t->ntile_cols = (nyh + t->col_tile - 1) / t->col_tile;
   t->comp_rows = std::max(1, std::min(tx, CM_COMP_ELEMS / std::max(1, ty)));
-  // register-resident power-of-two transforms: one thread per 8 elements
+  // register-resident power-of-two transforms: one thread per 8 elements;
+  // their shared buffers carry one padding slot per 8 elements
   t->p2_threads_row = np * (ny / 8);
   t->p2_threads_col = (1 << lw) * (nx / 8);
+  t->smem_row = std::max(t->smem_row, (size_t)(2 * smem_padded(np * ny) + ny) * csize);
+  t->smem_col = std::max(t->smem_col, (size_t)(2 * smem_padded((1 << lw) * nx) + nx) * csize);
   auto is_p2 = [](int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; };
   t->p2 = is_p2(nx) && is_p2(ny) && t->p2_threads_row >= 32 && t->p2_threads_row <= CM_FFT_THREADS &&
           t->p2_threads_col >= 32 && t->p2_threads_col <= CM_FFT_THREADS;
@@ -396,6 +404,10 @@ struct Work {
   double* partials = nullptr;
   unsigned int* counter = nullptr;
   bool ccg_ready = false;
+  GridBarrier* bar = nullptr;   // persistent solver: grid barrier
+  bool persist = false;         // persistent cooperative kernel usable
+  int persist_grid = 0, persist_threads = 0, persist_logn = 0;
+  size_t persist_smem = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
   int nt_comp = 0, nt_rowt = 0, nt_rowd = 0, nt_col = 0;
@@ -551,6 +563,7 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
   w.nt_col = s.nt_col;
   CK(cudaMemcpyAsync(w.d_ccg, &s, sizeof(s), cudaMemcpyHostToDevice, p->stream));
   CK(cudaStreamSynchronize(p->stream));
+  CKS(setup_persist(p, w));
   w.ccg_ready = true;
   return CM_OK;
 }
@@ -738,6 +751,60 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
   return CM_OK;
 }
 
+// ---- persistent cooperative solver --------------------------------------------
+template <typename R>
+static const void* persist_kernel(int logn) {
+  switch (logn) {
+#define CM_CASE(L) case L: return (const void*)k_ccg_persist<R, L>;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return nullptr;
+  }
+}
+
+// Decide whether the persistent kernel can run this plan and size its grid.
+template <typename R>
+static int setup_persist(cm_plan* p, Work<R>& w) {
+  w.persist = false;
+  const Tiles& T = w.tiles;
+  if (!T.p2 || p->nx != p->ny || T.p2_threads_row != T.p2_threads_col) return CM_OK;
+  const int logn = log2_exact(p->nx);
+  const void* k = persist_kernel<R>(logn);
+  if (!k) return CM_OK;
+  typedef typename CT<R>::C C;
+  const int ebuf = smem_padded(std::max((T.row_tile / 2) * p->nx, T.col_tile * p->nx));
+  const size_t smem = (size_t)(p->nx + 2 * ebuf) * sizeof(C);
+  if (smem > CM_SMEM_COL_MAX) return CM_OK;
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+  int per_sm = 0, dev = 0, nsm = 0, coop = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, T.p2_threads_row, smem));
+  if (!coop || per_sm < 1) return CM_OK;
+  const int tiles = std::max({w.nt_comp, w.nt_rowd, w.nt_col});
+  w.persist_grid = std::min(per_sm * nsm, tiles);
+  w.persist_threads = T.p2_threads_row;
+  w.persist_smem = smem;
+  w.persist_logn = logn;
+  if (!w.bar) CKS(dalloc(p, &w.bar, 1));
+  w.persist = true;
+  return CM_OK;
+}
+
+template <typename R>
+static int launch_persist(cm_plan* p, Work<R>& w, int iters, int bisect_passes, cudaStream_t s) {
+  CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
+  const Slot<R>* S = w.d_ccg;
+  GridBarrier* bar = w.bar;
+  void* args[] = {(void*)&S, (void*)&bar, (void*)&iters, (void*)&bisect_passes};
+  CK(cudaLaunchCooperativeKernel(persist_kernel<R>(w.persist_logn), dim3(w.persist_grid),
+                                 dim3(w.persist_threads), args, w.persist_smem, s));
+  g_launches += 1;
+  return CM_OK;
+}
+
 struct SolveInput {
   const double* h64;
   const double* u0;
@@ -793,6 +860,25 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   }
   CK(cudaGetLastError());
   const bool bisect = prm->has_hardness && prm->load_control;
+  if (prof_iters > 0 && w.persist) {
+    // profiler: one cooperative launch of prof_iters iterations
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    CKS(launch_persist(p, w, prof_iters, bisect ? CM_BISECT_PASSES : 0, s));
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    prof_ms[0] = ms / prof_iters;
+    CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *fin = *p->h_state;
+    return CM_OK;
+  }
   if (prof_iters > 0) {
     // profiler: eager launches with an event between kernels
     std::vector<cudaEvent_t> ev(CM_ITER_KERNELS + 1);
@@ -818,14 +904,35 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     const long work = (long)p->nx * p->ny;
     every = work >= (1L << 20) ? 4 : (work >= (1L << 16) ? 8 : 16);
   }
+  auto t0 = std::chrono::steady_clock::now();
+  if (w.persist) {
+    for (int done_iters = 0;; done_iters += CM_PERSIST_ITERS) {
+      CKS(launch_persist(p, w, CM_PERSIST_ITERS, bisect ? CM_BISECT_PASSES : 0, s));
+      CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      ++g_polls;
+      if (p->h_state->done) break;
+      if (prm->timeout_s > 0) {
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > prm->timeout_s) return CM_ERR_TIMEOUT;
+      }
+      if (done_iters > maxiter + 2 * CM_PERSIST_ITERS) return CM_ERR_CUDA;
+    }
+    *fin = *p->h_state;
+    if (fin->status == CMS_TIMEOUT) return CM_ERR_TIMEOUT;
+    if (fin->status == CMS_NAN) return CM_ERR_NAN;
+    if (fin->status == CMS_BISECT_SIGN) return CM_ERR_BISECT;
+    if (fin->status == CMS_BISECT_SIGN + 1) return CM_ERR_BISECT_CONV;
+    return CM_OK;
+  }
   cudaGraphExec_t g;
   CKS(get_graph<R>(p, w, bisect, every, &g));
-  auto t0 = std::chrono::steady_clock::now();
   for (int done_iters = 0;; done_iters += every) {
     CK(cudaGraphLaunch(g, s));
     g_launches += (unsigned long long)every * iteration_launches(bisect);
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    ++g_polls;
     if (p->h_state->done) break;
     if (prm->timeout_s > 0) {
       const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1039,10 +1146,18 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   memset(res, 0, sizeof(*res));
   SolveInput in{h, u0, f0, p->ny};
   CcgState fin;
+  g_polls = 0;
+  typedef std::chrono::steady_clock clk;
+  const auto t0 = clk::now();
+  auto ms_since = [](clk::time_point a) {
+    return std::chrono::duration<double, std::milli>(clk::now() - a).count();
+  };
   if (prm->precision == CM_FP64) {
     CKS(run_ccg<double>(p, p->w64, prm, in, 0.0, 0.0, prm->maxiter, &fin));
     CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
     fill_result(fin, res);
+    res->ms_fp64 = res->ms_total = ms_since(t0);
+    res->polls = g_polls;
     return CM_OK;
   }
   const double rp = prm->precision == CM_MIXED ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
@@ -1051,12 +1166,16 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   // reach them within its iteration cap hands over to the FP64 refinement
   const int cap32 = prm->precision == CM_MIXED ? std::min(prm->maxiter, CM_FP32_ITER_CAP) : prm->maxiter;
   CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin));
+  const double ms32 = ms_since(t0);
   if (prm->precision == CM_FP32) {
     CKS(finish_ccg<float>(p, p->w32, x, jac, active, plastic, &fin));
     fill_result(fin, res);
     res->nit_fp32 = fin.it;
+    res->ms_fp32 = res->ms_total = ms_since(t0);
+    res->polls = g_polls;
     return CM_OK;
   }
+  const auto t1 = clk::now();
   // FP64 refinement warm-started from the FP32 forces (initial_forces semantics)
   const int nit32 = fin.it, nfev32 = fin.nfev;
   double* f64 = nullptr;
@@ -1078,6 +1197,10 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   res->nit += nit32;
   res->nfev += nfev32;
   res->nit_fp32 = nit32;
+  res->ms_fp32 = ms32;
+  res->ms_fp64 = ms_since(t1);
+  res->ms_total = ms_since(t0);
+  res->polls = g_polls;
   return CM_OK;
 }
 
@@ -1094,9 +1217,15 @@ int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int it
     CKS(run_ccg<double>(p, p->w64, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
   else
     CKS(run_ccg<float>(p, p->w32, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
-  if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
-  if (names)
-    for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) names[k] = k_iter_names[k];
+  const bool persist = prm->precision == CM_FP64 ? p->w64.persist : p->w32.persist;
+  if (persist) {
+    if (n_kernels) *n_kernels = 1;
+    if (names) names[0] = "k_ccg_persist";
+  } else {
+    if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
+    if (names)
+      for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) names[k] = k_iter_names[k];
+  }
   return fin.done && fin.it < iters ? CM_ERR_ARG : CM_OK;
 }
 

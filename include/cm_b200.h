@@ -105,6 +105,8 @@ typedef struct {
   double rms_pen, max_pen, max_pres, pad_pres, maxdu, total_force;
   double pentol_used;
   long long area, cg_area, plastic_area;
+  double ms_fp32, ms_fp64, ms_total;  /* host wall time of the phases of the call */
+  int polls;                          /* host convergence polls */
 } cm_ccg_result;
 
 /* Returns the message for a status code. */
