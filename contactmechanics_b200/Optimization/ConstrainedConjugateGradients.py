@@ -182,3 +182,134 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
                       pad_pressure=res.pad_pres, penetration_tol=res.pentol_used,
                       pressure_tol=forcetol))
     return result
+
+
+def _params(precision, external_force, offset, hardness, pentol, forcetol, thermotol, mixfac,
+            mixdecfac, minmixsteps, maxiter, timeout=None):
+    P = _lib.CcgParams()
+    P.precision = _lib.PRECISIONS[precision]
+    P.load_control = int(external_force is not None)
+    P.external_force = float(external_force) if external_force is not None else 0.0
+    P.offset = float(offset) if offset is not None else 0.0
+    P.has_hardness = int(hardness is not None)
+    P.hardness = float(hardness) if hardness is not None else 0.0
+    P.pentol = float(pentol) if pentol is not None else -1.0
+    P.forcetol = float(forcetol)
+    P.thermotol = float(thermotol)
+    P.mixfac = float(mixfac)
+    P.mixdecfac = float(mixdecfac)
+    P.minmixsteps = int(minmixsteps)
+    P.maxiter = int(maxiter)
+    P.timeout_s = float(timeout) if timeout else 0.0
+    return P
+
+
+def _per_solve(value, n, name):
+    if value is None or np.isscalar(value):
+        return [value] * n
+    value = list(value)
+    if len(value) != n:
+        raise ValueError(f"{name} needs one entry per solve")
+    return value
+
+
+def constrained_conjugate_gradients_batch(substrates, topographies, hardness=None,
+                                          external_force=None, offset=None,
+                                          initial_displacements=None, pentol=None,
+                                          forcetol=1e-5, thermotol=1e-6, mixfac=0.1,
+                                          mixdecfac=0.95, minmixsteps=10, maxiter=100000,
+                                          precision="fp64", timeout=None):
+    """Solve several independent contact problems together.
+
+    ``substrates`` and ``topographies`` are sequences of equal length (one
+    substrate per solve; grid sizes may differ).  ``hardness``,
+    ``external_force``, ``offset``, ``initial_displacements``, ``pentol``
+    and ``forcetol`` are scalars applied to every solve or sequences with one
+    entry per solve.  Every solve keeps the semantics of
+    :func:`constrained_conjugate_gradients`; all solves advance together on the
+    device (``cm_ccg_solve_batch``).  Returns a list of ``OptimizeResult``.
+    """
+    torch = _torch()
+    n = len(substrates)
+    if n == 0 or len(topographies) != n:
+        raise ValueError("need one topography per substrate")
+    if precision not in _lib.PRECISIONS:
+        raise ValueError("precision must be one of {}".format(sorted(_lib.PRECISIONS)))
+    H = _per_solve(hardness, n, "hardness")
+    F = _per_solve(external_force, n, "external_force")
+    O = _per_solve(offset, n, "offset")
+    U0 = (_per_solve(initial_displacements, n, "initial_displacements")
+          if initial_displacements is not None and not hasattr(initial_displacements, "shape")
+          else [initial_displacements] * n)
+    PT = _per_solve(pentol, n, "pentol")
+    FT = _per_solve(forcetol, n, "forcetol")
+    plans, params, keep = [], [], []
+    hs, u0s, xs, jacs, acts, pls = [], [], [], [], [], []
+    as_torch = []
+    for i in range(n):
+        sub, topo = substrates[i], topographies[i]
+        if getattr(sub, "_plan", None) is None or sub.dim != 2:
+            raise ValueError("batch solves need 2D contactmechanics_b200 half-spaces")
+        heights = topo.heights() if hasattr(topo, "nb_grid_pts") else topo
+        if tuple(heights.shape) != tuple(sub.nb_grid_pts):
+            raise ValueError("topography shape does not match its substrate")
+        if H[i] is not None and not float(H[i]) > 0:
+            raise ValueError("hardness must be positive")
+        as_torch.append(isinstance(heights, torch.Tensor) and heights.is_cuda)
+        dom = tuple(sub.nb_domain_grid_pts)
+        h = _device_f64(heights)
+        u0 = _device_f64(U0[i], dom) if U0[i] is not None else None
+        x = torch.empty(dom, dtype=torch.float64, device="cuda")
+        jac = torch.empty(tuple(sub.nb_grid_pts), dtype=torch.float64, device="cuda")
+        act = torch.empty(tuple(sub.nb_grid_pts), dtype=torch.uint8, device="cuda")
+        pl = torch.empty(tuple(sub.nb_grid_pts), dtype=torch.uint8, device="cuda") if H[i] is not None else None
+        keep += [h, u0, x, jac, act, pl]
+        hs.append(h); u0s.append(u0); xs.append(x); jacs.append(jac); acts.append(act); pls.append(pl)
+        plans.append(sub._plan.ptr)
+        params.append(_params(precision, F[i], O[i], H[i], PT[i], FT[i], thermotol, mixfac,
+                              mixdecfac, minmixsteps, maxiter, timeout))
+
+    def arr(ts):
+        return (ctypes.c_void_p * n)(*[t.data_ptr() if t is not None else None for t in ts])
+
+    plan_arr = (ctypes.c_void_p * n)(*[p.value for p in plans])
+    par_arr = (_lib.CcgParams * n)(*params)
+    res_arr = (_lib.CcgResult * n)()
+    torch.cuda.current_stream().synchronize()
+    L = substrates[0]._plan._L
+    code = L.cm_ccg_solve_batch(n, plan_arr, par_arr, arr(hs), arr(u0s), arr(xs), arr(jacs),
+                                arr(acts), arr(pls), res_arr, None)
+    if code == _lib.CM_ERR_NAN:
+        raise RuntimeError("nan encountered.")
+    if code == _lib.CM_ERR_BISECT:
+        raise ValueError("f(a) and f(b) must have different signs")
+    if code == _lib.CM_ERR_BISECT_CONV:
+        raise RuntimeError("Failed to converge after 100 iterations")
+    _lib.check(code)
+    out = []
+    for i in range(n):
+        r = res_arr[i]
+        result = optim.OptimizeResult()
+        result.nit, result.nfev, result.nit_fp32 = r.nit, r.nfev, r.nit_fp32
+        result.success = r.status == _lib.CM_SOLVE_CONVERGED
+        result.message = ("Polonsky converged" if result.success
+                          else "Reached maxiter = {}".format(maxiter))
+        result.maxcv = {"max_pen": r.max_pen, "max_pres": r.max_pres}
+        result.offset, result.fun, result.pentol = r.offset, r.fun, r.pentol_used
+        result.timing = {"ms_fp32": r.ms_fp32, "ms_fp64": r.ms_fp64, "ms_total": r.ms_total,
+                         "polls": r.polls}
+        sub = substrates[i]
+        act_dom = torch.zeros(tuple(sub.nb_domain_grid_pts), dtype=torch.bool, device="cuda")
+        nb = sub.nb_grid_pts
+        act_dom[:nb[0], :nb[1]] = acts[i].bool()
+        if as_torch[i]:
+            result.x, result.jac, result.active_set = xs[i], jacs[i], act_dom
+            if pls[i] is not None and result.success:
+                result.plastic = pls[i].bool()
+        else:
+            result.x, result.jac = xs[i].cpu().numpy(), jacs[i].cpu().numpy()
+            result.active_set = act_dom.cpu().numpy()
+            if pls[i] is not None and result.success:
+                result.plastic = pls[i].bool().cpu().numpy()
+        out.append(result)
+    return out

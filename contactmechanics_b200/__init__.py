@@ -8,7 +8,8 @@ reference's Substrates / Systems / Optimization call signatures.
 from .Substrates import ElasticSubstrate, PlasticSubstrate, Substrate  # noqa: F401
 from .FFTElasticHalfSpace import (FreeFFTElasticHalfSpace,  # noqa: F401
                                   PeriodicFFTElasticHalfSpace)
-from .Optimization import constrained_conjugate_gradients  # noqa: F401
+from .Optimization import (constrained_conjugate_gradients,  # noqa: F401
+                           constrained_conjugate_gradients_batch)
 from .Systems import NonSmoothContactSystem  # noqa: F401
 from .PlasticSystemSpecialisations import PlasticNonSmoothContactSystem  # noqa: F401
 from .Factory import make_plastic_system, make_system  # noqa: F401

@@ -87,6 +87,8 @@ SIGNATURES = {
                           ctypes.POINTER(CcgResult)]),
     "cm_ccg_solve_host": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp, ctypes.POINTER(CcgResult)]),
+    "cm_ccg_solve_batch": (_i, [_i, _vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp,
+                                ctypes.POINTER(CcgResult), _vp]),
     "cm_launch_count": (ctypes.c_ulonglong, []),
     "cm_ccg_profile": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _i,
                             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i),

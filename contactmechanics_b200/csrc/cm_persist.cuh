@@ -450,7 +450,7 @@ CM_DEVINL void ph_row_inv(const Slot<R>& S, const CcgView& cv, int tile,
 // the kernel
 // ---------------------------------------------------------------------------
 template <typename R, int LOGN>
-__global__ void __launch_bounds__(sizeof(R) == 8 ? CM_FFT_THREADS / 2 : CM_FFT_THREADS)
+__global__ void __launch_bounds__(CM_FFT_THREADS / 2)
 k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters, int bisect_passes) {
   typedef typename CT<R>::C C;
   constexpr int N = 1 << LOGN;

@@ -430,6 +430,10 @@ struct cm_plan {
   std::vector<void*> allocs;
 };
 
+template <typename R> static Work<R>& work_of(cm_plan* p);
+template <> Work<float>& work_of<float>(cm_plan* p) { return p->w32; }
+template <> Work<double>& work_of<double>(cm_plan* p) { return p->w64; }
+
 static int dev_alloc(cm_plan* p, void** ptr, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMalloc(ptr, bytes);
@@ -812,11 +816,11 @@ struct SolveInput {
   int f0_ld;
 };
 
+// State, heights and initial fields of one solve (ConstrainedConjugateGradients.py
+// :132-219), enqueued on stream s.
 template <typename R>
-static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
-                   double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
-                   int prof_iters = 0, float* prof_ms = nullptr) {
-  cudaStream_t s = p->stream;
+static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
+                    double rel_pentol, double rel_forcetol, int maxiter, cudaStream_t s) {
   set_smem_attrs<R>();
   CKS(ensure_ccg(p, w));
   CcgState st;
@@ -859,6 +863,15 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
                               p->ty, p->ty, s));
   }
   CK(cudaGetLastError());
+  return CM_OK;
+}
+
+template <typename R>
+static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
+                   double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
+                   int prof_iters = 0, float* prof_ms = nullptr) {
+  cudaStream_t s = p->stream;
+  CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   const bool bisect = prm->has_hardness && prm->load_control;
   if (prof_iters > 0 && w.persist) {
     // profiler: one cooperative launch of prof_iters iterations
@@ -949,8 +962,8 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
 
 template <typename R>
 static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned char* active,
-                      unsigned char* plastic, CcgState* fin) {
-  cudaStream_t s = p->stream;
+                      unsigned char* plastic, CcgState* fin, cudaStream_t s = nullptr) {
+  if (!s) s = p->stream;
   k_ccg_result<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, jac, active, plastic);
   g_launches += 1;
   if (x) {
@@ -981,6 +994,136 @@ static void fill_result(const CcgState& st, cm_ccg_result* r) {
   r->area = st.A_contact;
   r->cg_area = st.A_cg;
   r->plastic_area = st.A_fl;
+}
+
+// ---------------------------------------------------------------------------
+// batches of independent solves
+// ---------------------------------------------------------------------------
+// Count the solves of a batch that have not finished.
+template <typename R>
+__global__ void k_count_running(const Slot<R>* __restrict__ slots, int n, int* out) {
+  int c = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c += slots[i].st->done ? 0 : 1;
+  c = __reduce_add_sync(0xffffffffu, c);
+  __shared__ int sm[32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) t += sm[i];
+    *out = t;
+  }
+}
+
+// Device arrays of one batch: slot descriptors and the (slot, tile) work
+// lists of the four tile spaces.
+template <typename R>
+struct BatchDev {
+  Slot<R>* slots = nullptr;
+  int2* items[4] = {nullptr, nullptr, nullptr, nullptr};  // comp, rows<tx, rows<nx, columns
+  int n_items[4] = {0, 0, 0, 0};
+  int* running = nullptr;
+  size_t smem_row = 0, smem_col = 0;
+  std::vector<void*> allocs;
+  ~BatchDev() {
+    for (void* a : allocs) cudaFree(a);
+  }
+};
+
+template <typename R>
+static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_t s) {
+  std::vector<Slot<R>> hs(n);
+  std::vector<int2> it[4];
+  for (int i = 0; i < n; ++i) {
+    Work<R>& w = work_of<R>(plans[i]);
+    hs[i] = base_slot(plans[i], w);
+    for (int t = 0; t < hs[i].nt_comp; ++t) it[0].push_back(make_int2(i, t));
+    for (int t = 0; t < hs[i].nt_rowt; ++t) it[1].push_back(make_int2(i, t));
+    for (int t = 0; t < hs[i].nt_rowd; ++t) it[2].push_back(make_int2(i, t));
+    for (int t = 0; t < hs[i].nt_col; ++t) it[3].push_back(make_int2(i, t));
+    b.smem_row = std::max(b.smem_row, w.tiles.smem_row);
+    b.smem_col = std::max(b.smem_col, w.tiles.smem_col);
+  }
+  auto al = [&](void** ptr, size_t bytes) -> int {
+    if (cudaMalloc(ptr, bytes) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+    b.allocs.push_back(*ptr);
+    return CM_OK;
+  };
+  CKS(al((void**)&b.slots, sizeof(Slot<R>) * n));
+  CK(cudaMemcpyAsync(b.slots, hs.data(), sizeof(Slot<R>) * n, cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < 4; ++k) {
+    b.n_items[k] = (int)it[k].size();
+    CKS(al((void**)&b.items[k], sizeof(int2) * std::max<size_t>(1, it[k].size())));
+    CK(cudaMemcpyAsync(b.items[k], it[k].data(), sizeof(int2) * it[k].size(), cudaMemcpyHostToDevice, s));
+  }
+  CKS(al((void**)&b.running, sizeof(int)));
+  CK(cudaStreamSynchronize(s));
+  return CM_OK;
+}
+
+// One iteration of every solve of the batch (generic transforms: the solves
+// may all have different sizes).
+template <typename R>
+static void launch_iteration_batch(const BatchDev<R>& b, bool bisect, cudaStream_t s) {
+  const Slot<R>* S = b.slots;
+  k_ccg_begin<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  if (bisect)
+    for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  k_ccg_gsum<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  k_row_fwd<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
+  k_col<R, MODE_T><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
+  k_row_inv<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
+  k_ccg_update<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  k_row_fwd<R, MODE_F><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
+  k_col<R, MODE_F><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
+  k_row_inv<R, MODE_F><<<b.n_items[2], CM_THREADS, b.smem_row, s>>>(S, b.items[2]);
+}
+
+// Run the CCG loop of every solve of the batch to completion.
+template <typename R>
+static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, double timeout_s,
+                      cudaStream_t s, int* polls) {
+  set_smem_attrs<R>();
+  BatchDev<R> b;
+  CKS(batch_build<R>(n, plans, b, s));
+  long work = 0;
+  for (int i = 0; i < n; ++i) work += (long)plans[i]->nx * plans[i]->ny;
+  const int every = work >= (1L << 22) ? 4 : 16;
+  cudaGraph_t g;
+  cudaGraphExec_t ge;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  for (int i = 0; i < every; ++i) launch_iteration_batch<R>(b, bisect, s);
+  k_count_running<R><<<1, 256, 0, s>>>(b.slots, n, b.running);
+  CK(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
+  int running = n;
+  int rc = CM_OK;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int done_iters = 0; running > 0; done_iters += every) {
+    if (cudaGraphLaunch(ge, s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
+    g_launches += (unsigned long long)every * (iteration_launches(bisect)) + 1;
+    if (cudaMemcpyAsync(&running, b.running, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
+    if (polls) ++*polls;
+    if (timeout_s > 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s) {
+      rc = CM_ERR_TIMEOUT;
+      break;
+    }
+    if (done_iters > maxiter + 2 * every) { rc = CM_ERR_CUDA; break; }
+  }
+  cudaGraphExecDestroy(ge);
+  return rc;
+}
+
+static int status_error(const CcgState& st) {
+  if (st.status == CMS_NAN) return CM_ERR_NAN;
+  if (st.status == CMS_BISECT_SIGN) return CM_ERR_BISECT;
+  if (st.status == CMS_BISECT_SIGN + 1) return CM_ERR_BISECT_CONV;
+  if (st.status == CMS_TIMEOUT) return CM_ERR_TIMEOUT;
+  return CM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1201,6 +1344,102 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   res->ms_fp64 = ms_since(t1);
   res->ms_total = ms_since(t0);
   res->polls = g_polls;
+  return CM_OK;
+}
+
+int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params,
+                       const double* const* h, const double* const* u0, double* const* x,
+                       double* const* jac, unsigned char* const* active,
+                       unsigned char* const* plastic, cm_ccg_result* res, void* stream) {
+  if (n < 1 || !plans || !params || !h || !res) return CM_ERR_ARG;
+  const int prec = params[0].precision;
+  bool bisect = false;
+  for (int i = 0; i < n; ++i) {
+    if (!plans[i] || !h[i]) return CM_ERR_ARG;
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return CM_ERR_ARG;  // a plan's buffers serve one solve at a time
+    if (params[i].precision != prec || params[i].maxiter < 1) return CM_ERR_ARG;
+    if (params[i].has_hardness && !(params[i].hardness > 0)) return CM_ERR_ARG;
+    bisect = bisect || (params[i].has_hardness && params[i].load_control);
+    memset(&res[i], 0, sizeof(res[i]));
+  }
+  if (prec != CM_FP64 && prec != CM_FP32 && prec != CM_MIXED) return CM_ERR_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : plans[0]->stream;
+  int maxiter = 0;
+  double timeout = 0;
+  for (int i = 0; i < n; ++i) {
+    maxiter = std::max(maxiter, params[i].maxiter);
+    timeout = std::max(timeout, params[i].timeout_s);
+  }
+  g_polls = 0;
+  typedef std::chrono::steady_clock clk;
+  const auto t0 = clk::now();
+  std::vector<int> nit32(n, 0), nfev32(n, 0);
+  if (prec != CM_FP64) {
+    const double rp = prec == CM_MIXED ? (params[0].fp32_pentol_rel > 0 ? params[0].fp32_pentol_rel : 2e-6) : 0.0;
+    const double rf = prec == CM_MIXED ? 1e-5 : 0.0;
+    for (int i = 0; i < n; ++i) {
+      SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, plans[i]->ny};
+      const int mi = prec == CM_MIXED ? std::min(params[i].maxiter, CM_FP32_ITER_CAP) : params[i].maxiter;
+      CKS(ccg_init<float>(plans[i], plans[i]->w32, &params[i], in, rp, rf, mi, s));
+    }
+    CKS(batch_loop<float>(n, plans, bisect, maxiter, timeout, s, &g_polls));
+    for (int i = 0; i < n; ++i) {
+      CcgState st;
+      CK(cudaMemcpyAsync(plans[i]->h_state, plans[i]->w32.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      st = *plans[i]->h_state;
+      CKS(status_error(st));
+      nit32[i] = st.it;
+      nfev32[i] = st.nfev;
+      if (prec == CM_FP32) {
+        CKS(finish_ccg<float>(plans[i], plans[i]->w32, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
+                              active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, &st, s));
+        fill_result(st, &res[i]);
+        res[i].nit_fp32 = nit32[i];
+      }
+    }
+    if (prec == CM_FP32) {
+      const double ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+      for (int i = 0; i < n; ++i) { res[i].ms_total = res[i].ms_fp32 = ms; res[i].polls = g_polls; }
+      return CM_OK;
+    }
+  }
+  const auto t1 = clk::now();
+  for (int i = 0; i < n; ++i) {
+    cm_plan* p = plans[i];
+    if (prec == CM_MIXED) {
+      CKS(ensure_ccg(p, p->w64));
+      CK(cudaMemcpyAsync(p->h_state, p->w32.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const int fpar = p->h_state->parity;
+      k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
+          p->w32.f[fpar], p->tx, p->ty, p->w64.u, p->nx, p->ny);
+      SolveInput in{h[i], nullptr, p->w64.u, p->ny};
+      CKS(ccg_init<double>(p, p->w64, &params[i], in, 0.0, 0.0,
+                           std::max(1, params[i].maxiter - nit32[i]), s));
+    } else {
+      SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, p->ny};
+      CKS(ccg_init<double>(p, p->w64, &params[i], in, 0.0, 0.0, params[i].maxiter, s));
+    }
+  }
+  CKS(batch_loop<double>(n, plans, bisect, maxiter, timeout, s, &g_polls));
+  const double ms64 = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
+  const double ms32 = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  for (int i = 0; i < n; ++i) {
+    CcgState st;
+    CKS(finish_ccg<double>(plans[i], plans[i]->w64, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
+                           active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, &st, s));
+    CKS(status_error(st));
+    fill_result(st, &res[i]);
+    res[i].nit += nit32[i];
+    res[i].nfev += nfev32[i];
+    res[i].nit_fp32 = nit32[i];
+    res[i].ms_fp32 = ms32;
+    res[i].ms_fp64 = ms64;
+    res[i].ms_total = ms32 + ms64;
+    res[i].polls = g_polls;
+  }
   return CM_OK;
 }
 

@@ -180,6 +180,25 @@ int cm_ccg_solve_host(cm_plan* plan, const cm_ccg_params* params, const double* 
                       unsigned char* plastic_host, cm_ccg_result* res);
 
 /*
+ * Solve n independent contact problems (each with its own plan, i.e. its own
+ * grid size, substrate and tables) together: every iteration advances all
+ * unfinished solves with one launch per field pass over the combined
+ * (solve, tile) work list, replayed from a CUDA graph.  CM_MIXED runs the
+ * FP32 phase of all solves, then the FP64 refinement of all solves.  All
+ * params must share the precision.  Arrays are per solve, device pointers;
+ * init_disp_dev, x_dev, jac_dev, active_dev, plastic_dev may be NULL (the
+ * whole array) or hold NULL entries.  Results in res[0..n).  The batch
+ * replaces n calls of constrained_conjugate_gradients
+ * (ConstrainedConjugateGradients.py:47-509); each solve keeps the reference's
+ * semantics, and its result does not depend on the other members of the batch.
+ */
+int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params,
+                       const double* const* heights_dev, const double* const* init_disp_dev,
+                       double* const* x_dev, double* const* jac_dev,
+                       unsigned char* const* active_dev, unsigned char* const* plastic_dev,
+                       cm_ccg_result* res, void* stream);
+
+/*
  * Number of kernels this library has launched in the process (graph nodes
  * count once per replay).  Instrumentation; no reference counterpart.
  */
