@@ -305,6 +305,81 @@ def run_gpu(args, rank, world, local_rank):
         h2d=h.nbytes + nxd * nyd * 8, d2h=nxd * nyd * 8 + h.nbytes + nxd * nyd)
 
 
+# ---------------------------------------------------------------------------
+# batched configuration: 512 independent periodic solves of uneven sizes
+# ---------------------------------------------------------------------------
+C3_SIDES = (64, 96, 128, 192, 256, 384, 512)
+C3_N = 512
+C3_WORKLOAD = ("512 periodic solves, nx, ny drawn uniformly from {64,96,128,192,256,384,512}, "
+               "self-affine H~U[0.3,0.9], rms slope~U[0.05,0.2], mean pressure log-uniform "
+               "1e-4..1e-2 E*, seed = index; pentol 1e-9*(max h-min h), forcetol 1e-12*F")
+
+
+def c3_problems(n=C3_N):
+    from contactmechanics_b200.Generation import self_affine
+    probs = []
+    for i in range(n):
+        rng = np.random.default_rng(i)
+        nx, ny = int(rng.choice(C3_SIDES)), int(rng.choice(C3_SIDES))
+        hurst = rng.uniform(0.3, 0.9)
+        slope = rng.uniform(0.05, 0.2)
+        p = 10 ** rng.uniform(-4, -2)
+        h = self_affine((nx, ny), (1.0, 1.0), hurst, slope, seed=i)
+        probs.append(((nx, ny), h, float(p)))
+    return probs
+
+
+def run_batched(fp64_subset=48):
+    """Mixed-precision batched solves/s of the 512-solve configuration, the
+    plain FP64 single-solve path on a subset of the same solves, and the
+    largest relative displacement difference between the two on that subset."""
+    import torch
+    import contactmechanics_b200 as cm
+    probs = c3_problems()
+    subs = [cm.PeriodicFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0)) for nb, _, _ in probs]
+    hs = [torch.from_numpy(h).cuda() for _, h, _ in probs]
+    F = [p for _, _, p in probs]
+    PT = [1e-9 * float(h.max() - h.min()) for _, h, _ in probs]
+    FT = [1e-12 * p for p in F]
+
+    def batch():
+        return cm.constrained_conjugate_gradients_batch(subs, hs, external_force=F, pentol=PT,
+                                                        forcetol=FT, precision="mixed")
+    batch()  # warm-up: allocations, graphs
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = batch()
+    e1.record()
+    e1.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    assert all(r.success for r in res)
+    idx = list(range(0, C3_N, C3_N // fp64_subset))[:fp64_subset]
+    for i in idx[:4]:  # warm-up of the single-solve path
+        cm.constrained_conjugate_gradients(subs[i], hs[i], external_force=F[i], pentol=PT[i],
+                                           forcetol=FT[i], precision="fp64")
+    torch.cuda.synchronize()
+    e0.record()
+    single = [cm.constrained_conjugate_gradients(subs[i], hs[i], external_force=F[i], pentol=PT[i],
+                                                 forcetol=FT[i], precision="fp64") for i in idx]
+    e1.record()
+    e1.synchronize()
+    ms_single = e0.elapsed_time(e1)
+    errs = []
+    for i, r in zip(idx, single):
+        nb = subs[i].nb_grid_pts
+        a, b = res[i].x[:nb[0], :nb[1]], r.x[:nb[0], :nb[1]]
+        errs.append(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)))
+    batched = C3_N / (ms_batch / 1e3)
+    single_rate = len(idx) / (ms_single / 1e3)
+    return {"workload": C3_WORKLOAD, "solves": C3_N,
+            "mixed_batched_solves_per_s": batched, "ms_batch": ms_batch,
+            "fp64_single_solve_solves_per_s": single_rate,
+            "fp64_single_solve_sample": f"{len(idx)} of the 512 solves (every {C3_N // fp64_subset}th)",
+            "speedup_vs_fp64_single": batched / single_rate, "rel_err_vs_fp64_max": max(errs),
+            "iterations_mean": float(np.mean([r.nit for r in res]))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,6 +387,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the 512-solve batched configuration")
     ap.add_argument("--profile-solve", choices=["mixed", "fp64", "fp32"], default=None,
                     help="run the first solve of the sweep once and exit (for profilers)")
     args = ap.parse_args()
@@ -350,6 +427,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     r = run_gpu(args, rank, world, local_rank)
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = run_batched()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -385,6 +465,7 @@ def main():
         "per_kernel_ms": {k: v["ms"] for k, v in r["per_kernel"].items()},
         "clocks": r["clocks"],
         "cpu_baseline": cpu,
+        "batched": batched,
     }
     print(json.dumps(line))
     return 0
