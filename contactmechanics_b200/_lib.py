@@ -90,6 +90,8 @@ SIGNATURES = {
     "cm_ccg_solve_batch": (_i, [_i, _vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp,
                                 ctypes.POINTER(CcgResult), _vp]),
     "cm_launch_count": (ctypes.c_ulonglong, []),
+    "cm_apply_periodic_noalloc": (_i, [_i, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, _i, _vp, _vp, _vp]),
     "cm_ccg_profile": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _i,
                             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i),
                             ctypes.POINTER(ctypes.c_char_p)]),

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1127,6 +1128,69 @@ static int status_error(const CcgState& st) {
 }
 
 // ---------------------------------------------------------------------------
+// periodic operator that allocates nothing
+// ---------------------------------------------------------------------------
+// Scratch of cm_apply_periodic_noalloc: a fixed 4 MiB array in the library's
+// own device memory (every GPU that loads the library holds it until exit).
+// It fits a periodic grid of up to 512 x 512 points.  Layout, in order:
+// slot descriptor, work list, twiddles (x then y), tiled Green's table,
+// spectrum.  Every call rewrites each part it reads, so nothing has to start
+// at zero; calls that overlap on the GPU (two streams, or two host threads)
+// share the array and race.
+#define CM_NOALLOC_MAX_SIDE 512
+#define CM_NOALLOC_BYTES (4u << 20)
+#define CM_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CM_NOALLOC_BYTES];
+
+static void* g_noalloc_addr[CM_NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mu;
+
+// device address of the scratch on the current device (resolved once)
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= CM_NOALLOC_MAX_DEVICES) return CM_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_addr[dev] = ptr;
+  }
+  *out = (unsigned char*)g_noalloc_addr[dev];
+  return CM_OK;
+}
+
+__global__ void k_noalloc_setup(Slot<double>* slot, Slot<double> sv, int2* items, int nitems,
+                                double2* twx, int nx, double2* twy, int ny) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i0 == 0) *slot = sv;
+  for (long i = i0; i < nitems; i += stride) items[i] = make_int2(0, (int)i);
+  for (long i = i0; i < nx; i += stride) {
+    double sn, cs;
+    sincospi(-2.0 * (double)i / (double)nx, &sn, &cs);
+    twx[i] = make_double2(cs, sn);
+  }
+  for (long i = i0; i < ny; i += stride) {
+    double sn, cs;
+    sincospi(-2.0 * (double)i / (double)ny, &sn, &cs);
+    twy[i] = make_double2(cs, sn);
+  }
+}
+
+// one scaled operator table (-G/(aN) or -K a/N) in the tiled spectrum layout
+__global__ void k_noalloc_table(const double* G, double* tab, int nx, int nyh, int lw, int op,
+                                double aN_inv, double a_over_N) {
+  const long n = (long)nx * nyh;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i / nyh), k = (int)(i % nyh);
+    const double g = G[i];
+    const double v = (op == CM_OP_DISP) ? -g * aN_inv : -((g != 0.0) ? 1.0 / g : 0.0) * a_over_N;
+    tab[spec_at(x, k, nx, lw)] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -1444,6 +1508,67 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
 }
 
 unsigned long long cm_launch_count(void) { return g_launches; }
+
+int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young, double poisson,
+                              int op, const double* in, double* out, void* stream) {
+  if (!in || !out || (op != CM_OP_DISP && op != CM_OP_FORCE)) return CM_ERR_ARG;
+  if (nx < 2 || ny < 2 || !(sx > 0) || !(sy > 0) || !(young > 0)) return CM_ERR_ARG;
+  if (nx > CM_NOALLOC_MAX_SIDE || ny > CM_NOALLOC_MAX_SIDE) return CM_ERR_SIZE;
+  FftDesc fx, fy;
+  if (!make_fft_desc(nx, &fx) || !make_fft_desc(ny, &fy)) return CM_ERR_SIZE;
+  const int nyh = ny / 2 + 1;
+  Tiles T;
+  CKS(choose_tiles(nx, ny, nyh, nx, ny, sizeof(double2), &T));
+  // carve the scratch
+  unsigned char* base = nullptr;
+  CKS(noalloc_scratch(&base));
+  const int nt_row = (nx + T.row_tile - 1) / T.row_tile;
+  const int nitems = std::max(nt_row, T.ntile_cols);
+  const size_t ncols = (size_t)T.ntile_cols * T.col_tile;
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  size_t off = 0;
+  const size_t o_slot = off; off = up(off + sizeof(Slot<double>));
+  const size_t o_items = off; off = up(off + sizeof(int2) * nitems);
+  const size_t o_twx = off; off = up(off + sizeof(double2) * nx);
+  const size_t o_twy = off; off = up(off + sizeof(double2) * ny);
+  const size_t o_tab = off; off = up(off + sizeof(double) * nx * ncols);
+  const size_t o_spec = off; off = up(off + sizeof(double2) * nx * ncols);
+  if (off > CM_NOALLOC_BYTES) return CM_ERR_SIZE;
+  Slot<double>* d_slot = (Slot<double>*)(base + o_slot);
+  int2* d_items = (int2*)(base + o_items);
+  double2* d_twx = (double2*)(base + o_twx);
+  double2* d_twy = (double2*)(base + o_twy);
+  double* d_tab = (double*)(base + o_tab);
+  double2* d_spec = (double2*)(base + o_spec);
+  double* d_G = (double*)d_spec;  // the unscaled table lives in the spectrum until the transform
+  Slot<double> sv;
+  memset(&sv, 0, sizeof(sv));
+  sv.nx = nx; sv.ny = ny; sv.nyh = nyh; sv.tx = nx; sv.ty = ny;
+  sv.row_tile = T.row_tile; sv.col_tile = T.col_tile; sv.lw = T.lw; sv.comp_rows = T.comp_rows;
+  sv.nt_rowt = nt_row; sv.nt_rowd = nt_row; sv.nt_col = T.ntile_cols; sv.nt_comp = 0;
+  sv.fx = fx; sv.fy = fy; sv.twx = d_twx; sv.twy = d_twy; sv.spec = d_spec;
+  sv.tab[0] = d_tab; sv.tab[1] = d_tab; sv.table_sel = 0;
+  sv.in = in; sv.out = out;
+  sv.in_rows = nx; sv.in_cols = ny; sv.in_ld = ny;
+  sv.out_rows = nx; sv.out_cols = ny; sv.out_ld = ny;
+  cudaStream_t s = (cudaStream_t)stream;
+  set_smem_attrs<double>();
+  const long nh = (long)nx * nyh;
+  k_noalloc_setup<<<grid_for(std::max<long>(nitems, std::max(nx, ny))), 256, 0, s>>>(
+      d_slot, sv, d_items, nitems, d_twx, nx, d_twy, ny);
+  const double Es = young / (1 - poisson * poisson);
+  k_table_periodic<<<grid_for(nh), 256, 0, s>>>(d_G, nx, ny, nyh, sx, sy, Es, young, poisson,
+                                                 CM_Q0_DEFAULT, 0.0, 0.0, 2);
+  const double area = (sx / nx) * (sy / ny);
+  const double N = (double)nx * (double)ny;
+  k_noalloc_table<<<grid_for(nh), 256, 0, s>>>(d_G, d_tab, nx, nyh, T.lw, op, 1.0 / (area * N), area / N);
+  k_row_fwd<double, MODE_PLAIN><<<nt_row, T.threads_row, T.smem_row, s>>>(d_slot, d_items);
+  k_col<double, MODE_PLAIN><<<T.ntile_cols, T.threads_col, T.smem_col, s>>>(d_slot, d_items);
+  k_row_inv<double, MODE_PLAIN><<<nt_row, T.threads_row, T.smem_row, s>>>(d_slot, d_items);
+  g_launches += 6;
+  CK(cudaGetLastError());
+  return CM_OK;
+}
 
 int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int iters,
                    float* ms_per_kernel, int* n_kernels, const char** names) {

@@ -199,6 +199,26 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
                        cm_ccg_result* res, void* stream);
 
 /*
+ * The periodic operator (evaluate_disp or evaluate_force of a 2D periodic
+ * half-space with the default q = 0 stiffness, FP64) for callers that must
+ * not allocate device memory: code that runs where the host application
+ * owns every device allocation through its own pool, or inside a loop that
+ * cannot afford the device-wide synchronisation cudaMalloc may cause.  No
+ * plan is needed and nothing is allocated: the Green's table, twiddles and
+ * spectrum are built in a fixed 4 MiB array that the library keeps in device
+ * memory (each GPU that loads the library holds it until the process exits),
+ * so nx and ny are limited to 512; larger grids return CM_ERR_SIZE.  in_dev
+ * and out_dev are caller-owned (nx, ny) FP64 device arrays; work is enqueued
+ * on `stream` (NULL: the legacy default stream).  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race and corrupt each other's results.
+ * This entry point has no counterpart in the reference.
+ */
+int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young, double poisson,
+                              int op, const double* in_dev, double* out_dev, void* stream);
+
+/*
  * Number of kernels this library has launched in the process (graph nodes
  * count once per replay).  Instrumentation; no reference counterpart.
  */
