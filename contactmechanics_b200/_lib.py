@@ -89,6 +89,12 @@ SIGNATURES = {
                                _vp, ctypes.POINTER(CcgResult)]),
     "cm_ccg_solve_batch": (_i, [_i, _vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp,
                                 ctypes.POINTER(CcgResult), _vp]),
+    "cm_stepper_create": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cm_stepper_destroy": (_i, [_vp]),
+    "cm_ccg_begin": (_i, [_vp, _vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp]),
+    "cm_ccg_step": (_i, [_vp, _i, _vp, _i, ctypes.POINTER(_i)]),
+    "cm_ccg_handover": (_i, [_vp, _vp, _vp, ctypes.POINTER(_i)]),
+    "cm_ccg_end": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(CcgResult)]),
     "cm_launch_count": (ctypes.c_ulonglong, []),
     "cm_apply_periodic_noalloc": (_i, [_i, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, _i, _vp, _vp, _vp]),

@@ -429,6 +429,11 @@ struct cm_plan {
   Work<double> w64;
   CcgState* h_state = nullptr;  // pinned readback
   std::vector<void*> allocs;
+  // stepping interface: phase of the solve this plan holds
+  int phase = 0;          // 0 none, 1 FP32, 2 FP64
+  int phase_prec = 0;     // CM_FP32 / CM_FP64 / CM_MIXED of the solve
+  int nit32 = 0, nfev32 = 0;
+  cm_ccg_params params{};
 };
 
 template <typename R> static Work<R>& work_of(cm_plan* p);
@@ -1128,6 +1133,114 @@ static int status_error(const CcgState& st) {
 }
 
 // ---------------------------------------------------------------------------
+// stepping interface (continuous batching)
+// ---------------------------------------------------------------------------
+// Reusable device and pinned host buffers of a stepper: slot descriptors and
+// work lists of the solves advanced together in one step.
+struct cm_stepper {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t cap_slots = 0, cap_items = 0;
+  void* d_slots = nullptr;       // Slot<float> or Slot<double> array
+  int2* d_items[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* d_done = nullptr;
+  void* h_slots = nullptr;       // pinned staging
+  int2* h_items = nullptr;
+  int* h_done = nullptr;
+  size_t cap_h_items = 0;
+};
+
+static void stepper_free(cm_stepper* st) {
+  cudaFree(st->d_slots);
+  for (int k = 0; k < 4; ++k) cudaFree(st->d_items[k]);
+  cudaFree(st->d_done);
+  cudaFreeHost(st->h_slots);
+  cudaFreeHost(st->h_items);
+  cudaFreeHost(st->h_done);
+  st->d_slots = nullptr;
+  for (int k = 0; k < 4; ++k) st->d_items[k] = nullptr;
+  st->d_done = nullptr;
+  st->h_slots = nullptr;
+  st->h_items = nullptr;
+  st->h_done = nullptr;
+  st->cap_slots = st->cap_items = st->cap_h_items = 0;
+}
+
+// grow the buffers to n slots (of the larger slot type) and `items` entries per list
+static int stepper_reserve(cm_stepper* st, size_t n, size_t items) {
+  if (n <= st->cap_slots && items <= st->cap_items) return CM_OK;
+  CK(cudaStreamSynchronize(st->stream));
+  const size_t ns = std::max(n, st->cap_slots * 2), ni = std::max(items, st->cap_items * 2);
+  stepper_free(st);
+  const size_t slot_bytes = std::max(sizeof(Slot<float>), sizeof(Slot<double>));
+  if (cudaMalloc(&st->d_slots, slot_bytes * ns) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  for (int k = 0; k < 4; ++k)
+    if (cudaMalloc(&st->d_items[k], sizeof(int2) * ni) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  if (cudaMalloc(&st->d_done, sizeof(int) * ns) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  if (cudaMallocHost(&st->h_slots, slot_bytes * ns) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  if (cudaMallocHost(&st->h_items, sizeof(int2) * ni * 4) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  if (cudaMallocHost(&st->h_done, sizeof(int) * ns) != cudaSuccess) { cudaGetLastError(); return CM_ERR_OOM; }
+  st->cap_slots = ns;
+  st->cap_items = ni;
+  return CM_OK;
+}
+
+template <typename R>
+__global__ void k_collect_done(const Slot<R>* __restrict__ slots, int n, int* done) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    done[i] = slots[i].st->done;
+}
+
+// Advance the solves of one precision by `iters` iterations; done flags to h_done[off..].
+template <typename R>
+static int stepper_run(cm_stepper* stp, const std::vector<cm_plan*>& plans, int iters, int* done_out) {
+  const int n = (int)plans.size();
+  if (n == 0) return CM_OK;
+  cudaStream_t s = stp->stream;
+  set_smem_attrs<R>();
+  size_t ni[4] = {0, 0, 0, 0};
+  bool bisect = false;
+  for (cm_plan* p : plans) {
+    Work<R>& w = work_of<R>(p);
+    ni[0] += w.nt_comp; ni[1] += w.nt_rowt; ni[2] += w.nt_rowd; ni[3] += w.nt_col;
+    bisect = bisect || (p->params.has_hardness && p->params.load_control);
+  }
+  CKS(stepper_reserve(stp, n, std::max({ni[0], ni[1], ni[2], ni[3], (size_t)1})));
+  Slot<R>* hs = (Slot<R>*)stp->h_slots;
+  int2* hi[4];
+  for (int k = 0; k < 4; ++k) hi[k] = stp->h_items + k * stp->cap_items;
+  size_t c[4] = {0, 0, 0, 0};
+  BatchDev<R> b;  // views into the stepper's buffers (owns nothing)
+  for (int i = 0; i < n; ++i) {
+    Work<R>& w = work_of<R>(plans[i]);
+    hs[i] = base_slot(plans[i], w);
+    for (int t = 0; t < hs[i].nt_comp; ++t) hi[0][c[0]++] = make_int2(i, t);
+    for (int t = 0; t < hs[i].nt_rowt; ++t) hi[1][c[1]++] = make_int2(i, t);
+    for (int t = 0; t < hs[i].nt_rowd; ++t) hi[2][c[2]++] = make_int2(i, t);
+    for (int t = 0; t < hs[i].nt_col; ++t) hi[3][c[3]++] = make_int2(i, t);
+    b.smem_row = std::max(b.smem_row, w.tiles.smem_row);
+    b.smem_col = std::max(b.smem_col, w.tiles.smem_col);
+  }
+  CK(cudaMemcpyAsync(stp->d_slots, hs, sizeof(Slot<R>) * n, cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < 4; ++k) {
+    CK(cudaMemcpyAsync(stp->d_items[k], hi[k], sizeof(int2) * c[k], cudaMemcpyHostToDevice, s));
+    b.items[k] = stp->d_items[k];
+    b.n_items[k] = (int)c[k];
+  }
+  b.slots = (Slot<R>*)stp->d_slots;
+  for (int it = 0; it < iters; ++it) launch_iteration_batch<R>(b, bisect, s);
+  g_launches += (unsigned long long)iters * iteration_launches(bisect) + 1;
+  k_collect_done<R><<<grid_for(n), 256, 0, s>>>(b.slots, n, stp->d_done);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(stp->h_done, stp->d_done, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int i = 0; i < n; ++i) done_out[i] = stp->h_done[i];
+  b.slots = nullptr;
+  for (int k = 0; k < 4; ++k) b.items[k] = nullptr;
+  return CM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // periodic operator that allocates nothing
 // ---------------------------------------------------------------------------
 // Scratch of cm_apply_periodic_noalloc: a fixed 4 MiB array in the library's
@@ -1508,6 +1621,123 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
 }
 
 unsigned long long cm_launch_count(void) { return g_launches; }
+
+int cm_stepper_create(void* stream, cm_stepper** out) {
+  if (!out) return CM_ERR_ARG;
+  cm_stepper* st = new (std::nothrow) cm_stepper();
+  if (!st) return CM_ERR_OOM;
+  if (stream) {
+    st->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreate(&st->stream) != cudaSuccess) { delete st; return CM_ERR_CUDA; }
+    st->own_stream = true;
+  }
+  *out = st;
+  return CM_OK;
+}
+
+int cm_stepper_destroy(cm_stepper* st) {
+  if (!st) return CM_OK;
+  if (st->stream) cudaStreamSynchronize(st->stream);
+  stepper_free(st);
+  if (st->own_stream) cudaStreamDestroy(st->stream);
+  delete st;
+  return CM_OK;
+}
+
+int cm_ccg_begin(cm_stepper* stp, cm_plan* p, const cm_ccg_params* prm, const double* h,
+                 const double* u0, const double* f0) {
+  if (!stp || !p || !prm || !h || prm->maxiter < 1) return CM_ERR_ARG;
+  if (prm->precision != CM_FP64 && prm->precision != CM_FP32 && prm->precision != CM_MIXED) return CM_ERR_ARG;
+  if (prm->has_hardness && !(prm->hardness > 0)) return CM_ERR_ARG;
+  if (p->phase != 0) return CM_ERR_ARG;  // the plan already holds a solve
+  p->params = *prm;
+  p->phase_prec = prm->precision;
+  p->nit32 = p->nfev32 = 0;
+  SolveInput in{h, u0, f0, p->ny};
+  if (prm->precision == CM_FP64) {
+    CKS(ccg_init<double>(p, p->w64, prm, in, 0.0, 0.0, prm->maxiter, stp->stream));
+    p->phase = 2;
+  } else {
+    const bool mixed = prm->precision == CM_MIXED;
+    const double rp = mixed ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
+    const int mi = mixed ? std::min(prm->maxiter, CM_FP32_ITER_CAP) : prm->maxiter;
+    CKS(ccg_init<float>(p, p->w32, prm, in, rp, mixed ? 1e-5 : 0.0, mi, stp->stream));
+    p->phase = 1;
+  }
+  return CM_OK;
+}
+
+int cm_ccg_step(cm_stepper* stp, int n, cm_plan* const* plans, int iters, int* done) {
+  if (!stp || n < 0 || (n > 0 && (!plans || !done)) || iters < 1) return CM_ERR_ARG;
+  std::vector<cm_plan*> g32, g64;
+  std::vector<int> i32, i64;
+  for (int i = 0; i < n; ++i) {
+    if (!plans[i] || plans[i]->phase == 0) return CM_ERR_ARG;
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return CM_ERR_ARG;
+    if (plans[i]->phase == 1) { g32.push_back(plans[i]); i32.push_back(i); }
+    else { g64.push_back(plans[i]); i64.push_back(i); }
+  }
+  std::vector<int> d32(g32.size()), d64(g64.size());
+  CKS(stepper_run<float>(stp, g32, iters, d32.data()));
+  CKS(stepper_run<double>(stp, g64, iters, d64.data()));
+  for (size_t k = 0; k < g32.size(); ++k) done[i32[k]] = d32[k];
+  for (size_t k = 0; k < g64.size(); ++k) done[i64[k]] = d64[k];
+  return CM_OK;
+}
+
+int cm_ccg_handover(cm_stepper* stp, cm_plan* p, const double* h, int* finished) {
+  if (!stp || !p || !h || !finished) return CM_ERR_ARG;
+  cudaStream_t s = stp->stream;
+  *finished = 0;
+  if (p->phase == 1) {
+    CK(cudaMemcpyAsync(p->h_state, p->w32.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const CcgState st = *p->h_state;
+    if (!st.done) return CM_ERR_ARG;
+    const int err = status_error(st);
+    if (err != CM_OK) { p->phase = 0; return err; }
+    if (p->phase_prec == CM_FP32) { *finished = 1; return CM_OK; }
+    p->nit32 = st.it;
+    p->nfev32 = st.nfev;
+    CKS(ensure_ccg(p, p->w64));
+    k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
+        p->w32.f[st.parity], p->tx, p->ty, p->w64.u, p->nx, p->ny);
+    SolveInput in{h, nullptr, p->w64.u, p->ny};
+    CKS(ccg_init<double>(p, p->w64, &p->params, in, 0.0, 0.0,
+                         std::max(1, p->params.maxiter - st.it), s));
+    p->phase = 2;
+    return CM_OK;
+  }
+  if (p->phase == 2) {
+    *finished = 1;
+    return CM_OK;
+  }
+  return CM_ERR_ARG;
+}
+
+int cm_ccg_end(cm_stepper* stp, cm_plan* p, double* x, double* jac, unsigned char* active,
+               unsigned char* plastic, cm_ccg_result* res) {
+  if (!stp || !p || !res || p->phase == 0) return CM_ERR_ARG;
+  memset(res, 0, sizeof(*res));
+  CcgState st;
+  int rc;
+  if (p->phase == 1) rc = finish_ccg<float>(p, p->w32, x, jac, active, plastic, &st, stp->stream);
+  else rc = finish_ccg<double>(p, p->w64, x, jac, active, plastic, &st, stp->stream);
+  p->phase = 0;
+  if (rc != CM_OK) return rc;
+  CKS(status_error(st));
+  fill_result(st, res);
+  if (p->phase_prec == CM_MIXED) {
+    res->nit += p->nit32;
+    res->nfev += p->nfev32;
+    res->nit_fp32 = p->nit32;
+  } else if (p->phase_prec == CM_FP32) {
+    res->nit_fp32 = st.it;
+  }
+  return CM_OK;
+}
 
 int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young, double poisson,
                               int op, const double* in, double* out, void* stream) {

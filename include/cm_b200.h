@@ -199,6 +199,33 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
                        cm_ccg_result* res, void* stream);
 
 /*
+ * Stepping interface for continuous batching.  A stepper owns a stream and
+ * reusable staging buffers.  Each in-flight solve lives on its own plan:
+ *   cm_ccg_begin     set up a solve on a free plan (FP32 phase for CM_FP32 and
+ *                    CM_MIXED, FP64 phase for CM_FP64)
+ *   cm_ccg_step      advance any set of in-flight solves (different sizes and
+ *                    phases) by `iters` iterations each, together; done[i] tells
+ *                    whether solve i has finished its current phase
+ *   cm_ccg_handover  for a solve whose phase finished: CM_MIXED moves from the
+ *                    FP32 phase to the FP64 refinement (*finished = 0); otherwise
+ *                    *finished = 1
+ *   cm_ccg_end       write the results and free the plan for the next solve
+ * Together they run constrained_conjugate_gradients
+ * (ConstrainedConjugateGradients.py:47-509) in pieces, so that a request loop
+ * can admit and retire solves between steps; a solve's result does not depend
+ * on which others share its steps.
+ */
+typedef struct cm_stepper cm_stepper;
+int cm_stepper_create(void* stream, cm_stepper** out);
+int cm_stepper_destroy(cm_stepper* stepper);
+int cm_ccg_begin(cm_stepper* stepper, cm_plan* plan, const cm_ccg_params* params,
+                 const double* heights_dev, const double* init_disp_dev, const double* init_force_dev);
+int cm_ccg_step(cm_stepper* stepper, int n, cm_plan* const* plans, int iters, int* done);
+int cm_ccg_handover(cm_stepper* stepper, cm_plan* plan, const double* heights_dev, int* finished);
+int cm_ccg_end(cm_stepper* stepper, cm_plan* plan, double* x_dev, double* jac_dev,
+               unsigned char* active_dev, unsigned char* plastic_dev, cm_ccg_result* res);
+
+/*
  * The periodic operator (evaluate_disp or evaluate_force of a 2D periodic
  * half-space with the default q = 0 stiffness, FP64) for callers that must
  * not allocate device memory: code that runs where the host application
