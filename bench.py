@@ -279,9 +279,12 @@ def run_gpu(args, rank, world, local_rank):
     # the persistent solver kernel runs whole iterations: its unit is one
     # iteration and its algorithmic bytes are the iteration's compulsory bytes
     kb["k_ccg_persist"] = iteration_bytes(nxd, nyd, n, n)
-    per_kernel = {}
+    per_kernel, phases = {}, {}
     for i in range(nk.value):
         name = names[i].decode()
+        if ":" in name:  # a phase inside the persistent kernel
+            phases[name.split(":", 1)[1]] = float(ms_k[i])
+            continue
         per_kernel[name] = {"ms": float(ms_k[i]), "bytes": kb.get(name)}
     dom = max(per_kernel, key=lambda k: per_kernel[k]["ms"])
     peak, peak_kind = peaks()
@@ -301,7 +304,7 @@ def run_gpu(args, rank, world, local_rank):
                   "ms_per_launch": per_kernel[dom]["ms"]},
         iteration_roofline={"bytes": b_iter, "ms": t_iter * 1e3,
                             "achieved": b_iter / t_iter / 1e9, "frac": b_iter / t_iter / 1e9 / peak},
-        per_kernel=per_kernel,
+        per_kernel=per_kernel, phases=phases,
         h2d=h.nbytes + nxd * nyd * 8, d2h=nxd * nyd * 8 + h.nbytes + nxd * nyd)
 
 
@@ -380,6 +383,78 @@ def run_batched(fp64_subset=48):
             "iterations_mean": float(np.mean([r.nit for r in res]))}
 
 
+# ---------------------------------------------------------------------------
+# serving: Poisson request stream through the continuous-batching loop
+# ---------------------------------------------------------------------------
+SERVE_SIDES = (64, 96, 128, 192, 256, 384, 512, 768, 1024)
+SERVE_WORKLOAD = ("Poisson arrivals {rate:g} req/s for {dur:g} s; side log-uniform 64..1024 rounded "
+                  "to {{64,96,128,192,256,384,512,768,1024}}; 30% free (domain x2), 20% plastic "
+                  "with hardness U[0.02,0.1] E*; mean pressure log-uniform 1e-4..1e-2 E*; rough "
+                  "surfaces H 0.8 slope 0.1 from 8 seeds per size; pentol 1e-9*(max h-min h)")
+
+
+def run_serving(rate=20.0, duration=10.0, seed=7):
+    """p50 / p99 latency (arrival to result) and solves/s of a bounded request
+    stream (scaled down from 2000 req/s for 60 s with sides up to 4096)."""
+    import torch
+    from contactmechanics_b200.Generation import self_affine
+    from contactmechanics_b200.Serving import ContactServer
+    rng = np.random.default_rng(seed)
+    n = int(rate * duration)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    logs = rng.uniform(np.log(64), np.log(1024), n)
+    sides = [min(SERVE_SIDES, key=lambda s: abs(np.log(s) - v)) for v in logs]
+    surfaces = {}
+
+    def surface(side, k):
+        if (side, k) not in surfaces:
+            surfaces[(side, k)] = torch.from_numpy(
+                self_affine((side, side), (1.0, 1.0), 0.8, 0.1, seed=1000 * side + k)).cuda()
+        return surfaces[(side, k)]
+    reqs = []
+    for i in range(n):
+        side = sides[i]
+        kind = "free" if rng.random() < 0.3 else "periodic"
+        plastic = rng.random() < 0.2
+        p = 10 ** rng.uniform(-4, -2)
+        h = surface(side, int(rng.integers(8)))
+        span = float(h.max() - h.min())
+        kw = dict(external_force=p, pentol=1e-9 * span, forcetol=1e-12 * p, maxiter=20000)
+        if plastic:
+            kw["hardness"] = rng.uniform(0.02, 0.1) / (side * side)
+            kw["forcetol"] = 1e-9 * p
+        reqs.append((arrivals[i], kind, side, h, kw))
+    srv = ContactServer(iters_per_step=8)
+    # warm-up: one request of every size and kind, so plans and kernels exist
+    for side in SERVE_SIDES:
+        for kind in ("periodic", "free"):
+            h = surface(side, 0)
+            srv.submit(kind, (side, side), (1.0, 1.0), h, external_force=1e-3,
+                       pentol=1e-9 * float(h.max() - h.min()), forcetol=1e-15)
+    srv.run_until_idle(timeout=300)
+    srv.completed.clear()
+    torch.cuda.synchronize()
+    handles = []
+    t0 = time.perf_counter()
+    srv.start()
+    for at, kind, side, h, kw in reqs:
+        now = time.perf_counter() - t0
+        if at > now:
+            time.sleep(at - now)
+        handles.append(srv.submit(kind, (side, side), (1.0, 1.0), h, arrival=t0 + at, **kw))
+    for hd in handles:
+        hd.done_event.wait(600)
+    t1 = time.perf_counter()
+    srv.close()
+    ok = [hd for hd in handles if hd.error is None and hd.result_value is not None]
+    lat = np.array([hd.latency_s for hd in ok]) * 1e3
+    return {"workload": SERVE_WORKLOAD.format(rate=rate, dur=duration), "requests": n,
+            "completed": len(ok), "converged": int(sum(hd.result_value.success for hd in ok)),
+            "solves_per_s": len(ok) / (t1 - t0), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "steps": srv.steps,
+            "offered_req_per_s": rate, "precision": "mixed"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,6 +464,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the 512-solve batched configuration")
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-stream run")
     ap.add_argument("--profile-solve", choices=["mixed", "fp64", "fp32"], default=None,
                     help="run the first solve of the sweep once and exit (for profilers)")
     args = ap.parse_args()
@@ -427,9 +503,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     r = run_gpu(args, rank, world, local_rank)
-    batched = None
+    batched = serving = None
     if world == 1 and not args.no_batched:
         batched = run_batched()
+    if world == 1 and not args.no_serving:
+        serving = run_serving()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -463,9 +541,11 @@ def main():
         "roofline": r["roofline"],
         "iteration_roofline": r["iteration_roofline"],
         "per_kernel_ms": {k: v["ms"] for k, v in r["per_kernel"].items()},
+        "persist_phase_ms": r["phases"] or None,
         "clocks": r["clocks"],
         "cpu_baseline": cpu,
         "batched": batched,
+        "serving": serving,
     }
     print(json.dumps(line))
     return 0

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "lib", "libcm_b200.so")
-SOURCES = ["cm_plan.cu"]
+SOURCES = ["cm_plan.cu", "cm_p2.cu", "cm_persist_f32.cu", "cm_persist_f64.cu"]  # compiled in parallel
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,16 +36,32 @@ def build(force=False, ptxas_verbose=False):
     if not force and not _stale():
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", INCLUDE, "-o", OUT + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    objdir = os.path.join(os.path.dirname(OUT), "obj")
+    os.makedirs(objdir, exist_ok=True)
+    base = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE]
     if ptxas_verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    proc = subprocess.run(cmd, capture_output=True, text=True)
+        base.append("-Xptxas=-v")
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        objs.append(obj)
+        procs.append(subprocess.Popen(base + ["-c", os.path.join(CSRC, src), "-o", obj],
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    failed = False
+    for src, proc in zip(SOURCES, procs):
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(out + err)
+            failed = True
+        elif ptxas_verbose:
+            sys.stdout.write(err)
+    if failed:
+        raise RuntimeError("nvcc failed building libcm_b200.so")
+    link = [_nvcc(), *ARCH, "-shared", "-o", OUT + ".tmp"] + objs
+    proc = subprocess.run(link, capture_output=True, text=True)
     if proc.returncode != 0:
         sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError("nvcc failed building libcm_b200.so")
-    if ptxas_verbose:
-        sys.stdout.write(proc.stderr)
+        raise RuntimeError("nvcc failed linking libcm_b200.so")
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -5,6 +5,13 @@
 
 #define CM_DEVINL __device__ __forceinline__
 
+// Shared-memory index with one padding slot per 8 elements: the strided
+// Stockham writes (stride 4 or 8 elements across a warp) and the column
+// layouts of the power-of-two passes then hit distinct banks.  A buffer of
+// E elements needs smem_padded(E) slots.
+CM_DEVINL int spad(int e) { return e + (e >> 3); }
+__host__ __device__ inline int smem_padded(int e) { return e + (e >> 3) + 1; }
+
 template <typename R> struct CT;
 template <> struct CT<float> { typedef float2 C; };
 template <> struct CT<double> { typedef double2 C; };

@@ -26,12 +26,29 @@ struct P2Plan {
   static constexpr int NST = 1 + (LOGN - (LOGN % 3 == 0 ? 3 : LOGN % 3)) / 3;
 };
 
-// Shared-memory index with one padding slot per 8 elements: the strided
-// Stockham writes (stride 4 or 8 elements across a warp) and the column
-// layouts then hit distinct banks.  A buffer of E elements needs
-// smem_padded(E) slots.
-CM_DEVINL int spad(int e) { return e + (e >> 3); }
-__host__ __device__ inline int smem_padded(int e) { return e + (e >> 3) + 1; }
+
+// Twiddles of the radix-8 stages in shared memory, one table per stage:
+// stage s (Ns = FIRST * 8^(s-1) butterfly groups) holds
+// tw[toff(s) + (q-1)*Ns + k] = W^(q k N/(8 Ns)), W = exp(-2 pi i / N), for
+// q = 1..7, k < Ns, so the threads of a warp (consecutive k, or a shared k)
+// read consecutive words or one broadcast word.  The stage tables sum to at
+// most N entries.  Built from the length-N table tw_n[m] = W^m, so every
+// value is an entry of that table.
+template <int LOGN, typename C>
+CM_DEVINL void stage_tw_p2(C* tws, const C* __restrict__ tw_n) {
+  typedef P2Plan<LOGN> P;
+  constexpr int N = P::N;
+  int toff = 0;
+#pragma unroll
+  for (int s = 1, Ns = P::FIRST; s < P::NST; ++s, Ns *= 8) {
+    const int step = N / (Ns * 8);
+    for (int i = threadIdx.x; i < 7 * Ns; i += blockDim.x) {
+      const int q = 1 + i / Ns, k = i & (Ns - 1);
+      tws[toff + i] = __ldg(tw_n + ((q * k * step) & (N - 1)));
+    }
+    toff += 7 * Ns;
+  }
+}
 
 template <bool INV, int R, typename C>
 CM_DEVINL void dft_r(C* v) {
@@ -46,8 +63,8 @@ CM_DEVINL void dft_r(C* v) {
 
 // Transform the thread's 8 elements in place.  Sequence layout in shared
 // memory: element i of this thread's sequence at buf[spad(base + i*estride)];
-// sA / sB are the two ping-pong buffers; tw: twiddle table exp(-2 pi i m / N)
-// in shared memory.  Ends with the result in v and no pending shared-memory
+// sA / sB are the two ping-pong buffers; tw: the stage tables of
+// stage_tw_p2 in shared memory.  Ends with the result in v and no pending shared-memory
 // reads (a barrier is needed before reusing sA/sB).
 template <typename C, bool INV, int LOGN>
 CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int base, int estride, int tt, const C* tw) {
@@ -85,18 +102,19 @@ CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int base, int estride, int tt, co
   C* src = sA;
   C* dst = sB;
   int Ns = P::FIRST;
+  int toff = 0;
 #pragma unroll
   for (int s = 1; s < P::NST; ++s) {
     const int k = tt & (Ns - 1);
     C g[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) g[q] = src[spad(base + (tt + q * P::TPS) * estride)];
-    const int step = N / (Ns * 8);
 #pragma unroll
     for (int q = 1; q < 8; ++q) {
-      const C w = tw[(q * k * step) & (N - 1)];
+      const C w = tw[toff + (q - 1) * Ns + k];
       g[q] = INV ? cmulc(g[q], w) : cmul(g[q], w);
     }
+    toff += 7 * Ns;
     Dft<INV, 8, C>::run(g, nullptr, 8);
     if (s == P::NST - 1) {
       // last stage: output index tt + q*N/8, i.e. the thread's own elements

@@ -16,11 +16,6 @@
 #define CM_P2_MIN 6
 #define CM_P2_MAX 12
 
-template <typename C>
-CM_DEVINL void stage_tw(C* tws, const C* __restrict__ tw, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tws[i] = __ldg(tw + i);
-}
-
 template <typename R, int MODE, int LOGN>
 __global__ void __launch_bounds__(sizeof(R) == 8 ? CM_FFT_THREADS / 2 : CM_FFT_THREADS)
 k_row_fwd_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
@@ -43,7 +38,7 @@ k_row_fwd_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded((row_tile >> 1) * N);
-  stage_tw(tws, Sp->twy, N);
+  stage_tw_p2<LOGN>(tws, Sp->twy);
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int xa = x0 + 2 * s;
   const bool va_ok = xa < x0 + nrows, vb_ok = xa + 1 < x0 + nrows;
@@ -163,7 +158,7 @@ k_col_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(N * W);
-  stage_tw(tws, Sp->twx, N);
+  stage_tw_p2<LOGN>(tws, Sp->twx);
   const int c = threadIdx.x & (W - 1), tt = threadIdx.x >> lw;
   C* __restrict__ blk = Sp->spec + (size_t)item.y * N * W;
   const R* __restrict__ tblk = Sp->tab[0] + (size_t)item.y * N * W;
@@ -214,7 +209,7 @@ k_row_inv_p2(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded((row_tile >> 1) * N);
-  stage_tw(tws, Sp->twy, N);
+  stage_tw_p2<LOGN>(tws, Sp->twy);
   const C* __restrict__ spec = Sp->spec;
   struct XY { C X, Y; };
   batched_loop<4>(npairs * nyh, [&](int e) {

@@ -1,0 +1,60 @@
+// Host-side declarations shared by the translation units of the library:
+// launchers of the power-of-two FFT passes (cm_p2.cu) and the persistent
+// solver kernel (cm_persist.cu), and the types their callers need.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "cm_slot.cuh"
+
+#define CMS_TIMEOUT 6  // solve status: a grid-barrier wait gave up
+
+// Grid barrier of the persistent kernel (zeroed before every launch).
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+  unsigned int abort;
+  unsigned int pad;
+};
+
+// Phases of one iteration as timed by the persistent kernel's stamps buffer.
+enum PersistPhase {
+  PH_BEGIN, PH_BISECT, PH_GSUM, PH_ROW_FWD_T, PH_COL_T, PH_ROW_INV_T, PH_UPDATE, PH_ROW_FWD_F,
+  PH_COL_F, PH_ROW_INV_F, PH_COUNT
+};
+
+#define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+
+// Launch one power-of-two pass of the CCG iteration (MODE_T or MODE_F) for
+// sides 2^logn; false if logn has no specialisation.
+template <typename R, int MODE>
+bool p2_row_fwd(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
+                const int2* it);
+template <typename R, int MODE>
+bool p2_col(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
+            const int2* it);
+template <typename R, int MODE>
+bool p2_row_inv(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
+                const int2* it);
+// Shared-memory attributes of every power-of-two pass (once per process).
+template <typename R>
+void set_p2_attrs();
+
+// Dynamic shared memory of the persistent kernel for sides n: twiddles, the
+// transform's two ping-pong buffers and two column-tile stages (each
+// 128-byte aligned).
+template <typename R>
+inline size_t persist_smem_bytes(int n, int row_tile, int col_tile) {
+  const size_t csize = 2 * sizeof(R);
+  int e = (row_tile / 2) * n;
+  if (col_tile * n > e) e = col_tile * n;
+  const size_t ebuf = (size_t)(e + (e >> 3) + 1);
+  const size_t head = ((n + 2 * ebuf) * csize + 127) & ~(size_t)127;
+  const size_t stage = ((size_t)n * col_tile * (csize + sizeof(R)) + 127) & ~(size_t)127;
+  return head + 2 * stage;
+}
+
+// Host stub of the persistent kernel for square 2^logn domains, or nullptr.
+// Kernel arguments: (const Slot<R>*, GridBarrier*, int max_iters,
+// int bisect_passes, unsigned long long* stamps).
+template <typename R>
+const void* persist_kernel(int logn);

@@ -21,15 +21,80 @@
 #pragma once
 #include "cm_kernels_p2.cuh"
 
-#define CM_BARRIER_TIMEOUT_CYCLES 4000000000LL  // about two seconds
-#define CMS_TIMEOUT 6
+#include "cm_launch.h"
 
-struct GridBarrier {
-  unsigned int count;
-  unsigned int gen;
-  unsigned int abort;
-  unsigned int pad;
-};
+#define CM_BARRIER_TIMEOUT_CYCLES 4000000000LL  // about two seconds
+#ifndef CM_BARRIER_SLEEP_NS
+#define CM_BARRIER_SLEEP_NS 32  // back-off between polls of the barrier word
+#endif
+#ifndef CM_PERSIST_MIN_BLOCKS_F
+#define CM_PERSIST_MIN_BLOCKS_F 1  // resident blocks per SM the FP32 kernel is compiled for
+#endif
+#ifndef CM_PERSIST_MIN_BLOCKS_D
+#define CM_PERSIST_MIN_BLOCKS_D 1
+#endif
+
+CM_DEVINL unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+CM_DEVINL unsigned ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// bulk asynchronous copies global -> shared (TMA engine), completed on an
+// mbarrier.  Sources and destinations 16-byte aligned, sizes multiples of 16.
+// ---------------------------------------------------------------------------
+CM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+CM_DEVINL void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+
+// make initialised mbarriers visible to the async proxy (before first use)
+CM_DEVINL void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+CM_DEVINL void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
+               : "memory");
+}
+
+// order this thread's view of global memory (written by the generic proxy of
+// any block before the last grid barrier) before its following bulk copies
+CM_DEVINL void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+CM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(b))
+      : "memory");
+}
+
+CM_DEVINL bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Wait for the completion of phase `parity` of mbarrier b; false after about
+// two seconds (the copies it tracks read valid device memory and always
+// complete, so this only bounds the wait).
+CM_DEVINL bool mbar_wait(unsigned long long* b, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(b, parity))
+    if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) return false;
+  return true;
+}
 
 // All blocks of the grid meet; returns false if the wait gave up.
 CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
@@ -46,14 +111,14 @@ CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
     } else {
       const long long t0 = clock64();
       while (true) {
-        if (atomicAdd(&bar->gen, 0u) != g) break;
-        if (atomicAdd(&bar->abort, 0u) != 0u) { ok = 0; break; }
+        if (ld_acquire_gpu(&bar->gen) != g) break;
+        if (ld_relaxed_gpu(&bar->abort) != 0u) { ok = 0; break; }
         if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) {
           atomicExch(&bar->abort, 1u);
           ok = 0;
           break;
         }
-        __nanosleep(64);
+        if (CM_BARRIER_SLEEP_NS > 0) __nanosleep(CM_BARRIER_SLEEP_NS);
       }
     }
     __threadfence();
@@ -350,6 +415,70 @@ CM_DEVINL void ph_col(const Slot<R>& S, int tile, typename CT<R>::C* tws, typena
   __syncthreads();
 }
 
+// Stage of one column tile: its spectrum block (N x W complex, of which the
+// first `rows` rows are copied; the transform treats the others as zero) and
+// its Green's table block (N x W reals).
+template <typename R>
+struct ColStage {
+  typedef typename CT<R>::C C;
+  static __host__ __device__ size_t bytes(int n, int w) { return (size_t)n * w * (sizeof(C) + sizeof(R)); }
+};
+
+// Issue (one thread) the bulk copies of column tile `tile` into `stage`.
+template <typename R, int LOGN>
+CM_DEVINL void col_issue(const Slot<R>& S, int tile, unsigned char* stage, unsigned long long* mbar) {
+  typedef typename CT<R>::C C;
+  constexpr int N = 1 << LOGN;
+  const int W = 1 << S.lw;
+  // the forward input holds the topography's rows only (the rest are zero);
+  // rounded up to whole 16-byte units, still inside the N x W block
+  const unsigned b_spec = (unsigned)min((S.tx * W * sizeof(C) + 15) & ~(size_t)15, N * W * sizeof(C));
+  const unsigned b_tab = (unsigned)(N * W * sizeof(R));
+  mbar_expect_tx(mbar, b_spec + b_tab);
+  bulk_g2s(stage, S.spec + (size_t)tile * N * W, b_spec, mbar);
+  bulk_g2s(stage + (size_t)N * W * sizeof(C), S.tab[0] + (size_t)tile * N * W, b_tab, mbar);
+}
+
+// Column pass of one tile from its staged copy (see ph_col).
+template <typename R, int MODE, int LOGN>
+CM_DEVINL void ph_col_staged(const Slot<R>& S, int tile, const unsigned char* stage,
+                             typename CT<R>::C* tws, typename CT<R>::C* bufA, typename CT<R>::C* bufB) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  constexpr int N = P::N;
+  const int nyh = S.nyh, lw = S.lw;
+  const int W = 1 << lw;
+  const int wc = min(W, nyh - tile * W);
+  const int nx_in = S.tx;
+  const int nx_out = (MODE == MODE_T) ? S.tx : N;
+  const int c = threadIdx.x & (W - 1), tt = threadIdx.x >> lw;
+  C* __restrict__ blk = S.spec + (size_t)tile * N * W;
+  const C* __restrict__ sblk = reinterpret_cast<const C*>(stage);
+  const R* __restrict__ stab = reinterpret_cast<const R*>(stage + (size_t)N * W * sizeof(C));
+  const bool col_ok = c < wc;
+  C v[8];
+  R g[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int x = tt + q * P::TPS;
+    v[q] = (x < nx_in) ? sblk[x * W + c] : czero<C>();
+    g[q] = stab[x * W + c];
+  }
+  fft_p2<C, false, LOGN>(v, bufA, bufB, c, W, tt, tws);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) v[q] = cscale(v[q], g[q]);
+  __syncthreads();
+  fft_p2<C, true, LOGN>(v, bufA, bufB, c, W, tt, tws);
+  if (col_ok) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int x = tt + q * P::TPS;
+      if (x < nx_out) blk[x * W + c] = v[q];
+    }
+  }
+  __syncthreads();
+}
+
 template <typename R, int MODE, int LOGN>
 CM_DEVINL void ph_row_inv(const Slot<R>& S, const CcgView& cv, int tile,
                           typename CT<R>::C* tws, typename CT<R>::C* bufA,
@@ -449,9 +578,54 @@ CM_DEVINL void ph_row_inv(const Slot<R>& S, const CcgView& cv, int tile,
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
+CM_DEVINL unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Column pass over this block's tiles, two stages deep: the bulk copies of
+// the next tile run while the current one is transformed.  Returns false if
+// a copy did not complete in time (after waiting, bounded, for the other
+// stage's copy so that none is in flight when the block leaves).
+template <typename R, int MODE, int LOGN>
+CM_DEVINL bool col_pass(const Slot<R>& S, typename CT<R>::C* tws, typename CT<R>::C* bufA,
+                        typename CT<R>::C* bufB, unsigned char* (&stage)[2],
+                        unsigned long long* mbar, unsigned& mphase) {
+  const int G = gridDim.x;
+  int t = blockIdx.x;
+  if (t >= S.nt_col) return true;
+  if (threadIdx.x == 0) {
+    fence_async_global();
+    col_issue<R, LOGN>(S, t, stage[0], &mbar[0]);
+  }
+  int b = 0;
+  for (; t < S.nt_col; t += G) {
+    const bool next = t + G < S.nt_col;
+    if (next && threadIdx.x == 0) col_issue<R, LOGN>(S, t + G, stage[b ^ 1], &mbar[b ^ 1]);
+    // every thread waits; the outcome is made block-uniform before any
+    // thread proceeds to the transform's barriers
+    const bool ok = __syncthreads_and(mbar_wait(&mbar[b], (mphase >> b) & 1u)) != 0;
+    if (!ok) {
+      if (next) mbar_wait(&mbar[b ^ 1], (mphase >> (b ^ 1)) & 1u);
+      return false;
+    }
+    mphase ^= 1u << b;
+    ph_col_staged<R, MODE, LOGN>(S, t, stage[b], tws, bufA, bufB);
+    b ^= 1;
+  }
+  return true;
+}
+
+// stamps (optional, PH_COUNT entries, zeroed by the caller): block 0 adds
+// the nanoseconds from the previous grid barrier to the end of each phase's
+// barrier, so every phase is charged its tile work, its wait for the slowest
+// block and the reduction that follows the previous barrier.
 template <typename R, int LOGN>
-__global__ void __launch_bounds__(CM_FFT_THREADS / 2)
-k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters, int bisect_passes) {
+__global__ void __launch_bounds__(CM_FFT_THREADS / 2,
+                                  sizeof(R) == 8 ? CM_PERSIST_MIN_BLOCKS_D : CM_PERSIST_MIN_BLOCKS_F)
+k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters, int bisect_passes,
+              unsigned long long* stamps) {
   typedef typename CT<R>::C C;
   constexpr int N = 1 << LOGN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -474,13 +648,45 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
   C* bufA = tws + N;
   const int ebuf = smem_padded(max((S.row_tile >> 1) * N, (1 << S.lw) * N));
   C* bufB = bufA + ebuf;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = __ldg(S.twy + i);
+  // two stages of column tiles, filled by bulk copies (see persist_smem_bytes)
+  unsigned char* stage[2];
+  {
+    const size_t o = ((size_t)(N + 2 * ebuf) * sizeof(C) + 127) & ~(size_t)127;
+    stage[0] = smem_raw + o;
+    stage[1] = stage[0] + ((ColStage<R>::bytes(N, 1 << S.lw) + 127) & ~(size_t)127);
+  }
+  __shared__ __align__(8) unsigned long long mbar[2];
+  unsigned mphase = 0;  // bit b: parity of stage b's next completion
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_init_fence();
+  }
+  stage_tw_p2<LOGN>(tws, S.twy);
   __syncthreads();
   double* partials = S.partials;
   const int G = gridDim.x;
   bool alive = true;
-  auto barrier = [&]() -> bool {
-    if (!grid_barrier(bar, gen, &bar_ok)) {
+  const bool timed = stamps != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+  unsigned long long t_last = timed ? global_ns() : 0ull;
+  auto abort_solve = [&]() {
+    alive = false;
+    if (threadIdx.x == 0) {
+      atomicExch(&bar->abort, 1u);
+      if (blockIdx.x == 0) {
+        st.status = CMS_TIMEOUT;
+        st.done = 1;
+      }
+    }
+  };
+  auto barrier = [&](int phase) -> bool {
+    const bool ok = grid_barrier(bar, gen, &bar_ok);
+    if (timed) {
+      const unsigned long long t = global_ns();
+      stamps[phase] += t - t_last;
+      t_last = t;
+    }
+    if (!ok) {
       alive = false;
       if (threadIdx.x == 0 && blockIdx.x == 0) {
         st.status = CMS_TIMEOUT;
@@ -499,7 +705,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
         ph_begin<R>(S, st, t, v);
         write_partials<5>(partials, t, v, kinds, red_sm);
       }
-      if (!barrier()) break;
+      if (!barrier(PH_BEGIN)) break;
       reduce_partials<5>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_begin(st, v);
       __syncthreads();
@@ -514,7 +720,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
         ph_bisect<R>(S, st, t, v);
         write_partials<CM_BIS_CAND>(partials, t, v, kinds, red_sm);
       }
-      if (!barrier()) break;
+      if (!barrier(PH_BISECT)) break;
       reduce_partials<CM_BIS_CAND>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_bisect(st, v);
       __syncthreads();
@@ -530,7 +736,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
           ph_gsum<R>(S, st, t, v);
           write_partials<1>(partials, t, v, kinds, red_sm);
         }
-        if (!barrier()) break;
+        if (!barrier(PH_GSUM)) break;
         reduce_partials<1>(partials, S.nt_comp, kinds, v, red_sm);
         if (threadIdx.x == 0) fin_gsum(st, v);
         __syncthreads();
@@ -544,13 +750,13 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
           ph_row_fwd<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, v);
           write_partials<2>(partials, t, v, kinds, red_sm);
         }
-        if (!barrier()) break;
+        if (!barrier(PH_ROW_FWD_T)) break;
         reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
         if (threadIdx.x == 0) st.sum_cgt = v[0];
         __syncthreads();
       }
-      for (int t = blockIdx.x; t < S.nt_col; t += G) ph_col<R, MODE_T, LOGN>(S, t, tws, bufA, bufB);
-      if (!barrier()) break;
+      if (!col_pass<R, MODE_T, LOGN>(S, tws, bufA, bufB, stage, mbar, mphase)) { abort_solve(); break; }
+      if (!barrier(PH_COL_T)) break;
       {
         double v[2];
         const int kinds[2] = {RED_SUM, RED_MAX};
@@ -558,7 +764,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
           ph_row_inv<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, v);
           write_partials<2>(partials, t, v, kinds, red_sm);
         }
-        if (!barrier()) break;
+        if (!barrier(PH_ROW_INV_T)) break;
         reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
         if (threadIdx.x == 0) {
           double a[1] = {v[0]};
@@ -575,7 +781,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
         ph_update<R>(S, st, t, v);
         write_partials<5>(partials, t, v, kinds, red_sm);
       }
-      if (!barrier()) break;
+      if (!barrier(PH_UPDATE)) break;
       reduce_partials<5>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_update(st, v);
       __syncthreads();
@@ -589,13 +795,13 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
         ph_row_fwd<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, v);
         write_partials<2>(partials, t, v, kinds, red_sm);
       }
-      if (!barrier()) break;
+      if (!barrier(PH_ROW_FWD_F)) break;
       reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_force(st, v);
       __syncthreads();
     }
-    for (int t = blockIdx.x; t < S.nt_col; t += G) ph_col<R, MODE_F, LOGN>(S, t, tws, bufA, bufB);
-    if (!barrier()) break;
+    if (!col_pass<R, MODE_F, LOGN>(S, tws, bufA, bufB, stage, mbar, mphase)) { abort_solve(); break; }
+    if (!barrier(PH_COL_F)) break;
     {
       double v[2];
       const int kinds[2] = {RED_MAX, RED_MAX};
@@ -603,7 +809,7 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
         ph_row_inv<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, v);
         write_partials<2>(partials, t, v, kinds, red_sm);
       }
-      if (!barrier()) break;
+      if (!barrier(PH_ROW_INV_F)) break;
       reduce_partials<2>(partials, S.nt_rowd, kinds, v, red_sm);
       if (threadIdx.x == 0) ccg_converge(st, v[0], v[1]);
       __syncthreads();
@@ -615,5 +821,16 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
     const int nst = (int)(sizeof(CcgState) / sizeof(int));
     for (int i = threadIdx.x; i < nst; i += blockDim.x)
       reinterpret_cast<int*>(S.st)[i] = reinterpret_cast<const int*>(&st)[i];
+  }
+}
+
+// Host stub of k_ccg_persist for square 2^logn domains (declared in cm_launch.h).
+template <typename R>
+const void* persist_kernel(int logn) {
+  switch (logn) {
+#define CM_CASE(L) case L: return (const void*)k_ccg_persist<R, L>;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return nullptr;
   }
 }

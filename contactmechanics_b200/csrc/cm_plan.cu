@@ -13,11 +13,11 @@
 
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
-#include "cm_kernels_p2.cuh"
-#include "cm_persist.cuh"
+#include "cm_launch.h"
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
 #define CM_SMEM_COL_MAX (160 * 1024)
+#define CM_SMEM_PERSIST_MAX (212 * 1024)  // dynamic shared memory of the persistent kernel
 #define CM_COMP_ELEMS 2048
 #define CM_BISECT_PASSES 21
 #define CM_MAX_PARTIAL_VALS 32
@@ -465,9 +465,6 @@ static int grid_for(long n) {
 }
 
 template <typename R>
-static void set_p2_attrs();
-
-template <typename R>
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
@@ -628,63 +625,6 @@ static int log2_exact(int n) {
   return (1 << l) == n ? l : -1;
 }
 
-#define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
-
-template <typename R, int MODE>
-static bool p2_row_fwd(int logn, int grid, int threads, size_t smem, cudaStream_t s,
-                       const Slot<R>* S, const int2* it) {
-  switch (logn) {
-#define CM_CASE(L) case L: k_row_fwd_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
-    CM_P2_CASES(CM_CASE)
-#undef CM_CASE
-    default: return false;
-  }
-}
-
-template <typename R, int MODE>
-static bool p2_col(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
-                   const int2* it) {
-  switch (logn) {
-#define CM_CASE(L) case L: k_col_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
-    CM_P2_CASES(CM_CASE)
-#undef CM_CASE
-    default: return false;
-  }
-}
-
-template <typename R, int MODE>
-static bool p2_row_inv(int logn, int grid, int threads, size_t smem, cudaStream_t s,
-                       const Slot<R>* S, const int2* it) {
-  switch (logn) {
-#define CM_CASE(L) case L: k_row_inv_p2<R, MODE, L><<<grid, threads, smem, s>>>(S, it); return true;
-    CM_P2_CASES(CM_CASE)
-#undef CM_CASE
-    default: return false;
-  }
-}
-
-template <typename R>
-static void set_p2_attrs() {
-  static bool done = false;
-  if (done) return;
-  done = true;
-  const int mx = 200 * 1024;
-  const int carve = cudaSharedmemCarveoutMaxShared;
-#define CM_ATTR(K)                                                                  \
-  cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);         \
-  cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-#define CM_CASE(L)                           \
-  CM_ATTR((k_row_fwd_p2<R, MODE_T, L>))      \
-  CM_ATTR((k_row_fwd_p2<R, MODE_F, L>))      \
-  CM_ATTR((k_col_p2<R, MODE_T, L>))          \
-  CM_ATTR((k_col_p2<R, MODE_F, L>))          \
-  CM_ATTR((k_row_inv_p2<R, MODE_T, L>))      \
-  CM_ATTR((k_row_inv_p2<R, MODE_F, L>))
-  CM_P2_CASES(CM_CASE)
-#undef CM_CASE
-#undef CM_ATTR
-}
-
 // kernels of one iteration, in launch order (bisection passes excluded)
 #define CM_ITER_KERNELS 10
 static const char* const k_iter_names[CM_ITER_KERNELS] = {
@@ -762,16 +702,6 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
 }
 
 // ---- persistent cooperative solver --------------------------------------------
-template <typename R>
-static const void* persist_kernel(int logn) {
-  switch (logn) {
-#define CM_CASE(L) case L: return (const void*)k_ccg_persist<R, L>;
-    CM_P2_CASES(CM_CASE)
-#undef CM_CASE
-    default: return nullptr;
-  }
-}
-
 // Decide whether the persistent kernel can run this plan and size its grid.
 template <typename R>
 static int setup_persist(cm_plan* p, Work<R>& w) {
@@ -781,10 +711,8 @@ static int setup_persist(cm_plan* p, Work<R>& w) {
   const int logn = log2_exact(p->nx);
   const void* k = persist_kernel<R>(logn);
   if (!k) return CM_OK;
-  typedef typename CT<R>::C C;
-  const int ebuf = smem_padded(std::max((T.row_tile / 2) * p->nx, T.col_tile * p->nx));
-  const size_t smem = (size_t)(p->nx + 2 * ebuf) * sizeof(C);
-  if (smem > CM_SMEM_COL_MAX) return CM_OK;
+  const size_t smem = persist_smem_bytes<R>(p->nx, T.row_tile, T.col_tile);
+  if (smem > CM_SMEM_PERSIST_MAX) return CM_OK;
   CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
   int per_sm = 0, dev = 0, nsm = 0, coop = 0;
@@ -804,11 +732,12 @@ static int setup_persist(cm_plan* p, Work<R>& w) {
 }
 
 template <typename R>
-static int launch_persist(cm_plan* p, Work<R>& w, int iters, int bisect_passes, cudaStream_t s) {
+static int launch_persist(cm_plan* p, Work<R>& w, int iters, int bisect_passes, cudaStream_t s,
+                          unsigned long long* stamps = nullptr) {
   CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
   const Slot<R>* S = w.d_ccg;
   GridBarrier* bar = w.bar;
-  void* args[] = {(void*)&S, (void*)&bar, (void*)&iters, (void*)&bisect_passes};
+  void* args[] = {(void*)&S, (void*)&bar, (void*)&iters, (void*)&bisect_passes, (void*)&stamps};
   CK(cudaLaunchCooperativeKernel(persist_kernel<R>(w.persist_logn), dim3(w.persist_grid),
                                  dim3(w.persist_threads), args, w.persist_smem, s));
   g_launches += 1;
@@ -880,7 +809,8 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   const bool bisect = prm->has_hardness && prm->load_control;
   if (prof_iters > 0 && w.persist) {
-    // profiler: one cooperative launch of prof_iters iterations
+    // profiler: one cooperative launch of prof_iters iterations timed with
+    // events, then a second one with phase stamps
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -893,6 +823,18 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     prof_ms[0] = ms / prof_iters;
+    CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
+    unsigned long long* stamps = nullptr;
+    CK(cudaMalloc(&stamps, PH_COUNT * sizeof(unsigned long long)));
+    unsigned long long ns[PH_COUNT];
+    int rc = cudaMemsetAsync(stamps, 0, sizeof(ns), s) == cudaSuccess ? CM_OK : CM_ERR_CUDA;
+    if (rc == CM_OK) rc = launch_persist(p, w, prof_iters, bisect ? CM_BISECT_PASSES : 0, s, stamps);
+    if (rc == CM_OK && cudaMemcpyAsync(ns, stamps, sizeof(ns), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      rc = CM_ERR_CUDA;
+    if (rc == CM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = CM_ERR_CUDA;
+    cudaFree(stamps);
+    CKS(rc);
+    for (int k = 0; k < PH_COUNT; ++k) prof_ms[1 + k] = (float)(ns[k] * 1e-6 / prof_iters);
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     *fin = *p->h_state;
@@ -1813,8 +1755,16 @@ int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int it
     CKS(run_ccg<float>(p, p->w32, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
   const bool persist = prm->precision == CM_FP64 ? p->w64.persist : p->w32.persist;
   if (persist) {
-    if (n_kernels) *n_kernels = 1;
-    if (names) names[0] = "k_ccg_persist";
+    static const char* phase_names[PH_COUNT] = {
+        "k_ccg_persist:begin",   "k_ccg_persist:bisect",    "k_ccg_persist:gsum",
+        "k_ccg_persist:row_fwd_t", "k_ccg_persist:col_t",   "k_ccg_persist:row_inv_t",
+        "k_ccg_persist:update",  "k_ccg_persist:row_fwd_f", "k_ccg_persist:col_f",
+        "k_ccg_persist:row_inv_f"};
+    if (n_kernels) *n_kernels = 1 + PH_COUNT;
+    if (names) {
+      names[0] = "k_ccg_persist";
+      for (int k = 0; k < PH_COUNT; ++k) names[1 + k] = phase_names[k];
+    }
   } else {
     if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
     if (names)

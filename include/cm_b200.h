@@ -257,6 +257,10 @@ unsigned long long cm_launch_count(void);
  * eagerly with a CUDA event between kernels on the plan's stream.  Writes
  * the average milliseconds of each of the *n_kernels kernels (launch order)
  * to ms_per_kernel (capacity >= 16) and, if names is not NULL, their names.
+ * Plans that run the persistent solver kernel report it as entry 0
+ * ("k_ccg_persist", event-timed milliseconds per iteration) followed by its
+ * phases ("k_ccg_persist:<phase>", milliseconds per iteration from
+ * in-kernel timer stamps of a second run; they sum to about entry 0).
  * Returns CM_ERR_ARG if the solve stopped before `iters` iterations.
  * Instrumentation; no reference counterpart.
  */
