@@ -166,7 +166,7 @@ def iteration_bytes(nx, ny, tx, ty, p=4, pt=4):
 
 
 def load_traffic():
-    path = os.path.join(ROOT, "profiles", "c2_kernel_traffic.json")
+    path = os.path.join(ROOT, "profiles", "traffic_free1024.json")
     try:
         with open(path) as fh:
             return json.load(fh)

@@ -69,7 +69,6 @@ CM_DEVINL void dft_r(C* v) {
 template <typename C, bool INV, int LOGN>
 CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int base, int estride, int tt, const C* tw) {
   typedef P2Plan<LOGN> P;
-  constexpr int N = P::N;
   // ---- first stage (Ns = 1): radix FIRST, 8/FIRST butterflies per thread
   {
     constexpr int R = P::FIRST;
