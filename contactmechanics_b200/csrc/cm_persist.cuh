@@ -152,6 +152,13 @@ CM_DEVINL void write_partials(double* partials, int tile, double (&v)[NV], const
   }
 }
 
+// The largest R not above -H: for any R value x, (double)x > -H exactly when
+// x > neg_down<R>(H), and (double)x <= -H exactly when x <= neg_down<R>(H),
+// so the hardness tests run in the field's own type.
+template <typename R> CM_DEVINL R neg_down(double H);
+template <> CM_DEVINL float neg_down<float>(double H) { return __double2float_rd(-H); }
+template <> CM_DEVINL double neg_down<double>(double H) { return -H; }
+
 // view of the state for the operator phases
 CM_DEVINL void view_of(const CcgState& s, CcgView& v) {
   v.par = s.parity;
@@ -176,8 +183,11 @@ CM_DEVINL void ph_begin(const Slot<R>& S, const CcgState& st, int tile, double (
   const int cn = min(S.comp_rows, S.tx - cx0) * ty;
   const R* __restrict__ f = S.f[st.parity];
   const int has_h = st.p.has_h;
-  const double H = st.p.H;
-  double a_c = 0, a_cg = 0, s_cg = 0, gmax = -INFINITY, gmin = INFINITY;
+  const R hdn = neg_down<R>(st.p.H);
+  // counts in int and extrema in R are exact; only the sum is accumulated in FP64
+  int a_c = 0, a_cg = 0;
+  double s_cg = 0;
+  R gmax = -INFINITY, gmin = INFINITY;
   struct V3 { R f, u, h; };
   batched_loop<4>(cn, [&](int e) {
     const int r = e / ty, y = e - r * ty;
@@ -185,13 +195,13 @@ CM_DEVINL void ph_begin(const Slot<R>& S, const CcgState& st, int tile, double (
               __ldg(S.h + (size_t)cx0 * ty + e)};
   }, [&](int, V3 q) {
     const bool c0 = q.f < 0;
-    const bool c = c0 && (!has_h || (double)q.f > -H);
+    const bool c = c0 && (!has_h || q.f > hdn);
     const R g = q.u - q.h;
     a_c += c0;
     a_cg += c;
     if (c) s_cg += (double)g;
-    gmax = fmax(gmax, (double)g);
-    gmin = fmin(gmin, (double)g);
+    gmax = fmax(gmax, g);
+    gmin = fmin(gmin, g);
   });
   v[0] = a_c; v[1] = a_cg; v[2] = s_cg; v[3] = gmax; v[4] = gmin;
 }
@@ -202,7 +212,7 @@ CM_DEVINL void ph_gsum(const Slot<R>& S, const CcgState& st, int tile, double (&
   const int cn = min(S.comp_rows, S.tx - cx0) * ty;
   const R* __restrict__ f = S.f[st.parity];
   const int has_h = st.p.has_h;
-  const double H = st.p.H;
+  const R hdn = neg_down<R>(st.p.H);
   const R off = (R)st.offset;
   double G = 0;
   struct V3 { R f, u, h; };
@@ -211,7 +221,7 @@ CM_DEVINL void ph_gsum(const Slot<R>& S, const CcgState& st, int tile, double (&
     return V3{__ldcg(f + (size_t)cx0 * ty + e), __ldcg(S.u + (size_t)(cx0 + r) * ny + y),
               __ldg(S.h + (size_t)cx0 * ty + e)};
   }, [&](int, V3 q) {
-    const bool c = (q.f < 0) && (!has_h || (double)q.f > -H);
+    const bool c = (q.f < 0) && (!has_h || q.f > hdn);
     const R g = (q.u - q.h) - off;
     if (c) G += (double)g * (double)g;
   });
@@ -248,7 +258,12 @@ CM_DEVINL void ph_update(const Slot<R>& S, const CcgState& st, int tile, double 
   const double mix = st.cur_mixfac;
   const R* __restrict__ f = S.f[par];
   R* __restrict__ fo = S.f[par ^ 1];
-  double a_fl = 0, min_fl = INFINITY, max_t = 0, s_fp = 0, n_nc = 0;
+  const R hdn = neg_down<R>(H);
+  // counts in int and extrema in R are exact (x -> (double)x + H is monotonic,
+  // so the minimum of fn + H is the minimum fn plus H); only the sum is FP64
+  int a_fl = 0, n_nc = 0;
+  R min_fn = INFINITY, max_t = 0;
+  double s_fp = 0;
   struct V4 { R f, u, h, t; };
   batched_loop<4>(cn, [&](int e) {
     const int r = e / ty, y = e - r * ty;
@@ -260,23 +275,23 @@ CM_DEVINL void ph_update(const Slot<R>& S, const CcgState& st, int tile, double 
     const R g = (q.u - q.h) - off;
     R fn;
     if (branch == 0) {
-      const bool c = (q.f < 0) && (!has_h || (double)q.f > -H);
+      const bool c = (q.f < 0) && (!has_h || q.f > hdn);
       fn = c ? (R)(q.f + tau * q.t) : q.f;
     } else {
       fn = (R)((R)(1 - mix) * q.f - (g < 0 ? (R)(mix * H) : (R)0));
     }
     const bool tensile = fn >= 0;
-    const bool flowing = has_h && (double)fn <= -H;
+    const bool flowing = has_h && fn <= hdn;
     const bool nc = (tensile && g < 0) || (flowing && g > 0);
-    if (tensile) max_t = fmax(max_t, (double)fn);
-    if (flowing) { a_fl += 1; min_fl = fmin(min_fl, (double)fn + H); }
+    if (tensile) max_t = fmax(max_t, fn);
+    if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
     const R fp = tensile ? (R)0 : fn;
     s_fp += (double)fp;
     n_nc += nc;
     fo[ic] = fp;
     if (has_h) S.gneg[ic] = g < 0;
   });
-  v[0] = a_fl; v[1] = min_fl; v[2] = max_t; v[3] = s_fp; v[4] = n_nc;
+  v[0] = a_fl; v[1] = (double)min_fn + H; v[2] = max_t; v[3] = s_fp; v[4] = n_nc;
 }
 
 // ---------------------------------------------------------------------------
@@ -298,7 +313,9 @@ CM_DEVINL void ph_row_fwd(const Slot<R>& S, const CcgView& cv, int tile,
   const bool va_ok = xa < x0 + nrows, vb_ok = xa + 1 < x0 + nrows;
   R* __restrict__ fio = S.f[MODE == MODE_T ? cv.par : (cv.par ^ 1)];
   const R off = (R)cv.offset;
-  double acc = 0.0, amax = 0.0;
+  const R hdn = neg_down<R>(cv.H);
+  double acc = 0.0;
+  R amax = 0;  // exact in R
   const bool need_gap = (MODE == MODE_T) || cv.apply_nc;
   R fv[2][8], uv[2][8], hv[2][8], tv[2][8];
 #pragma unroll
@@ -332,7 +349,7 @@ CM_DEVINL void ph_row_fwd(const Slot<R>& S, const CcgView& cv, int tile,
       const size_t ic = (size_t)(xa + w) * ty + y;
       if (MODE == MODE_T) {
         const R fa = fv[w][q];
-        const bool c = (fa < 0) && (!cv.has_h || (double)fa > -cv.H);
+        const bool c = (fa < 0) && (!cv.has_h || fa > hdn);
         const R g = (uv[w][q] - hv[w][q]) - off;
         const R tn = c ? (R)(g + (R)cv.beta * tv[w][q]) : (R)0;
         S.t[ic] = tn;
@@ -341,7 +358,7 @@ CM_DEVINL void ph_row_fwd(const Slot<R>& S, const CcgView& cv, int tile,
       } else {
         const R fp = fv[w][q];
         double f = cv.uniform ? cv.funif : cv.scale * (double)fp;
-        const bool flowing = cv.has_h && (double)fp <= -cv.H;
+        const bool flowing = cv.has_h && fp <= hdn;
         if (flowing) f = -cv.H;
         if (cv.apply_nc) {
           const R g = (uv[w][q] - hv[w][q]) - off;
@@ -351,7 +368,7 @@ CM_DEVINL void ph_row_fwd(const Slot<R>& S, const CcgView& cv, int tile,
         const R fr = (R)f;
         fio[ic] = fr;
         acc += (double)fr;
-        amax = fmax(amax, fabs((double)fr));
+        amax = fmax(amax, fabs(fr));
         out[w] = fr;
       }
     }
@@ -529,6 +546,8 @@ CM_DEVINL void ph_row_inv(const Slot<R>& S, const CcgView& cv, int tile,
   } else {
     const R* __restrict__ fa_buf = S.f[cv.par];
     const R off = (R)cv.offset;
+    const R hdn = neg_down<R>(cv.H);
+    R du = 0, pmax = -INFINITY;  // extrema, exact in R
     R uo[2][8], hv[2][8], fa[2][8];
     unsigned char gn[2][8];
 #pragma unroll
@@ -558,17 +577,19 @@ CM_DEVINL void ph_row_inv(const Slot<R>& S, const CcgView& cv, int tile,
       for (int q = 0; q < 8; ++q) {
         const int y = tt + q * P::TPS;
         const R val = w ? v[q].y : v[q].x;
-        a0 = fmax(a0, (double)fabs(val - uo[w][q]));
+        du = fmax(du, fabs(val - uo[w][q]));
         S.u[(size_t)x * N + y] = val;
         if (x < tx && y < ty) {
           bool cc;
-          if (cv.branch == 0) cc = (fa[w][q] < 0) && (!cv.has_h || (double)fa[w][q] > -cv.H);
+          if (cv.branch == 0) cc = (fa[w][q] < 0) && (!cv.has_h || fa[w][q] > hdn);
           else cc = gn[w][q] != 0;
           const R pen = (hv[w][q] + off) - val;
-          a1 = fmax(a1, cc ? (double)pen : 0.0);
+          pmax = fmax(pmax, cc ? pen : (R)0);
         }
       }
     }
+    a0 = du;
+    a1 = pmax;
   }
   __syncthreads();  // shared buffers free before the next tile
   vr[0] = a0;
