@@ -142,22 +142,67 @@ CM_DEVINL void reduce_partials(const double* __restrict__ partials, int ntiles,
   block_reduce<NV>(out, kinds, red_sm);
 }
 
-template <int NV>
-CM_DEVINL void write_partials(double* partials, int tile, double (&v)[NV], const int (&kinds)[NV],
-                              double* red_sm) {
-  block_reduce<NV>(v, kinds, red_sm);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) partials[(size_t)tile * NV + i] = v[i];
-  }
-}
-
 // The largest R not above -H: for any R value x, (double)x > -H exactly when
 // x > neg_down<R>(H), and (double)x <= -H exactly when x <= neg_down<R>(H),
 // so the hardness tests run in the field's own type.
 template <typename R> CM_DEVINL R neg_down(double H);
 template <> CM_DEVINL float neg_down<float>(double H) { return __double2float_rd(-H); }
 template <> CM_DEVINL double neg_down<double>(double H) { return -H; }
+
+// Tile partials with the cross-warp step deferred.  body(t, v) fills the
+// thread's values v of tile t; each tile's warp-level tree runs at once and
+// its per-warp results wait in shared memory; after up to `slots` tiles (and
+// after the last one) every warp finishes one parked tile with block_reduce's
+// cross-warp tree and writes its partials.  Same arithmetic in the same order
+// as block_reduce per tile, with two block barriers per flush instead of
+// three per tile.  red_sm holds CM_RED_SM_VALS doubles, red_tiles
+// CM_RED_SLOTS ints.
+#define CM_RED_SLOTS 8
+#define CM_RED_SM_VALS (CM_RED_SLOTS * 5 * 32)
+template <int NV, typename Body>
+CM_DEVINL void tile_partials(int ntiles, double* partials, const int (&kinds)[NV], double* red_sm,
+                             int* red_tiles, Body body) {
+  constexpr int SLOTS = (CM_RED_SLOTS * NV * 32 <= CM_RED_SM_VALS) ? CM_RED_SLOTS : 1;
+  static_assert(NV * 32 <= CM_RED_SM_VALS, "reduction buffer too small");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  auto flush = [&](int n) {
+    __syncthreads();
+    for (int sl = warp; sl < n; sl += nw) {
+      const int tile = red_tiles[sl];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        double x = lane < nw ? red_sm[(sl * NV + i) * 32 + lane] : red_neutral(kinds[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          x = red_apply(kinds[i], x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) partials[(size_t)tile * NV + i] = x;
+      }
+    }
+    __syncthreads();
+  };
+  int n = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double v[NV];
+    body(t, v);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+        v[i] = red_apply(kinds[i], v[i], __shfl_xor_sync(0xffffffffu, v[i], o));
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) red_sm[(n * NV + i) * 32 + warp] = v[i];
+    }
+    if (threadIdx.x == 0) red_tiles[n] = t;
+    if (++n == SLOTS) {
+      flush(n);
+      n = 0;
+    }
+  }
+  if (n > 0) flush(n);
+}
 
 // view of the state for the operator phases
 CM_DEVINL void view_of(const CcgState& s, CcgView& v) {
@@ -652,7 +697,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ CcgState st;
   __shared__ int bar_ok;
-  __shared__ double red_sm[32 * CM_BIS_CAND];
+  __shared__ double red_sm[CM_RED_SM_VALS > 32 * CM_BIS_CAND ? CM_RED_SM_VALS : 32 * CM_BIS_CAND];
+  __shared__ int red_tiles[CM_RED_SLOTS];
   __shared__ Slot<R> S;
   {
     const int nS = (int)(sizeof(Slot<R>) / sizeof(int));
@@ -686,7 +732,6 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
   stage_tw_p2<LOGN>(tws, S.twy);
   __syncthreads();
   double* partials = S.partials;
-  const int G = gridDim.x;
   bool alive = true;
   const bool timed = stamps != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
   unsigned long long t_last = timed ? global_ns() : 0ull;
@@ -722,10 +767,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
     {
       double v[5];
       const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-      for (int t = blockIdx.x; t < S.nt_comp; t += G) {
-        ph_begin<R>(S, st, t, v);
-        write_partials<5>(partials, t, v, kinds, red_sm);
-      }
+      tile_partials<5>(S.nt_comp, partials, kinds, red_sm, red_tiles,
+                       [&](int t, double (&tv)[5]) { ph_begin<R>(S, st, t, tv); });
       if (!barrier(PH_BEGIN)) break;
       reduce_partials<5>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_begin(st, v);
@@ -737,10 +780,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
       int kinds[CM_BIS_CAND];
 #pragma unroll
       for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
-      for (int t = blockIdx.x; t < S.nt_comp; t += G) {
-        ph_bisect<R>(S, st, t, v);
-        write_partials<CM_BIS_CAND>(partials, t, v, kinds, red_sm);
-      }
+      tile_partials<CM_BIS_CAND>(S.nt_comp, partials, kinds, red_sm, red_tiles,
+                       [&](int t, double (&tv)[CM_BIS_CAND]) { ph_bisect<R>(S, st, t, tv); });
       if (!barrier(PH_BISECT)) break;
       reduce_partials<CM_BIS_CAND>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_bisect(st, v);
@@ -753,10 +794,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
       {
         double v[1];
         const int kinds[1] = {RED_SUM};
-        for (int t = blockIdx.x; t < S.nt_comp; t += G) {
-          ph_gsum<R>(S, st, t, v);
-          write_partials<1>(partials, t, v, kinds, red_sm);
-        }
+        tile_partials<1>(S.nt_comp, partials, kinds, red_sm, red_tiles,
+                         [&](int t, double (&tv)[1]) { ph_gsum<R>(S, st, t, tv); });
         if (!barrier(PH_GSUM)) break;
         reduce_partials<1>(partials, S.nt_comp, kinds, v, red_sm);
         if (threadIdx.x == 0) fin_gsum(st, v);
@@ -767,10 +806,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
       {
         double v[2];
         const int kinds[2] = {RED_SUM, RED_MAX};
-        for (int t = blockIdx.x; t < S.nt_rowt; t += G) {
-          ph_row_fwd<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, v);
-          write_partials<2>(partials, t, v, kinds, red_sm);
-        }
+        tile_partials<2>(S.nt_rowt, partials, kinds, red_sm, red_tiles,
+                         [&](int t, double (&tv)[2]) { ph_row_fwd<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, tv); });
         if (!barrier(PH_ROW_FWD_T)) break;
         reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
         if (threadIdx.x == 0) st.sum_cgt = v[0];
@@ -781,10 +818,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
       {
         double v[2];
         const int kinds[2] = {RED_SUM, RED_MAX};
-        for (int t = blockIdx.x; t < S.nt_rowt; t += G) {
-          ph_row_inv<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, v);
-          write_partials<2>(partials, t, v, kinds, red_sm);
-        }
+        tile_partials<2>(S.nt_rowt, partials, kinds, red_sm, red_tiles,
+                         [&](int t, double (&tv)[2]) { ph_row_inv<R, MODE_T, LOGN>(S, cv, t, tws, bufA, bufB, tv); });
         if (!barrier(PH_ROW_INV_T)) break;
         reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
         if (threadIdx.x == 0) {
@@ -798,10 +833,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
     {
       double v[5];
       const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
-      for (int t = blockIdx.x; t < S.nt_comp; t += G) {
-        ph_update<R>(S, st, t, v);
-        write_partials<5>(partials, t, v, kinds, red_sm);
-      }
+      tile_partials<5>(S.nt_comp, partials, kinds, red_sm, red_tiles,
+                       [&](int t, double (&tv)[5]) { ph_update<R>(S, st, t, tv); });
       if (!barrier(PH_UPDATE)) break;
       reduce_partials<5>(partials, S.nt_comp, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_update(st, v);
@@ -812,10 +845,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
     {
       double v[2];
       const int kinds[2] = {RED_SUM, RED_MAX};
-      for (int t = blockIdx.x; t < S.nt_rowt; t += G) {
-        ph_row_fwd<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, v);
-        write_partials<2>(partials, t, v, kinds, red_sm);
-      }
+      tile_partials<2>(S.nt_rowt, partials, kinds, red_sm, red_tiles,
+                       [&](int t, double (&tv)[2]) { ph_row_fwd<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, tv); });
       if (!barrier(PH_ROW_FWD_F)) break;
       reduce_partials<2>(partials, S.nt_rowt, kinds, v, red_sm);
       if (threadIdx.x == 0) fin_force(st, v);
@@ -826,10 +857,8 @@ k_ccg_persist(const Slot<R>* __restrict__ slot, GridBarrier* bar, int max_iters,
     {
       double v[2];
       const int kinds[2] = {RED_MAX, RED_MAX};
-      for (int t = blockIdx.x; t < S.nt_rowd; t += G) {
-        ph_row_inv<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, v);
-        write_partials<2>(partials, t, v, kinds, red_sm);
-      }
+      tile_partials<2>(S.nt_rowd, partials, kinds, red_sm, red_tiles,
+                       [&](int t, double (&tv)[2]) { ph_row_inv<R, MODE_F, LOGN>(S, cv, t, tws, bufA, bufB, tv); });
       if (!barrier(PH_ROW_INV_F)) break;
       reduce_partials<2>(partials, S.nt_rowd, kinds, v, red_sm);
       if (threadIdx.x == 0) ccg_converge(st, v[0], v[1]);
