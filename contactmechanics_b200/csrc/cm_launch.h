@@ -8,6 +8,10 @@
 
 #define CMS_TIMEOUT 6  // solve status: a grid-barrier wait gave up
 
+// Dynamic shared memory a transform kernel may use (of the 227 KB a block can
+// hold on sm_100, leaving room for its static shared variables).
+#define CM_SMEM_DYN_MAX (220 * 1024)
+
 // Grid barrier of the persistent kernel (zeroed before every launch).
 struct GridBarrier {
   unsigned int count;
@@ -52,6 +56,30 @@ inline size_t persist_smem_bytes(int n, int row_tile, int col_tile) {
   const size_t stage = ((size_t)n * col_tile * (csize + sizeof(R)) + 127) & ~(size_t)127;
   return head + 2 * stage;
 }
+
+// The plain operator on power-of-two domains (cm_op_p2.cuh): three launches
+// on stream s.  op_p2_supported: whether sides 2^logx x 2^logy with column
+// tiles of width 2^lw can use it.  op_p2_apply returns 0 when launched, -1
+// when not supported, 1 on a CUDA error.
+// Arguments of the operator passes, passed by value to every launch.
+template <typename R>
+struct OpArgs {
+  typedef typename CT<R>::C C;
+  const R* in;
+  R* out;
+  int in_rows, in_cols, in_ld;
+  int out_rows, out_cols, out_ld;
+  int nx, nyh, lw;  // domain rows, half-spectrum columns, log2 of the column-tile width
+  int ntile_cols;
+  C* spec;
+  const R* tab;     // the selected Green's table, tiled like the spectrum
+  const C* twx;     // twiddles of length nx
+  const C* twy;     // twiddles of length ny
+};
+template <typename R>
+int op_p2_supported(int logx, int logy, int lw);
+template <typename R>
+int op_p2_apply(const OpArgs<R>& a, int logx, int logy, cudaStream_t s);
 
 // Host stub of the persistent kernel for square 2^logn domains, or nullptr.
 // Kernel arguments: (const Slot<R>*, GridBarrier*, int max_iters,

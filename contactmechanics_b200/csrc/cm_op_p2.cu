@@ -1,0 +1,143 @@
+// Launcher of the power-of-two operator passes (cm_op_p2.cuh).
+#include <mutex>
+
+#include "cm_launch.h"
+#include "cm_op_p2.cuh"
+
+namespace {
+
+struct KernelInfo {
+  bool ready = false;
+  int grid_per_sm = 0;
+};
+
+template <typename R, int LOGN, typename K>
+int prepare(K kernel, KernelInfo& info) {
+  typedef OpShape<R, LOGN> Sh;
+  if (info.ready) return info.grid_per_sm > 0 ? 0 : -1;
+  const size_t smem = Sh::smem();
+  if (cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 1;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, Sh::THREADS, smem) != cudaSuccess)
+    return 1;
+  info.grid_per_sm = per_sm;
+  info.ready = true;
+  return per_sm > 0 ? 0 : -1;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return n;
+}
+
+std::mutex g_op_mu;
+
+template <typename R, int LOGN>
+int row_fwd(const OpArgs<R>& a, cudaStream_t s) {
+  typedef OpShape<R, LOGN> Sh;
+  static KernelInfo info;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare<R, LOGN>(k_op_row_fwd<R, LOGN>, info);
+  }
+  if (rc) return rc;
+  const int tiles = (a.in_rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
+  const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
+  k_op_row_fwd<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
+template <typename R, int LOGN>
+int col(const OpArgs<R>& a, cudaStream_t s) {
+  typedef OpShape<R, LOGN> Sh;
+  static KernelInfo info;
+  if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;  // a column tile wider than a block
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare<R, LOGN>(k_op_col<R, LOGN>, info);
+  }
+  if (rc) return rc;
+  const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
+  const int groups = (a.ntile_cols + per_block - 1) / per_block;
+  const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
+  k_op_col<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
+template <typename R, int LOGN>
+int row_inv(const OpArgs<R>& a, cudaStream_t s) {
+  typedef OpShape<R, LOGN> Sh;
+  static KernelInfo info;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare<R, LOGN>(k_op_row_inv<R, LOGN>, info);
+  }
+  if (rc) return rc;
+  const int tiles = (a.out_rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
+  const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
+  k_op_row_inv<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
+template <typename R>
+int dispatch_row_fwd(int logn, const OpArgs<R>& a, cudaStream_t s) {
+  switch (logn) {
+#define CM_CASE(L) case L: return row_fwd<R, L>(a, s);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
+template <typename R>
+int dispatch_col(int logn, const OpArgs<R>& a, cudaStream_t s) {
+  switch (logn) {
+#define CM_CASE(L) case L: return col<R, L>(a, s);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
+template <typename R>
+int dispatch_row_inv(int logn, const OpArgs<R>& a, cudaStream_t s) {
+  switch (logn) {
+#define CM_CASE(L) case L: return row_inv<R, L>(a, s);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
+
+}  // namespace
+
+template <typename R>
+int op_p2_supported(int logx, int logy, int lw) {
+  if (logx < 6 || logx > 12 || logy < 6 || logy > 12) return 0;
+  const int tps = 1 << (logx - 3);
+  const int threads = std::max(tps, sizeof(R) == 8 ? 256 : 512);
+  return ((1 << lw) * tps) <= threads;
+}
+
+template <typename R>
+int op_p2_apply(const OpArgs<R>& a, int logx, int logy, cudaStream_t s) {
+  if (!op_p2_supported<R>(logx, logy, a.lw)) return -1;
+  int rc = dispatch_row_fwd<R>(logy, a, s);
+  if (!rc) rc = dispatch_col<R>(logx, a, s);
+  if (!rc) rc = dispatch_row_inv<R>(logy, a, s);
+  if (!rc && cudaGetLastError() != cudaSuccess) rc = 1;
+  return rc;
+}
+
+template int op_p2_supported<float>(int, int, int);
+template int op_p2_supported<double>(int, int, int);
+template int op_p2_apply<float>(const OpArgs<float>&, int, int, cudaStream_t);
+template int op_p2_apply<double>(const OpArgs<double>&, int, int, cudaStream_t);

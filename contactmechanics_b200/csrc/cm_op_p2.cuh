@@ -1,0 +1,197 @@
+// The elastic operator u = IFFT(T . FFT(f)) (FFTElasticHalfSpace.py:573-611,
+// free :1141-1197) for power-of-two domains (sides 64..4096), as three
+// bandwidth-oriented passes over caller buffers:
+//
+//   k_op_row_fwd  rows x < in_rows: packed real-to-complex row transforms
+//                 (two rows per complex transform), half spectrum written
+//                 into the plan's column-tiled spectrum;
+//   k_op_col      every column tile: forward transform along x (input rows
+//                 >= in_rows are zero), times the real Green's table,
+//                 inverse transform, rows < out_rows written back;
+//   k_op_row_inv  rows x < out_rows: complex-to-real row transforms, output
+//                 columns < out_cols written to the caller's buffer.
+//
+// Arguments travel by value (no descriptor upload), so a call is a plain
+// sequence of three launches on the caller's stream.  Blocks walk their
+// tiles with a grid stride, so the twiddle tables are staged once per block.
+// A block covers 2*NP rows (row passes) or several column tiles (column
+// pass) with N/8 threads per transform, the register-resident engine of
+// cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
+// touches whole rows-of-a-tile runs: (row, column-in-tile) fastest, which in
+// the plan's layout ((k >> lw) * nx + x) * W + (k & (W-1)) are contiguous.
+#pragma once
+#include "cm_fft_p2.cuh"
+#include "cm_kernels.cuh"
+#include "cm_launch.h"
+
+// threads of one block of the operator passes for transform length 2^LOGN
+template <typename R, int LOGN>
+struct OpShape {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int TPS = N / 8;
+  static constexpr int BASE = sizeof(R) == 8 ? 256 : 512;
+  static constexpr int THREADS = TPS > BASE ? TPS : BASE;
+  static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
+  static constexpr int MINB = sizeof(R) == 8 ? 1 : 2;
+  static constexpr int LNP = NP >= 512 ? 9 : NP >= 256 ? 8 : NP >= 128 ? 7 : NP >= 64 ? 6 : NP >= 32 ? 5
+                             : NP >= 16 ? 4 : NP >= 8 ? 3 : NP >= 4 ? 2 : NP >= 2 ? 1 : 0;
+  static size_t smem() {
+    return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
+  }
+};
+
+template <typename R, int LOGN>
+__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+k_op_row_fwd(OpArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  typedef OpShape<R, LOGN> Sh;
+  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  stage_tw_p2<LOGN>(tws, a.twy);
+  __syncthreads();
+  const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
+  const int W = 1 << a.lw, nkb = (a.nyh + W - 1) >> a.lw;
+  const int ntiles = (a.in_rows + ROWS - 1) / ROWS;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int x0 = tile * ROWS, xa = x0 + 2 * s;
+    C v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int y = tt + q * P::TPS;
+      R ra = 0, rb = 0;
+      if (y < a.in_cols) {
+        if (xa < a.in_rows) ra = __ldg(a.in + (size_t)xa * a.in_ld + y);
+        if (xa + 1 < a.in_rows) rb = __ldg(a.in + (size_t)(xa + 1) * a.in_ld + y);
+      }
+      v[q] = cmake<C>(ra, rb);
+    }
+    fft_p2<C, false, LOGN>(v, bufA, bufB, s * N, 1, tt, tws);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
+    __syncthreads();
+    // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
+    const int total = nkb * ROWS * W;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int kw = e & (W - 1);
+      const int r = (e >> a.lw) & (ROWS - 1);
+      const int kb = e >> (a.lw + Sh::LNP + 1);
+      const int k = kb * W + kw, x = x0 + r;
+      if (k >= a.nyh || x >= a.in_rows) continue;
+      const int p = r >> 1;
+      const C z = bufA[spad(p * N + k)];
+      const C zm = bufA[spad(p * N + ((N - k) & (N - 1)))];
+      const C val = (r & 1) ? cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5)
+                            : cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
+      a.spec[((size_t)kb * a.nx + x) * W + kw] = val;
+    }
+    __syncthreads();  // bufA free for the next tile
+  }
+}
+
+template <typename R, int LOGN>
+__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+k_op_col(OpArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  typedef OpShape<R, LOGN> Sh;
+  constexpr int N = P::N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(Sh::NP * N);
+  stage_tw_p2<LOGN>(tws, a.twx);
+  __syncthreads();
+  const int lw = a.lw, W = 1 << lw;
+  // thread -> (tile of the block j, column c of the tile, element group tt)
+  const int c = threadIdx.x & (W - 1);
+  const int tt = (threadIdx.x >> lw) & (P::TPS - 1);
+  const int j = threadIdx.x >> (lw + P::LTPS);
+  const int tiles_per_block = blockDim.x >> (lw + P::LTPS);
+  const int ngroups = (a.ntile_cols + tiles_per_block - 1) / tiles_per_block;
+  const int base = j * N * W + c;
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int tile = grp * tiles_per_block + j;
+    const bool tile_ok = tile < a.ntile_cols;
+    const int wc = tile_ok ? min(W, a.nyh - tile * W) : 0;
+    const bool col_ok = c < wc;
+    C* __restrict__ blk = a.spec + (size_t)tile * N * W;
+    const R* __restrict__ tblk = a.tab + (size_t)tile * N * W;
+    C v[8];
+    R g[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int x = tt + q * P::TPS;
+      v[q] = (col_ok && x < a.in_rows) ? blk[x * W + c] : czero<C>();
+      g[q] = col_ok ? __ldg(tblk + x * W + c) : (R)0;
+    }
+    fft_p2<C, false, LOGN>(v, bufA, bufB, base, W, tt, tws);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = cscale(v[q], g[q]);
+    __syncthreads();
+    fft_p2<C, true, LOGN>(v, bufA, bufB, base, W, tt, tws);
+    if (col_ok) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int x = tt + q * P::TPS;
+        if (x < a.out_rows) blk[x * W + c] = v[q];
+      }
+    }
+    __syncthreads();  // buffers free for the next group
+  }
+}
+
+template <typename R, int LOGN>
+__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+k_op_row_inv(OpArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  typedef OpShape<R, LOGN> Sh;
+  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  stage_tw_p2<LOGN>(tws, a.twy);
+  __syncthreads();
+  const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
+  const int W = 1 << a.lw, nkb = (a.nyh + W - 1) >> a.lw;
+  const int ntiles = (a.out_rows + ROWS - 1) / ROWS;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int x0 = tile * ROWS;
+    // gather the row pairs' half spectra; e = ((kb * NP) + p) * W + kw
+    const int total = nkb * NP * W;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int kw = e & (W - 1);
+      const int p = (e >> a.lw) & (NP - 1);
+      const int kb = e >> (a.lw + Sh::LNP);
+      const int k = kb * W + kw, xa = x0 + 2 * p;
+      if (k >= a.nyh || xa >= a.out_rows) continue;
+      const size_t ia = ((size_t)kb * a.nx + xa) * W + kw;
+      C X = a.spec[ia];
+      C Y = (xa + 1 < a.out_rows) ? a.spec[ia + W] : czero<C>();
+      const bool selfconj = (k == 0) || (2 * k == N);
+      if (selfconj) { X.y = 0; Y.y = 0; }
+      bufA[spad(p * N + k)] = cmake<C>(X.x - Y.y, X.y + Y.x);
+      if (!selfconj) bufA[spad(p * N + N - k)] = cmake<C>(X.x + Y.y, Y.x - X.y);
+    }
+    __syncthreads();
+    C v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
+    fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
+    const int xa = x0 + 2 * s;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int y = tt + q * P::TPS;
+      if (y >= a.out_cols) continue;
+      if (xa < a.out_rows) a.out[(size_t)xa * a.out_ld + y] = v[q].x;
+      if (xa + 1 < a.out_rows) a.out[(size_t)(xa + 1) * a.out_ld + y] = v[q].y;
+    }
+    __syncthreads();  // buffers free for the next tile
+  }
+}

@@ -41,7 +41,7 @@ void set_p2_attrs() {
   bool done = false;
   if (done) return;
   done = true;
-  const int mx = 200 * 1024;
+  const int mx = CM_SMEM_DYN_MAX;
   const int carve = cudaSharedmemCarveoutMaxShared;
 #define CM_ATTR(K)                                                                  \
   cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);         \

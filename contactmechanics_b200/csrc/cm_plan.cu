@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "cm_b200.h"
@@ -16,7 +17,6 @@
 #include "cm_launch.h"
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
-#define CM_SMEM_COL_MAX (160 * 1024)
 #define CM_SMEM_PERSIST_MAX (212 * 1024)  // dynamic shared memory of the persistent kernel
 #define CM_COMP_ELEMS 2048
 #define CM_BISECT_PASSES 21
@@ -114,14 +114,14 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   int np = (int)std::max<size_t>(1, elems / (size_t)ny);
   np = std::min(np, (nx + 1) / 2);
   const size_t srow = (2 * (size_t)np * ny + ny) * csize;
-  if (srow > CM_SMEM_COL_MAX) return CM_ERR_SIZE;
+  if (srow > CM_SMEM_DYN_MAX) return CM_ERR_SIZE;
   t->row_tile = 2 * np;
   t->smem_row = srow;
   t->threads_row = pow2_threads((size_t)np * ny);
   int lw = 0;
   while ((2ul << lw) * (size_t)nx <= elems && (1 << (lw + 1)) <= nyh) ++lw;
   const size_t scol = (2 * ((size_t)1 << lw) * nx + nx) * csize;
-  if (scol > CM_SMEM_COL_MAX) return CM_ERR_SIZE;
+  if (scol > CM_SMEM_DYN_MAX) return CM_ERR_SIZE;
   t->lw = lw;
   t->col_tile = 1 << lw;
   t->smem_col = scol;
@@ -132,11 +132,18 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   // their shared buffers carry one padding slot per 8 elements
   t->p2_threads_row = np * (ny / 8);
   t->p2_threads_col = (1 << lw) * (nx / 8);
-  t->smem_row = std::max(t->smem_row, (size_t)(2 * smem_padded(np * ny) + ny) * csize);
-  t->smem_col = std::max(t->smem_col, (size_t)(2 * smem_padded((1 << lw) * nx) + nx) * csize);
+  const size_t p2row = (size_t)(2 * smem_padded(np * ny) + ny) * csize;
+  const size_t p2col = (size_t)(2 * smem_padded((1 << lw) * nx) + nx) * csize;
+  // the FP64 power-of-two kernels are compiled for at most half the threads
+  const int p2max = csize == 16 ? CM_FFT_THREADS / 2 : CM_FFT_THREADS;
   auto is_p2 = [](int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; };
-  t->p2 = is_p2(nx) && is_p2(ny) && t->p2_threads_row >= 32 && t->p2_threads_row <= CM_FFT_THREADS &&
-          t->p2_threads_col >= 32 && t->p2_threads_col <= CM_FFT_THREADS;
+  t->p2 = is_p2(nx) && is_p2(ny) && t->p2_threads_row >= 32 && t->p2_threads_row <= p2max &&
+          t->p2_threads_col >= 32 && t->p2_threads_col <= p2max && p2row <= CM_SMEM_DYN_MAX &&
+          p2col <= CM_SMEM_DYN_MAX;
+  if (t->p2) {
+    t->smem_row = std::max(t->smem_row, p2row);
+    t->smem_col = std::max(t->smem_col, p2col);
+  }
   return CM_OK;
 }
 
@@ -181,21 +188,51 @@ __global__ void k_table_periodic(double* G, int nx, int ny, int nyh, double sx, 
 
 // Displacement of a uniformly loaded dx x dy pixel (Love / Johnson p.54) on
 // the doubled domain, coordinates wrapped at i > nx.
-__global__ void k_love(double* out, int tx, int ty, int nxd, int nyd, double dx, double dy,
-                       double young) {
-  const double pi = 3.14159265358979323846;
-  const double a = dx * 0.5, b = dy * 0.5;
+// Love's kernel: displacement of a uniformly loaded dx x dy pixel
+// (FFTElasticHalfSpace.py:1033-1137, Johnson 1985 p.54) on the doubled
+// domain.  The formula sums four corner terms that cancel: at a distance of
+// r pixels they exceed the result by about r^2, so evaluated in FP64 it
+// carries relative errors of about r^2 * 1e-16 (1e-9 of the displacement at
+// a 1024^2 topography).  It is therefore evaluated on the host in extended
+// precision, on the quadrant |x| <= tx dx, |y| <= ty dy only (the kernel is
+// even in x and y), and rounded once to FP64.
+static void love_quadrant(std::vector<double>& q, int tx, int ty, double dx_d, double dy_d,
+                          double young) {
+  typedef long double L;
+  const L pi = 3.141592653589793238462643383279502884L;
+  const L dx = dx_d, dy = dy_d, a = dx / 2, b = dy / 2, c = 1 / (pi * (L)young);
+  q.assign((size_t)(tx + 1) * (ty + 1), 0.0);
+  auto rows = [&](int i0, int i1) {
+    for (int i = i0; i < i1; ++i) {
+      const L x = (L)i * dx, xp = x + a, xm = x - a;
+      for (int j = 0; j <= ty; ++j) {
+        const L y = (L)j * dy, yp = y + b, ym = y - b;
+        const L r_pp = sqrtl(yp * yp + xp * xp), r_mp = sqrtl(ym * ym + xp * xp);
+        const L r_pm = sqrtl(yp * yp + xm * xm), r_mm = sqrtl(ym * ym + xm * xm);
+        const L v = xp * logl((yp + r_pp) / (ym + r_mp)) + yp * logl((xp + r_pp) / (xm + r_pm)) +
+                    xm * logl((ym + r_mm) / (yp + r_pm)) + ym * logl((xm + r_mm) / (xp + r_mp));
+        q[(size_t)i * (ty + 1) + j] = (double)(c * v);
+      }
+    }
+  };
+  const int nt = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  const int per = (tx + 1 + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const int i0 = t * per, i1 = std::min(tx + 1, i0 + per);
+    if (i0 < i1) pool.emplace_back(rows, i0, i1);
+  }
+  for (auto& th : pool) th.join();
+}
+
+// out[i][j] of the doubled (nxd, nyd) domain = quadrant value at
+// (|x|, |y|) = (min(i, nxd - i), min(j, nyd - j)) pixels
+__global__ void k_love_expand(double* out, const double* q, int tx, int ty, int nxd, int nyd) {
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nxd * nyd;
        idx += (long)gridDim.x * blockDim.x) {
     const int i = (int)(idx / nyd), j = (int)(idx % nyd);
-    const double x = (double)(i <= tx ? i : i - 2 * tx) * dx;
-    const double y = (double)(j <= ty ? j : j - 2 * ty) * dy;
-    const double xp = x + a, xm = x - a, yp = y + b, ym = y - b;
-    const double r_pp = sqrt(yp * yp + xp * xp), r_mp = sqrt(ym * ym + xp * xp);
-    const double r_pm = sqrt(yp * yp + xm * xm), r_mm = sqrt(ym * ym + xm * xm);
-    const double v = xp * log((yp + r_pp) / (ym + r_mp)) + yp * log((xp + r_pp) / (xm + r_pm)) +
-                     xm * log((ym + r_mm) / (yp + r_pm)) + ym * log((xm + r_mm) / (xp + r_mp));
-    out[idx] = 1 / (pi * young) * v;
+    const int ai = min(i, nxd - i), aj = min(j, nyd - j);
+    out[idx] = q[(size_t)ai * (ty + 1) + aj];
   }
 }
 
@@ -457,6 +494,12 @@ static int dalloc(cm_plan* p, T** ptr, size_t count) {
   return dev_alloc(p, reinterpret_cast<void**>(ptr), count * sizeof(T));
 }
 
+static int log2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return (1 << l) == n ? l : -1;
+}
+
 static int grid_for(long n) {
   long g = (n + 255) / 256;
   if (g > 148L * 16) g = 148L * 16;
@@ -470,7 +513,7 @@ static void set_smem_attrs() {
   if (done) return;
   done = true;
   set_p2_attrs<R>();
-  const int mx = 200 * 1024;
+  const int mx = CM_SMEM_DYN_MAX;
   const int carve = cudaSharedmemCarveoutMaxShared;
   cudaFuncSetAttribute(k_row_fwd<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
   cudaFuncSetAttribute(k_row_fwd<R, MODE_F>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
@@ -590,6 +633,35 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
   hs.out_cols = out_cols;
   hs.out_ld = out_ld;
   hs.table_sel = table_sel;
+  if (mode == MODE_PLAIN) {
+    // power-of-two domains: the by-value operator passes (cm_op_p2.cuh)
+    const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+    if (lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw)) {
+      OpArgs<R> a;
+      a.in = in;
+      a.out = out;
+      a.in_rows = in_rows;
+      a.in_cols = in_cols;
+      a.in_ld = in_ld;
+      a.out_rows = out_rows;
+      a.out_cols = out_cols;
+      a.out_ld = out_ld;
+      a.nx = p->nx;
+      a.nyh = p->nyh;
+      a.lw = w.tiles.lw;
+      a.ntile_cols = w.tiles.ntile_cols;
+      a.spec = w.spec;
+      a.tab = w.tab[table_sel];
+      a.twx = hs.twx;
+      a.twy = hs.twy;
+      const int rc = op_p2_apply<R>(a, lx, ly, s);
+      if (rc == 0) {
+        g_launches += 3;
+        return CM_OK;
+      }
+      if (rc > 0) return CM_ERR_CUDA;
+    }
+  }
   CK(cudaMemcpyAsync(w.d_plain, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
   const int nt_in = (in_rows + hs.row_tile - 1) / hs.row_tile;
   const int nt_out = (out_rows + hs.row_tile - 1) / hs.row_tile;
@@ -619,11 +691,6 @@ static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int
 // solver driver
 // ---------------------------------------------------------------------------
 // ---- power-of-two specialisations -------------------------------------------
-static int log2_exact(int n) {
-  int l = 0;
-  while ((1 << l) < n) ++l;
-  return (1 << l) == n ? l : -1;
-}
 
 // kernels of one iteration, in launch order (bisection passes excluded)
 #define CM_ITER_KERNELS 10
@@ -1337,10 +1404,15 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
                                                    desc->young, desc->poisson, desc->q0_mode,
                                                    desc->stiffness_q0, desc->thickness, desc->dim);
   } else {
-    double* love = nullptr;
+    double *love = nullptr, *quad = nullptr;
     if ((rc = dalloc(p, &love, (long)p->nx * p->ny)) != CM_OK) return fail(rc);
-    k_love<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, p->tx, p->ty, p->nx, p->ny,
-                                                          desc->sx / p->tx, desc->sy / p->ty, desc->young);
+    std::vector<double> hq;
+    love_quadrant(hq, p->tx, p->ty, desc->sx / p->tx, desc->sy / p->ty, desc->young);
+    if ((rc = dalloc(p, &quad, (long)hq.size())) != CM_OK) return fail(rc);
+    if (cudaMemcpyAsync(quad, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, s) !=
+        cudaSuccess)
+      return fail(CM_ERR_CUDA);
+    k_love_expand<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, quad, p->tx, p->ty, p->nx, p->ny);
     rc = launch_plain<double>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
                                          0, 0, s);
     if (rc != CM_OK) return fail(rc);

@@ -154,6 +154,32 @@ def love_kernel(nb_grid_pts, physical_sizes, young):
     return val / (np.pi * young)
 
 
+def love_kernel_extended(nb_grid_pts, physical_sizes, young):
+    """:func:`love_kernel` evaluated in numpy's extended precision
+    (``longdouble``) and rounded once to FP64.  Test helper: the four corner
+    terms cancel (by about r^2 at r pixels from the load), so the FP64
+    evaluation of the reference formula carries errors of about r^2 eps; the
+    extended evaluation measures that error."""
+    nx, ny = nb_grid_pts
+    L = np.longdouble
+    dx, dy = L(physical_sizes[0] / nx), L(physical_sizes[1] / ny)
+    a, b = dx / 2, dy / 2
+    i = np.arange(2 * nx)
+    j = np.arange(2 * ny)
+    x = (np.where(i <= nx, i, i - 2 * nx).astype(L) * dx).reshape(-1, 1)
+    y = (np.where(j <= ny, j, j - 2 * ny).astype(L) * dy).reshape(1, -1)
+
+    def r(p, q):
+        return np.sqrt(p * p + q * q)
+
+    xp, xm, yp, ym = x + a, x - a, y + b, y - b
+    val = (xp * np.log((yp + r(yp, xp)) / (ym + r(ym, xp)))
+           + yp * np.log((xp + r(yp, xp)) / (xm + r(yp, xm)))
+           + xm * np.log((ym + r(ym, xm)) / (yp + r(yp, xm)))
+           + ym * np.log((xm + r(ym, xm)) / (xp + r(ym, xp))))
+    return (val / (L(np.pi) * L(young))).astype(np.float64)
+
+
 def free_greens_function(nb_grid_pts, physical_sizes, young):
     """Hockney table: forward FFT of :func:`love_kernel`
     (FFTElasticHalfSpace.py:1138-1139).  Shape ``(nx+1, 2ny)`` complex."""

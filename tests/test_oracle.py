@@ -145,3 +145,14 @@ def test_shape_error():
     s = oc.PeriodicSubstrate((8, 8), 1.0, (1.0, 1.0))
     with pytest.raises(oc.SubstrateError):
         s.evaluate_disp(np.zeros((8, 9)))
+
+
+def test_love_kernel_extended_precision():
+    """The extended-precision evaluation of the Love kernel agrees with the
+    FP64 one to the cancellation error of the FP64 formula (about r^2 eps at
+    r pixels from the load): tight on a small grid, looser on a larger one."""
+    for n, tol in ((8, 1e-13), (64, 1e-11)):
+        a = oc.love_kernel((n, n), (1.3, 0.7), 1.1)
+        b = oc.love_kernel_extended((n, n), (1.3, 0.7), 1.1)
+        assert a.shape == b.shape
+        assert abs(a - b).max() <= tol * abs(b).max()
