@@ -15,6 +15,10 @@ path on the same sweep (`fp64_value`); the relative displacement error of the
 mixed result against the FP64 result; p50 / p99 per-solve latency; `e2e`
 through the public API with host (numpy) arrays; a roofline of the dominant
 kernel from live CUDA-event timing; the CPU oracle on a bounded sample.
+Further entries: `batched` (512 uneven periodic solves in one lockstep
+batch), `serving` (a Poisson request stream through ContactServer),
+`plastic` (periodic 2048^2 with hardness, mixed vs FP64) and `operator` (the
+standalone evaluate_disp against the HBM roofline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -384,6 +388,96 @@ def run_batched(fp64_subset=48):
 
 
 # ---------------------------------------------------------------------------
+# C4 plastic solve and the standalone operator
+# ---------------------------------------------------------------------------
+C4_WORKLOAD = ("periodic 2048x2048, self-affine H=0.7 slope 0.2 seed 4, hardness 0.05 E*, mean "
+               "pressure 5e-3 E*; pentol 1e-9*(max h-min h), forcetol 1e-9*F")
+
+
+def run_plastic(reps=2):
+    """Plastic configuration (C4): mixed vs FP64 solve, best of `reps`."""
+    import torch
+    import contactmechanics_b200 as cm
+    from contactmechanics_b200.Generation import self_affine
+    n = 2048
+    h = self_affine((n, n), (1.0, 1.0), 0.7, 0.2, seed=4)
+    hd = torch.from_numpy(h).cuda()
+    sub = cm.PeriodicFFTElasticHalfSpace((n, n), 1.0, (1.0, 1.0))
+    F = 5e-3
+    kw = dict(external_force=F, hardness=0.05 / (n * n), pentol=1e-9 * float(h.max() - h.min()),
+              forcetol=1e-9 * F, maxiter=20000)
+    out, res = {"workload": C4_WORKLOAD}, {}
+    for prec in ("mixed", "fp64"):
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = cm.constrained_conjugate_gradients(sub, hd, precision=prec, **kw)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        res[prec] = r
+        out[prec] = {"solves_per_s": 1.0 / best, "ms": best * 1e3, "nit": r.nit,
+                     "converged": bool(r.success)}
+    a, b = res["mixed"], res["fp64"]
+    out["rel_err_vs_fp64"] = float(torch.linalg.norm(a.x - b.x) / torch.linalg.norm(b.x))
+    pa, pb = int(a.plastic.sum()), int(b.plastic.sum())
+    ca, cb = int((a.jac > 0).sum()), int((b.jac > 0).sum())
+    out["plastic_area_rel_err"] = abs(pa - pb) / max(pb, 1)
+    out["contact_area_rel_err"] = abs(ca - cb) / max(cb, 1)
+    out["plastic_fraction"] = pb / (n * n)
+    out["speedup_vs_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    return out
+
+
+def run_operator(reps=50):
+    """The standalone operator (evaluate_disp, device-resident fields) on the
+    C4 grid and the free 1024^2 grid: microseconds per call from CUDA events
+    around `reps` back-to-back calls, and the operator's algorithmic bytes
+    p (N + N_d) + p_t N_h against the measured HBM peak."""
+    import torch
+    import contactmechanics_b200 as cm
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
+    peak, peak_kind = peaks()
+    out = {"workload": "evaluate_disp on device-resident fields; periodic 2048^2 and free "
+                       "1024^2 (2048^2 domain)", "peak_gbs": peak, "peak_source": peak_kind}
+    for kind, n in (("periodic", 2048), ("free", 1024)):
+        cls = cm.FreeFFTElasticHalfSpace if kind == "free" else cm.PeriodicFFTElasticHalfSpace
+        sub = cls((n, n), 1.0, (1.0, 1.0))
+        nxd, nyd = sub.nb_domain_grid_pts
+        for prec in ("fp32", "fp64"):
+            dt = torch.float32 if prec == "fp32" else torch.float64
+            x = torch.randn((nxd, nyd), dtype=dt, device="cuda")
+            y = torch.empty_like(x)
+            stream = torch.cuda.current_stream()
+
+            def call():
+                _lib.check(L.cm_apply(sub._plan.ptr, _lib.CM_OP_DISP, _lib.PRECISIONS[prec],
+                                      ctypes.c_void_p(x.data_ptr()), n if kind == "free" else nxd,
+                                      n if kind == "free" else nyd, nyd, ctypes.c_void_p(y.data_ptr()),
+                                      nxd, nyd, nyd, ctypes.c_void_p(stream.cuda_stream)))
+            for _ in range(5):
+                call()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                call()
+            e1.record()
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) * 1e3 / reps
+            p = 4 if prec == "fp32" else 8
+            N = n * n
+            b = p * (N + nxd * nyd) + p * nxd * (nyd // 2 + 1)
+            gbs = b / us / 1e3
+            out[f"{kind}{n}_{prec}"] = {"us": us, "algorithmic_bytes": b, "GBps": gbs,
+                                        "frac": gbs / peak}
+    return out
+
+
+# ---------------------------------------------------------------------------
 # serving: Poisson request stream through the continuous-batching loop
 # ---------------------------------------------------------------------------
 SERVE_SIDES = (64, 96, 128, 192, 256, 384, 512, 768, 1024)
@@ -465,6 +559,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the 512-solve batched configuration")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-stream run")
+    ap.add_argument("--no-plastic", action="store_true", help="skip the plastic configuration")
+    ap.add_argument("--no-operator", action="store_true", help="skip the standalone operator")
     ap.add_argument("--profile-solve", choices=["mixed", "fp64", "fp32"], default=None,
                     help="run the first solve of the sweep once and exit (for profilers)")
     args = ap.parse_args()
@@ -503,7 +599,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     r = run_gpu(args, rank, world, local_rank)
-    batched = serving = None
+    batched = serving = plastic = operator = None
+    if world == 1 and not args.no_operator:
+        operator = run_operator()
+    if world == 1 and not args.no_plastic:
+        plastic = run_plastic()
     if world == 1 and not args.no_batched:
         batched = run_batched()
     if world == 1 and not args.no_serving:
@@ -546,6 +646,8 @@ def main():
         "cpu_baseline": cpu,
         "batched": batched,
         "serving": serving,
+        "plastic": plastic,
+        "operator": operator,
     }
     print(json.dumps(line))
     return 0
