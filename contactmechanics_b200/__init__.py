@@ -14,5 +14,6 @@ from .Systems import NonSmoothContactSystem  # noqa: F401
 from .PlasticSystemSpecialisations import PlasticNonSmoothContactSystem  # noqa: F401
 from .Factory import make_plastic_system, make_system  # noqa: F401
 from .Topography import PlasticTopography, Topography  # noqa: F401
+from .PipelineFunction import contact_mechanics  # noqa: F401
 
 __version__ = "0.1.0"

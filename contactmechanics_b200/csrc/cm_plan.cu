@@ -42,6 +42,11 @@
 static unsigned long long g_launches = 0;  // kernels launched by this library
 static thread_local int g_polls = 0;        // convergence polls of the current call
 
+// Iterations the FP32 phase of a mixed solve may take: at most
+// CM_FP32_ITER_CAP and half of the solve's maxiter, so that a phase that
+// stalls at FP32 resolution leaves the FP64 refinement at least half.
+static int fp32_cap(int maxiter) { return std::min(CM_FP32_ITER_CAP, std::max(1, maxiter / 2)); }
+
 static cudaError_t& last_cuda_error() {
   static thread_local cudaError_t e = cudaSuccess;
   return e;
@@ -1498,7 +1503,7 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   const double rf = prm->precision == CM_MIXED ? 1e-5 : 0.0;
   // FP32 phase: tolerances widened to FP32 resolution; a phase that cannot
   // reach them within its iteration cap hands over to the FP64 refinement
-  const int cap32 = prm->precision == CM_MIXED ? std::min(prm->maxiter, CM_FP32_ITER_CAP) : prm->maxiter;
+  const int cap32 = prm->precision == CM_MIXED ? fp32_cap(prm->maxiter) : prm->maxiter;
   CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin));
   const double ms32 = ms_since(t0);
   if (prm->precision == CM_FP32) {
@@ -1571,7 +1576,7 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
     const double rf = prec == CM_MIXED ? 1e-5 : 0.0;
     for (int i = 0; i < n; ++i) {
       SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, plans[i]->ny};
-      const int mi = prec == CM_MIXED ? std::min(params[i].maxiter, CM_FP32_ITER_CAP) : params[i].maxiter;
+      const int mi = prec == CM_MIXED ? fp32_cap(params[i].maxiter) : params[i].maxiter;
       CKS(ccg_init<float>(plans[i], plans[i]->w32, &params[i], in, rp, rf, mi, s));
     }
     CKS(batch_loop<float>(n, plans, bisect, maxiter, timeout, s, &g_polls));
@@ -1675,7 +1680,7 @@ int cm_ccg_begin(cm_stepper* stp, cm_plan* p, const cm_ccg_params* prm, const do
   } else {
     const bool mixed = prm->precision == CM_MIXED;
     const double rp = mixed ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
-    const int mi = mixed ? std::min(prm->maxiter, CM_FP32_ITER_CAP) : prm->maxiter;
+    const int mi = mixed ? fp32_cap(prm->maxiter) : prm->maxiter;
     CKS(ccg_init<float>(p, p->w32, prm, in, rp, mixed ? 1e-5 : 0.0, mi, stp->stream));
     p->phase = 1;
   }

@@ -541,3 +541,82 @@ def self_affine(nb_grid_pts, physical_sizes, hurst, rms_slope, seed,
     dy = np.diff(h, axis=1, append=h[:, :1]) / (sy / ny)
     slope = np.sqrt(np.mean(dx * dx + dy * dy))
     return h * (rms_slope / slope)
+
+
+# ---------------------------------------------------------------------------
+# Automated sweeps (PipelineFunction.py:37-449)
+# ---------------------------------------------------------------------------
+
+def contact_mechanics(heights, physical_sizes, periodic=True, nsteps=None, offsets=None,
+                      pressures=None, hardness=None, maxiter=100, results_callback=None,
+                      **solver_kwargs):
+    """Restatement of ``contact_mechanics`` (PipelineFunction.py:229-449) with
+    this module's solver.  A hardness (units of E*) makes it plastic: the
+    solver gets ``hardness * area_per_pt`` and, after each converged solve,
+    the plastic gap is added to the plastic displacement
+    (PlasticSystemSpecialisations.py:60-69); automatically chosen steps reset
+    it first (PipelineFunction.py:171-178).  Returns mean pressure, contact
+    area, mean displacement, mean gap and convergence flags per step."""
+    h0 = np.asarray(heights, dtype=np.float64)
+    nb = h0.shape
+    sub = (PeriodicSubstrate if periodic else FreeSubstrate)(nb, 1.0, physical_sizes)
+    plastic = hardness is not None and hardness > 0
+    state = {"pd": np.zeros(nb)}
+
+    def cur_heights():
+        return h0 + state["pd"] if plastic else h0
+
+    # pentol from the rms height (PipelineFunction.py:390-393)
+    pentol = max(rms_height(h0 + state["pd"] if plastic else h0) / (10 * np.mean(nb)), 1e-12)
+    md, mg, mp, ta, conv = [], [], [], [], []
+
+    def calc(offset=None, external_force=None):
+        middle = np.mean(cur_heights())
+        kw = dict(solver_kwargs)
+        if plastic:
+            kw["hardness"] = hardness * sub.area_per_pt
+        r = constrained_conjugate_gradients(sub, cur_heights(), offset=offset,
+                                            external_force=external_force, pentol=pentol,
+                                            maxiter=maxiter, **kw)
+        force = r["jac"]
+        disp = r["x"][:force.shape[0], :force.shape[1]]
+        if plastic and r["success"]:
+            gap = disp - (cur_heights() + r["offset"])
+            state["pd"] = state["pd"] + np.where(r["plastic"], gap, 0.0)
+        md.append(r["offset"])
+        mg.append(np.mean(disp) - middle - r["offset"])
+        load = force.sum() / np.prod(physical_sizes)
+        mp.append(load)
+        area = (force > 0).sum() / np.prod(nb)
+        ta.append(area)
+        conv.append(bool(r["success"]))
+        if results_callback is not None:
+            gap_xy = disp - cur_heights() - r["offset"]
+            gap_xy[gap_xy < 0.0] = 0.0
+            results_callback(disp, gap_xy, force / sub.area_per_pt, force > 0, r["offset"], load,
+                             area)
+
+    if pressures is not None:
+        for p in pressures:
+            calc(external_force=p * np.prod(physical_sizes))
+    elif offsets is not None:
+        for o in offsets:
+            calc(offset=o)
+    else:
+        for step in range(nsteps):
+            state["pd"] = np.zeros(nb)
+            h = cur_heights()
+            top, middle, bot = np.max(h), np.mean(h), np.min(h)
+            if step == 0:
+                off = -middle
+            elif step == 1:
+                off = -top + 0.01 * (top - middle)
+            else:
+                sd, sa = np.transpose(sorted(zip(md, ta), key=lambda pair: pair[1]))
+                ref_area = np.log10(np.array(sa + 1 / np.prod(nb)))
+                darea = np.append(ref_area[1:] - ref_area[:-1], -ref_area[-1])
+                i = np.argmax(darea)
+                off = bot + 2 * (sd[-1] - bot) if i == step - 1 else (sd[i] + sd[i + 1]) / 2
+            calc(offset=off)
+    return np.array(mp), np.array(ta), np.array(md), np.array(mg), np.array(conv)
+

@@ -163,6 +163,43 @@ def main(ref_root):
     solve("wavy_periodic_offset", PeriodicFFTElasticHalfSpace(nb, 3.56, sizes),
           h, sizes, [-0.5, np.nan, np.nan, 1e-9, 1e-5], offset=-0.5, pentol=1e-9)
 
+    # ---- automated sweeps (PipelineFunction.contact_mechanics) -------------
+    from ContactMechanics.PipelineFunction import contact_mechanics
+
+    def pipeline(name, heights, sizes, periodic, hardness=None, **kw):
+        cfg = dict(nb_grid_pts=list(heights.shape), physical_sizes=list(sizes),
+                   periodic=periodic, hardness=hardness,
+                   **{k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v)
+                      for k, v in kw.items()})
+        out[f"pipe_{name}_config"] = np.array(json.dumps(cfg))
+        out[f"pipe_{name}_heights"] = heights
+        last = {}
+
+        def cb(disp, gap, pressure, contacting, offset, load, area):
+            last.update(disp=np.array(disp), gap=np.array(gap), pressure=np.array(pressure),
+                        contacting=np.array(contacting),
+                        scalars=np.array([offset, load, area], dtype=float))
+        topo = Topography(heights, sizes, periodic=periodic)
+        res = contact_mechanics(topo, hardness=hardness, results_callback=cb, **kw)
+        for key, arr in zip(("mean_pressure", "area", "mean_displacement", "mean_gap",
+                             "converged"), res):
+            out[f"pipe_{name}_{key}"] = np.asarray(arr, dtype=float)
+        for key, arr in last.items():
+            out[f"pipe_{name}_last_{key}"] = arr
+
+    nb, sizes = (32, 32), (1.0, 1.0)
+    pipeline("pressures_periodic", self_affine(nb, sizes, 0.8, 0.1, seed=31), sizes, True,
+             pressures=[2e-3, 1e-2], maxiter=2000, optimizer_kwargs=dict(forcetol=1e-13))
+    nb, sizes = (24, 24), (1.0, 1.0)
+    pipeline("nsteps_free", _sphere(nb, sizes, 2.0), sizes, False, nsteps=3, maxiter=2000,
+             optimizer_kwargs=dict(forcetol=1e-13))
+    nb, sizes = (32, 32), (1.0, 1.0)
+    h = self_affine(nb, sizes, 0.7, 0.2, seed=32)
+    span = float(np.max(h) - np.min(h))
+    pipeline("offsets_plastic", h, sizes, True, hardness=0.05,
+             offsets=[-(float(np.max(h)) - 0.2 * span), -(float(np.max(h)) - 0.35 * span)],
+             maxiter=2000, optimizer_kwargs=dict(forcetol=1e-10))
+
     path = os.path.join(HERE, "reference_vectors.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")

@@ -10,8 +10,9 @@ import numpy as np
 import pytest
 
 from oracle import contact_oracle as oc
-from tests.conftest import (GOLDEN, golden_config, golden_operator_config,
-                            golden_operator_names, golden_solve_names)
+from tests.conftest import (GOLDEN, PIPELINE_OUTPUTS, golden_config, golden_operator_config,
+                            golden_operator_names, golden_pipeline_case, golden_pipeline_names,
+                            golden_solve_names)
 
 _npz = np.load(GOLDEN)
 
@@ -156,3 +157,40 @@ def test_love_kernel_extended_precision():
         b = oc.love_kernel_extended((n, n), (1.3, 0.7), 1.1)
         assert a.shape == b.shape
         assert abs(a - b).max() <= tol * abs(b).max()
+
+
+@pytest.mark.parametrize("name", golden_pipeline_names(_npz))
+def test_pipeline_oracle_vs_reference(golden, name):
+    """The restated automated sweep reproduces the reference's
+    contact_mechanics: per-step means, areas and convergence flags, and the
+    last step's fields."""
+    h, sizes, periodic, kw = golden_pipeline_case(golden, name)
+    opt = kw.pop("optimizer_kwargs", {})
+    last = {}
+
+    def cb(disp, gap, pressure, contacting, offset, load, area):
+        last.update(disp=disp, gap=gap, pressure=pressure, contacting=contacting)
+    res = oc.contact_mechanics(h, sizes, periodic=periodic, results_callback=cb, **kw, **opt)
+    for key, got in zip(PIPELINE_OUTPUTS, res):
+        ref = golden[f"pipe_{name}_{key}"]
+        np.testing.assert_allclose(np.asarray(got, dtype=float), ref, rtol=1e-10, atol=1e-14,
+                                   err_msg=key)
+    for key in ("disp", "gap", "pressure"):
+        ref = golden[f"pipe_{name}_last_{key}"]
+        np.testing.assert_allclose(last[key], ref, rtol=0, atol=1e-10 * abs(ref).max(), err_msg=key)
+    assert np.array_equal(last["contacting"], golden[f"pipe_{name}_last_contacting"])
+
+
+def test_pipeline_argument_errors():
+    """contact_mechanics rejects missing or conflicting step specifications with
+    the reference's messages (PipelineFunction.py:314-337), before any solve."""
+    import contactmechanics_b200 as cm
+    topo = cm.Topography(np.zeros((8, 8)), (1.0, 1.0))
+    cases = [(dict(), "Either `nsteps`, `offsets` or `pressures` must be given"),
+             (dict(nsteps=2, offsets=[0.1], pressures=[0.1]), "All of"),
+             (dict(nsteps=2, offsets=[0.1]), "Both of `nsteps` and `offsets`"),
+             (dict(nsteps=2, pressures=[0.1]), "Both of `nsteps` and `pressures`"),
+             (dict(offsets=[0.1], pressures=[0.1]), "Both of `offsets` and `pressures`")]
+    for kw, msg in cases:
+        with pytest.raises(ValueError, match=msg.replace("`", ".")):
+            topo.contact_mechanics(**kw)
