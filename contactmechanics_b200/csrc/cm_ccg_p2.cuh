@@ -1,0 +1,264 @@
+// Row passes of one CCG iteration for a single solve on a power-of-two
+// domain, in the shape of the operator passes of cm_op_p2.cuh: arguments by
+// value, blocks of 2*NP rows walking their tiles with a grid stride,
+// spectrum stores and gathers in whole (row, column-in-tile) runs.  The
+// solver's element-wise work rides on the transforms as in the per-pass
+// kernels of cm_kernels_p2.cuh (same formulas):
+//
+//   k_ccg_row_fwd<MODE_T>  search direction t (ConstrainedConjugateGradients.py
+//                          :276-279), sum c g t, rows of the topography;
+//   k_ccg_row_fwd<MODE_F>  final force of the iteration (:362-389), its sum
+//                          and maximum;
+//   k_ccg_row_inv<MODE_T>  r = G t, sum r t -> step length (:287-294);
+//   k_ccg_row_inv<MODE_F>  u = G f on the whole domain, max |du|, maximum
+//                          penetration, convergence test (:391-434).
+//
+// The column pass between them is k_op_col with the solve's state attached.
+// Each tile writes its reduction partials and the last tile to finish runs
+// the scalar step (tile_finish), as in the per-pass kernels.
+#pragma once
+#include "cm_op_p2.cuh"
+
+template <typename R, int MODE, int LOGN>
+__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+k_ccg_row_fwd(CcgArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  typedef OpShape<R, LOGN> Sh;
+  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  CcgState* st = a.st;
+  if (st->done) return;
+  if (MODE == MODE_T && st->branch != 0) return;
+  CcgView cv;
+  load_view(st, cv);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  stage_tw_p2<LOGN>(tws, a.op.twy);
+  __syncthreads();
+  const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
+  const int tx = a.tx, ty = a.ty, ny = N;
+  const int lw = a.op.lw, W = 1 << lw, nkb = (a.op.nyh + W - 1) >> lw;
+  const int ntiles = (tx + ROWS - 1) / ROWS;
+  R* __restrict__ fio = a.f[MODE == MODE_T ? cv.par : (cv.par ^ 1)];
+  const R* __restrict__ u_in = a.u;
+  const R* __restrict__ h_in = a.h;
+  R* __restrict__ t_io = a.t;
+  const R off = (R)cv.offset;
+  const R hdn = neg_down<R>(cv.H);
+  const bool need_gap = (MODE == MODE_T) || cv.apply_nc;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int x0 = tile * ROWS, xa = x0 + 2 * s;
+    double acc = 0.0;
+    R amax = 0;
+    // prologue: every input of the thread's 16 elements first, then the
+    // element-wise step and its stores
+    R fv2[2][8], uv2[2][8], hv2[2][8], tv2[2][8];
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+      const int x = xa + w;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int y = tt + q * P::TPS;
+        fv2[w][q] = 0; uv2[w][q] = 0; hv2[w][q] = 0; tv2[w][q] = 0;
+        if (x >= tx || y >= ty) continue;
+        const size_t ic = (size_t)x * ty + y;
+        fv2[w][q] = fio[ic];
+        if (need_gap) {
+          uv2[w][q] = u_in[(size_t)x * ny + y];
+          hv2[w][q] = h_in[ic];
+        }
+        if (MODE == MODE_T) tv2[w][q] = t_io[ic];
+      }
+    }
+    R out[2][8];
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+      const int x = xa + w;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int y = tt + q * P::TPS;
+        out[w][q] = 0;
+        if (x >= tx || y >= ty) continue;
+        const size_t ic = (size_t)x * ty + y;
+        const R fv = fv2[w][q], uv = uv2[w][q], hv = hv2[w][q];
+        if (MODE == MODE_T) {
+          const bool c = (fv < 0) && (!cv.has_h || fv > hdn);
+          const R g = (uv - hv) - off;
+          const R tn = c ? (R)(g + (R)cv.beta * tv2[w][q]) : (R)0;
+          t_io[ic] = tn;
+          if (c) acc += (double)g * (double)tn;
+          out[w][q] = tn;
+        } else {
+          double f = cv.uniform ? cv.funif : cv.scale * (double)fv;
+          const bool flowing = cv.has_h && fv <= hdn;
+          if (flowing) f = -cv.H;
+          if (cv.apply_nc) {
+            const R g = (uv - hv) - off;
+            const bool nc = ((fv == (R)0) && g < 0) || (flowing && g > 0);
+            if (nc) f += cv.tau * (double)g;
+          }
+          const R fr = (R)f;
+          fio[ic] = fr;
+          acc += (double)fr;
+          amax = fmax(amax, fabs(fr));
+          out[w][q] = fr;
+        }
+      }
+    }
+    C v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
+    fft_p2<C, false, LOGN>(v, bufA, bufB, s * N, 1, tt, tws);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
+    __syncthreads();
+    // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
+    const int total = nkb * ROWS * W;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int kw = e & (W - 1);
+      const int r = (e >> lw) & (ROWS - 1);
+      const int kb = e >> (lw + Sh::LNP + 1);
+      const int k = kb * W + kw, x = x0 + r;
+      if (k >= a.op.nyh || x >= tx) continue;
+      const int p = r >> 1;
+      const C z = bufA[spad(p * N + k)];
+      const C zm = bufA[spad(p * N + ((N - k) & (N - 1)))];
+      const C val = (r & 1) ? cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5)
+                            : cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
+      a.op.spec[((size_t)kb * a.op.nx + x) * W + kw] = val;
+    }
+    if (MODE == MODE_T) {
+      double vr[1] = {acc};
+      const int kinds[1] = {RED_SUM};
+      tile_finish<1>(a.partials, a.counter, tile, ntiles, vr, kinds,
+                     [&](double (&r)[1]) { st->sum_cgt = r[0]; });
+    } else {
+      double vr[2] = {acc, (double)amax};
+      const int kinds[2] = {RED_SUM, RED_MAX};
+      tile_finish<2>(a.partials, a.counter, tile, ntiles, vr, kinds,
+                     [&](double (&r)[2]) { fin_force(*st, r); });
+    }
+    __syncthreads();  // bufA free for the next tile
+  }
+}
+
+template <typename R, int MODE, int LOGN>
+__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+k_ccg_row_inv(CcgArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2Plan<LOGN> P;
+  typedef OpShape<R, LOGN> Sh;
+  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  CcgState* st = a.st;
+  if (st->done) return;
+  if (MODE == MODE_T && st->branch != 0) return;
+  CcgView cv;
+  load_view(st, cv);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  stage_tw_p2<LOGN>(tws, a.op.twy);
+  __syncthreads();
+  const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
+  const int tx = a.tx, ty = a.ty, nx = a.op.nx;
+  const int rows_total = (MODE == MODE_T) ? tx : nx;
+  const int lw = a.op.lw, W = 1 << lw, nkb = (a.op.nyh + W - 1) >> lw;
+  const int ntiles = (rows_total + ROWS - 1) / ROWS;
+  const R off = (R)cv.offset;
+  const R hdn = neg_down<R>(cv.H);
+  const R* __restrict__ fa_buf = a.f[cv.par];
+  R* __restrict__ u_io = a.u;
+  const R* __restrict__ h_in = a.h;
+  const R* __restrict__ t_in = a.t;
+  const unsigned char* __restrict__ gneg = a.gneg;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int x0 = tile * ROWS;
+    // gather the row pairs' half spectra; e = ((kb * NP) + p) * W + kw
+    const int total = nkb * NP * W;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int kw = e & (W - 1);
+      const int p = (e >> lw) & (NP - 1);
+      const int kb = e >> (lw + Sh::LNP);
+      const int k = kb * W + kw, xa = x0 + 2 * p;
+      if (k >= a.op.nyh || xa >= rows_total) continue;
+      const size_t ia = ((size_t)kb * nx + xa) * W + kw;
+      C X = a.op.spec[ia];
+      C Y = (xa + 1 < rows_total) ? a.op.spec[ia + W] : czero<C>();
+      const bool selfconj = (k == 0) || (2 * k == N);
+      if (selfconj) { X.y = 0; Y.y = 0; }
+      bufA[spad(p * N + k)] = cmake<C>(X.x - Y.y, X.y + Y.x);
+      if (!selfconj) bufA[spad(p * N + N - k)] = cmake<C>(X.x + Y.y, Y.x - X.y);
+    }
+    __syncthreads();
+    C v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
+    fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
+    const int xa = x0 + 2 * s;
+    if (MODE == MODE_T) {
+      double a0 = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int y = tt + q * P::TPS;
+        if (y >= ty) continue;
+        if (xa < tx) a0 += (double)v[q].x * (double)t_in[(size_t)xa * ty + y];
+        if (xa + 1 < tx) a0 += (double)v[q].y * (double)t_in[(size_t)(xa + 1) * ty + y];
+      }
+      double vr[1] = {a0};
+      const int kinds[1] = {RED_SUM};
+      tile_finish<1>(a.partials, a.counter, tile, ntiles, vr, kinds,
+                     [&](double (&r)[1]) { fin_tau(*st, r); });
+    } else {
+      R du = 0, pmax = -INFINITY;  // extrema, exact in R
+      // every input of the thread's 16 elements first, then the stores
+      R uo[2][8], hv[2][8];
+      bool cc[2][8];
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = xa + w;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          uo[w][q] = 0; hv[w][q] = 0; cc[w][q] = false;
+          if (x >= rows_total) continue;
+          uo[w][q] = u_io[(size_t)x * N + y];
+          if (x < tx && y < ty) {
+            const size_t ic = (size_t)x * ty + y;
+            hv[w][q] = h_in[ic];
+            if (cv.branch == 0) {
+              const R fa = fa_buf[ic];
+              cc[w][q] = (fa < 0) && (!cv.has_h || fa > hdn);
+            } else {
+              cc[w][q] = gneg[ic] != 0;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = xa + w;
+        if (x >= rows_total) continue;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          const R val = w ? v[q].y : v[q].x;
+          du = fmax(du, fabs(val - uo[w][q]));
+          u_io[(size_t)x * N + y] = val;
+          if (x < tx && y < ty) {
+            const R pen = (hv[w][q] + off) - val;
+            pmax = fmax(pmax, cc[w][q] ? pen : (R)0);
+          }
+        }
+      }
+      double vr[2] = {(double)du, (double)pmax};
+      const int kinds[2] = {RED_MAX, RED_MAX};
+      tile_finish<2>(a.partials, a.counter, tile, ntiles, vr, kinds,
+                     [&](double (&r)[2]) { ccg_converge(*st, r[0], r[1]); });
+    }
+    __syncthreads();  // buffers free for the next tile
+  }
+}

@@ -82,6 +82,13 @@ CM_DEVINL void stage_fft(FftDesc& fd, const FftDesc& src, C* tws, const C* __res
   for (int i = threadIdx.x; i < n; i += blockDim.x) tws[i] = __ldg(tw + i);
 }
 
+// The largest R not above -H: for any R value x, (double)x > -H exactly when
+// x > neg_down<R>(H), and (double)x <= -H exactly when x <= neg_down<R>(H),
+// so the hardness tests run in the field's own type.
+template <typename R> CM_DEVINL R neg_down(double H);
+template <> CM_DEVINL float neg_down<float>(double H) { return __double2float_rd(-H); }
+template <> CM_DEVINL double neg_down<double>(double H) { return -H; }
+
 // scalar state of a contact solve that the operator prologues/epilogues use
 struct CcgView {
   int par, has_h, uniform, apply_nc, branch;

@@ -75,11 +75,40 @@ struct OpArgs {
   const R* tab;     // the selected Green's table, tiled like the spectrum
   const C* twx;     // twiddles of length nx
   const C* twy;     // twiddles of length ny
+  const CcgState* st;  // column pass of a solve: skip after convergence (else nullptr)
+  int cg_only;         // ... and skip unless the iteration takes a CG step
+};
+
+// Arguments of the row passes of one CCG iteration (cm_ccg_p2.cuh).
+template <typename R>
+struct CcgArgs {
+  OpArgs<R> op;  // geometry, spectrum, Green's table, twiddles
+  R* u;          // (nx, ny)
+  const R* h;    // (tx, ty)
+  R* f[2];       // (tx, ty)
+  R* t;          // (tx, ty)
+  const unsigned char* gneg;
+  CcgState* st;
+  double* partials;
+  unsigned int* counter;
+  int tx, ty;
 };
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw);
 template <typename R>
 int op_p2_apply(const OpArgs<R>& a, int logx, int logy, cudaStream_t s);
+// The passes of one CCG iteration of a single solve on a power-of-two domain
+// (MODE_T: r = G t, MODE_F: u = G f), same return codes.
+template <typename R, int MODE>
+int ccg_p2_row_fwd(const CcgArgs<R>& a, int logy, cudaStream_t s);
+template <typename R>
+int ccg_p2_col(const OpArgs<R>& a, int logx, cudaStream_t s);
+template <typename R, int MODE>
+int ccg_p2_row_inv(const CcgArgs<R>& a, int logy, cudaStream_t s);
+// Set the kernels' attributes and occupancy ahead of the first launch (which
+// may be inside a stream capture): 0, -1 unsupported, 1 CUDA error.
+template <typename R>
+int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy);
 
 // Host stub of the persistent kernel for square 2^logn domains, or nullptr.
 // Kernel arguments: (const Slot<R>*, GridBarrier*, int max_iters,

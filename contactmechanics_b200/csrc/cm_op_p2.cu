@@ -1,6 +1,7 @@
 // Launcher of the power-of-two operator passes (cm_op_p2.cuh).
 #include <mutex>
 
+#include "cm_ccg_p2.cuh"
 #include "cm_launch.h"
 #include "cm_op_p2.cuh"
 
@@ -40,7 +41,7 @@ int sm_count() {
 std::mutex g_op_mu;
 
 template <typename R, int LOGN>
-int row_fwd(const OpArgs<R>& a, cudaStream_t s) {
+int row_fwd(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   typedef OpShape<R, LOGN> Sh;
   static KernelInfo info;
   int rc;
@@ -48,7 +49,7 @@ int row_fwd(const OpArgs<R>& a, cudaStream_t s) {
     std::lock_guard<std::mutex> g(g_op_mu);
     rc = prepare<R, LOGN>(k_op_row_fwd<R, LOGN>, info);
   }
-  if (rc) return rc;
+  if (rc || !launch) return rc;
   const int tiles = (a.in_rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
   k_op_row_fwd<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
@@ -56,7 +57,7 @@ int row_fwd(const OpArgs<R>& a, cudaStream_t s) {
 }
 
 template <typename R, int LOGN>
-int col(const OpArgs<R>& a, cudaStream_t s) {
+int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   typedef OpShape<R, LOGN> Sh;
   static KernelInfo info;
   if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;  // a column tile wider than a block
@@ -65,7 +66,7 @@ int col(const OpArgs<R>& a, cudaStream_t s) {
     std::lock_guard<std::mutex> g(g_op_mu);
     rc = prepare<R, LOGN>(k_op_col<R, LOGN>, info);
   }
-  if (rc) return rc;
+  if (rc || !launch) return rc;
   const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
   const int groups = (a.ntile_cols + per_block - 1) / per_block;
   const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
@@ -74,7 +75,7 @@ int col(const OpArgs<R>& a, cudaStream_t s) {
 }
 
 template <typename R, int LOGN>
-int row_inv(const OpArgs<R>& a, cudaStream_t s) {
+int row_inv(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   typedef OpShape<R, LOGN> Sh;
   static KernelInfo info;
   int rc;
@@ -82,7 +83,7 @@ int row_inv(const OpArgs<R>& a, cudaStream_t s) {
     std::lock_guard<std::mutex> g(g_op_mu);
     rc = prepare<R, LOGN>(k_op_row_inv<R, LOGN>, info);
   }
-  if (rc) return rc;
+  if (rc || !launch) return rc;
   const int tiles = (a.out_rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
   k_op_row_inv<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
@@ -117,7 +118,89 @@ int dispatch_row_inv(int logn, const OpArgs<R>& a, cudaStream_t s) {
   }
 }
 
+template <typename R, int MODE, int LOGN>
+int ccg_row_fwd(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
+  typedef OpShape<R, LOGN> Sh;
+  static KernelInfo info;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare<R, LOGN>(k_ccg_row_fwd<R, MODE, LOGN>, info);
+  }
+  if (rc || !launch) return rc;
+  const int tiles = (a.tx + 2 * Sh::NP - 1) / (2 * Sh::NP);
+  const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
+  k_ccg_row_fwd<R, MODE, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
+template <typename R, int MODE, int LOGN>
+int ccg_row_inv(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
+  typedef OpShape<R, LOGN> Sh;
+  static KernelInfo info;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare<R, LOGN>(k_ccg_row_inv<R, MODE, LOGN>, info);
+  }
+  if (rc || !launch) return rc;
+  const int rows = MODE == MODE_T ? a.tx : a.op.nx;
+  const int tiles = (rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
+  const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
+  k_ccg_row_inv<R, MODE, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
 }  // namespace
+
+template <typename R, int MODE>
+int ccg_p2_row_fwd(const CcgArgs<R>& a, int logy, cudaStream_t s) {
+  switch (logy) {
+#define CM_CASE(L) case L: return ccg_row_fwd<R, MODE, L>(a, s);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
+
+template <typename R>
+int ccg_p2_col(const OpArgs<R>& a, int logx, cudaStream_t s) {
+  return dispatch_col<R>(logx, a, s);
+}
+
+template <typename R, int MODE>
+int ccg_p2_row_inv(const CcgArgs<R>& a, int logy, cudaStream_t s) {
+  switch (logy) {
+#define CM_CASE(L) case L: return ccg_row_inv<R, MODE, L>(a, s);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
+
+template <typename R>
+int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy) {
+  int rc = 0;
+  switch (logy) {
+#define CM_CASE(L)                                                       \
+  case L:                                                                \
+    rc = ccg_row_fwd<R, MODE_T, L>(a, nullptr, false);                   \
+    if (!rc) rc = ccg_row_fwd<R, MODE_F, L>(a, nullptr, false);          \
+    if (!rc) rc = ccg_row_inv<R, MODE_T, L>(a, nullptr, false);          \
+    if (!rc) rc = ccg_row_inv<R, MODE_F, L>(a, nullptr, false);          \
+    break;
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+  if (rc) return rc;
+  switch (logx) {
+#define CM_CASE(L) case L: return col<R, L>(a.op, nullptr, false);
+    CM_P2_CASES(CM_CASE)
+#undef CM_CASE
+    default: return -1;
+  }
+}
 
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw) {
@@ -141,3 +224,15 @@ template int op_p2_supported<float>(int, int, int);
 template int op_p2_supported<double>(int, int, int);
 template int op_p2_apply<float>(const OpArgs<float>&, int, int, cudaStream_t);
 template int op_p2_apply<double>(const OpArgs<double>&, int, int, cudaStream_t);
+template int ccg_p2_row_fwd<float, MODE_T>(const CcgArgs<float>&, int, cudaStream_t);
+template int ccg_p2_row_fwd<float, MODE_F>(const CcgArgs<float>&, int, cudaStream_t);
+template int ccg_p2_row_fwd<double, MODE_T>(const CcgArgs<double>&, int, cudaStream_t);
+template int ccg_p2_row_fwd<double, MODE_F>(const CcgArgs<double>&, int, cudaStream_t);
+template int ccg_p2_col<float>(const OpArgs<float>&, int, cudaStream_t);
+template int ccg_p2_col<double>(const OpArgs<double>&, int, cudaStream_t);
+template int ccg_p2_row_inv<float, MODE_T>(const CcgArgs<float>&, int, cudaStream_t);
+template int ccg_p2_row_inv<float, MODE_F>(const CcgArgs<float>&, int, cudaStream_t);
+template int ccg_p2_row_inv<double, MODE_T>(const CcgArgs<double>&, int, cudaStream_t);
+template int ccg_p2_row_inv<double, MODE_F>(const CcgArgs<double>&, int, cudaStream_t);
+template int ccg_p2_prepare<float>(const CcgArgs<float>&, int, int);
+template int ccg_p2_prepare<double>(const CcgArgs<double>&, int, int);

@@ -100,6 +100,7 @@ k_op_col(OpArgs<R> a) {
   typedef P2Plan<LOGN> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N;
+  if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;

@@ -142,13 +142,6 @@ CM_DEVINL void reduce_partials(const double* __restrict__ partials, int ntiles,
   block_reduce<NV>(out, kinds, red_sm);
 }
 
-// The largest R not above -H: for any R value x, (double)x > -H exactly when
-// x > neg_down<R>(H), and (double)x <= -H exactly when x <= neg_down<R>(H),
-// so the hardness tests run in the field's own type.
-template <typename R> CM_DEVINL R neg_down(double H);
-template <> CM_DEVINL float neg_down<float>(double H) { return __double2float_rd(-H); }
-template <> CM_DEVINL double neg_down<double>(double H) { return -H; }
-
 // Tile partials with the cross-warp step deferred.  body(t, v) fills the
 // thread's values v of tile t; each tile's warp-level tree runs at once and
 // its per-warp results wait in shared memory; after up to `slots` tiles (and

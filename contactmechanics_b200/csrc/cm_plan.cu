@@ -23,6 +23,9 @@
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
 #define CM_PERSIST_ITERS 32   // iterations per cooperative launch
+#ifndef CM_BY_VALUE_PASSES
+#define CM_BY_VALUE_PASSES 1  // single solves on power-of-two domains use cm_ccg_p2.cuh
+#endif
 
 #define CK(...)                               \
   do {                                        \
@@ -451,6 +454,8 @@ struct Work {
   bool persist = false;         // persistent cooperative kernel usable
   int persist_grid = 0, persist_threads = 0, persist_logn = 0;
   size_t persist_smem = 0;
+  bool by_value = false;    // single solves: the by-value power-of-two passes (cm_ccg_p2.cuh)
+  CcgArgs<R> ccg_args{};    // their arguments
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
   int nt_comp = 0, nt_rowt = 0, nt_rowd = 0, nt_col = 0;
@@ -619,6 +624,47 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
   CK(cudaMemcpyAsync(w.d_ccg, &s, sizeof(s), cudaMemcpyHostToDevice, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   CKS(setup_persist(p, w));
+  {
+    // by-value passes for power-of-two domains (single solves)
+    const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+    CcgArgs<R>& a = w.ccg_args;
+    a.op.in = nullptr;
+    a.op.out = nullptr;
+    a.op.in_rows = p->tx;
+    a.op.in_cols = p->ty;
+    a.op.in_ld = p->ty;
+    a.op.out_rows = p->nx;
+    a.op.out_cols = p->ny;
+    a.op.out_ld = p->ny;
+    a.op.nx = p->nx;
+    a.op.nyh = p->nyh;
+    a.op.lw = w.tiles.lw;
+    a.op.ntile_cols = w.tiles.ntile_cols;
+    a.op.spec = w.spec;
+    a.op.tab = w.tab[0];
+    a.op.twx = s.twx;
+    a.op.twy = s.twy;
+    a.op.st = s.st;
+    a.op.cg_only = 0;
+    a.u = w.u;
+    a.h = w.h;
+    a.f[0] = w.f[0];
+    a.f[1] = w.f[1];
+    a.t = w.t;
+    a.gneg = w.gneg;
+    a.st = s.st;
+    a.partials = w.partials;
+    a.counter = w.counter;
+    a.tx = p->tx;
+    a.ty = p->ty;
+    w.by_value = CM_BY_VALUE_PASSES && lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw);
+    if (w.by_value) {
+      const int rc = ccg_p2_prepare<R>(a, lx, ly);
+      if (rc > 0) return CM_ERR_CUDA;
+      w.by_value = rc == 0;
+    }
+    if (w.by_value) w.persist = false;
+  }
   w.ccg_ready = true;
   return CM_OK;
 }
@@ -659,6 +705,8 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
       a.tab = w.tab[table_sel];
       a.twx = hs.twx;
       a.twy = hs.twy;
+      a.st = nullptr;
+      a.cg_only = 0;
       const int rc = op_p2_apply<R>(a, lx, ly, s);
       if (rc == 0) {
         g_launches += 3;
@@ -727,6 +775,29 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   const bool p2 = T.p2;
   const int ly = p->fy.n, lx = p->fx.n;
   const int ry = log2_exact(ly), rx = log2_exact(lx);
+  if (w.by_value) {
+    // by-value passes: one launch each; a launch error surfaces at the next check
+    const CcgArgs<R>& a = w.ccg_args;
+    OpArgs<R> col_t = a.op, col_f = a.op;
+    col_t.out_rows = p->tx;
+    col_t.cg_only = 1;
+    col_f.out_rows = p->nx;
+    ccg_p2_row_fwd<R, MODE_T>(a, ry, s);
+    mark();
+    ccg_p2_col<R>(col_t, rx, s);
+    mark();
+    ccg_p2_row_inv<R, MODE_T>(a, ry, s);
+    mark();
+    k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+    mark();
+    ccg_p2_row_fwd<R, MODE_F>(a, ry, s);
+    mark();
+    ccg_p2_col<R>(col_f, rx, s);
+    mark();
+    ccg_p2_row_inv<R, MODE_F>(a, ry, s);
+    mark();
+    return;
+  }
   if (!(p2 && p2_row_fwd<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
     k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
