@@ -669,26 +669,29 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   CcgState* st = Sp->st;
   if (st->done) return;
   const int has_h = st->p.has_h;
-  const double H = st->p.H;
+  const R hdn = neg_down<R>(st->p.H);
   const R* __restrict__ f = Sp->f[st->parity];
   const CompTile<R> T(Sp, item.y);
-  double a_c = 0, a_cg = 0, s_cg = 0, gmax = -INFINITY, gmin = INFINITY;
+  // counts in int and extrema in R are exact; only the sum is accumulated in FP64
+  int a_c = 0, a_cg = 0;
+  double s_cg = 0;
+  R gmax = -INFINITY, gmin = INFINITY;
   struct V3 { R f, u, h; };
-  batched_loop<4>(T.cn, [&](int e) {
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
     size_t ic, iu;
     T.at(e, ic, iu);
     return V3{f[ic], T.u[iu], T.h[ic]};
   }, [&](int, V3 v) {
     const bool c0 = v.f < 0;
-    const bool c = c0 && (!has_h || (double)v.f > -H);
+    const bool c = c0 && (!has_h || v.f > hdn);
     const R g = v.u - v.h;
     a_c += c0;
     a_cg += c;
     if (c) s_cg += (double)g;
-    gmax = fmax(gmax, (double)g);
-    gmin = fmin(gmin, (double)g);
+    gmax = fmax(gmax, g);
+    gmin = fmin(gmin, g);
   });
-  double v[5] = {a_c, a_cg, s_cg, gmax, gmin};
+  double v[5] = {(double)a_c, (double)a_cg, s_cg, (double)gmax, (double)gmin};
   const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
   tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
                  [&](double (&a)[5]) { fin_begin(*st, a); });
@@ -703,18 +706,18 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   CcgState* st = Sp->st;
   if (st->done || st->branch != 0) return;
   const int has_h = st->p.has_h;
-  const double H = st->p.H;
+  const R hdn = neg_down<R>(st->p.H);
   const R off = (R)st->offset;
   const R* __restrict__ f = Sp->f[st->parity];
   const CompTile<R> T(Sp, item.y);
   double G = 0;
   struct V3 { R f, u, h; };
-  batched_loop<4>(T.cn, [&](int e) {
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
     size_t ic, iu;
     T.at(e, ic, iu);
     return V3{f[ic], T.u[iu], T.h[ic]};
   }, [&](int, V3 v) {
-    const bool c = (v.f < 0) && (!has_h || (double)v.f > -H);
+    const bool c = (v.f < 0) && (!has_h || v.f > hdn);
     const R g = (v.u - v.h) - off;
     if (c) G += (double)g * (double)g;
   });
@@ -740,9 +743,9 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   if (threadIdx.x < ncand) cand[threadIdx.x] = st->bs_cand[threadIdx.x];
   __syncthreads();
   const CompTile<R> T(Sp, item.y);
-  double cnt[CM_BIS_CAND];
+  int icnt[CM_BIS_CAND];  // counts: exact in int
 #pragma unroll
-  for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = 0;
+  for (int i = 0; i < CM_BIS_CAND; ++i) icnt[i] = 0;
   struct V2 { R u, h; };
   batched_loop<4>(T.cn, [&](int e) {
     size_t ic, iu;
@@ -752,8 +755,11 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     const double g = (double)(v.u - v.h);
 #pragma unroll
     for (int i = 0; i < CM_BIS_CAND; ++i)
-      if (i < ncand) cnt[i] += (g - cand[i] < 0.0) ? 1.0 : 0.0;
+      if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
   });
+  double cnt[CM_BIS_CAND];
+#pragma unroll
+  for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = (double)icnt[i];
   int kinds[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
@@ -780,9 +786,14 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const R* __restrict__ t = Sp->t;
   unsigned char* __restrict__ gneg = Sp->gneg;
   const CompTile<R> T(Sp, item.y);
-  double a_fl = 0, min_fl = INFINITY, max_t = 0, s_fp = 0, n_nc = 0;
+  const R hdn = neg_down<R>(H);
+  // counts in int and extrema in R are exact (x -> (double)x + H is monotonic,
+  // so the minimum of fn + H is the minimum fn plus H); only the sum is FP64
+  int a_fl = 0, n_nc = 0;
+  R min_fn = INFINITY, max_t = 0;
+  double s_fp = 0;
   struct V4 { R f, u, h, t; };
-  batched_loop<4>(T.cn, [&](int e) {
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
     size_t ic, iu;
     T.at(e, ic, iu);
     return V4{f[ic], T.u[iu], T.h[ic], branch == 0 ? t[ic] : (R)0};
@@ -792,23 +803,23 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     const R g = (v.u - v.h) - off;
     R fn;
     if (branch == 0) {
-      const bool c = (fa < 0) && (!has_h || (double)fa > -H);
+      const bool c = (fa < 0) && (!has_h || fa > hdn);
       fn = c ? (R)(fa + tau * v.t) : fa;
     } else {
       fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
     }
     const bool tensile = fn >= 0;
-    const bool flowing = has_h && (double)fn <= -H;
+    const bool flowing = has_h && fn <= hdn;
     const bool nc = (tensile && g < 0) || (flowing && g > 0);
-    if (tensile) max_t = fmax(max_t, (double)fn);
-    if (flowing) { a_fl += 1; min_fl = fmin(min_fl, (double)fn + H); }
+    if (tensile) max_t = fmax(max_t, fn);
+    if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
     const R fp = tensile ? (R)0 : fn;
     s_fp += (double)fp;
     n_nc += nc;
     fo[ic] = fp;
     if (has_h) gneg[ic] = g < 0;
   });
-  double v[5] = {a_fl, min_fl, max_t, s_fp, n_nc};
+  double v[5] = {(double)a_fl, (double)min_fn + H, (double)max_t, s_fp, (double)n_nc};
   const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
   tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
                  [&](double (&a)[5]) { fin_update(*st, a); });

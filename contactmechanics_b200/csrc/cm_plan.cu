@@ -1006,7 +1006,7 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   int every = prm->check_every;
   if (every <= 0) {
     const long work = (long)p->nx * p->ny;
-    every = work >= (1L << 20) ? 4 : (work >= (1L << 16) ? 8 : 16);
+    every = work >= (1L << 20) ? (w.by_value ? 8 : 4) : (work >= (1L << 16) ? 8 : 16);
   }
   auto t0 = std::chrono::steady_clock::now();
   if (w.persist) {
