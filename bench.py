@@ -52,8 +52,15 @@ def surface():
                        rolloff_wavelength=1.0 / 8)
 
 
+_SPANS = {}
+
+
 def tolerances(h, F):
-    return dict(pentol=1e-9 * float(np.max(h) - np.min(h)), forcetol=1e-12 * F)
+    """Solver tolerances of the sweep; the heights' span is computed once per array."""
+    key = id(h)
+    if key not in _SPANS:
+        _SPANS[key] = (h, float(np.max(h) - np.min(h)))
+    return dict(pentol=1e-9 * _SPANS[key][1], forcetol=1e-12 * F)
 
 
 def peaks():

@@ -739,9 +739,26 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   CcgState* st = Sp->st;
   if (st->done || st->branch != 1 || !st->bs_active) return;
   __shared__ double cand[CM_BIS_CAND];
+  __shared__ double cand_lo, cand_hi;
   const int ncand = (st->bs_iter < 0) ? 1 : CM_BIS_CAND;
   if (threadIdx.x < ncand) cand[threadIdx.x] = st->bs_cand[threadIdx.x];
   __syncthreads();
+  if (threadIdx.x == 0) {
+    double lo = cand[0], hi = cand[0];
+    for (int i = 1; i < ncand; ++i) {
+      lo = fmin(lo, cand[i]);
+      hi = fmax(hi, cand[i]);
+    }
+    cand_lo = lo;
+    cand_hi = hi;
+  }
+  __syncthreads();
+  // g below every candidate counts for all of them, g at or above every
+  // candidate for none (for doubles, g - c < 0 exactly when g < c); only gaps
+  // inside the candidates' bracket, which shrinks 32-fold per pass, are
+  // compared one by one
+  const double lo = cand_lo, hi = cand_hi;
+  int below_all = 0;
   const CompTile<R> T(Sp, item.y);
   int icnt[CM_BIS_CAND];  // counts: exact in int
 #pragma unroll
@@ -753,13 +770,17 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
     return V2{T.u[iu], T.h[ic]};
   }, [&](int, V2 v) {
     const double g = (double)(v.u - v.h);
+    if (g < lo) {
+      ++below_all;
+    } else if (g < hi) {
 #pragma unroll
-    for (int i = 0; i < CM_BIS_CAND; ++i)
-      if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
+      for (int i = 0; i < CM_BIS_CAND; ++i)
+        if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
+    }
   });
   double cnt[CM_BIS_CAND];
 #pragma unroll
-  for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = (double)icnt[i];
+  for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = (double)(icnt[i] + (i < ncand ? below_all : 0));
   int kinds[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
