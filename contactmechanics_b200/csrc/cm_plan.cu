@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <thread>
@@ -204,8 +205,8 @@ __global__ void k_table_periodic(double* G, int nx, int ny, int nyh, double sx, 
 // a 1024^2 topography).  It is therefore evaluated on the host in extended
 // precision, on the quadrant |x| <= tx dx, |y| <= ty dy only (the kernel is
 // even in x and y), and rounded once to FP64.
-static void love_quadrant(std::vector<double>& q, int tx, int ty, double dx_d, double dy_d,
-                          double young) {
+static void love_quadrant_compute(std::vector<double>& q, int tx, int ty, double dx_d, double dy_d,
+                                  double young) {
   typedef long double L;
   const L pi = 3.141592653589793238462643383279502884L;
   const L dx = dx_d, dy = dy_d, a = dx / 2, b = dy / 2, c = 1 / (pi * (L)young);
@@ -231,6 +232,40 @@ static void love_quadrant(std::vector<double>& q, int tx, int ty, double dx_d, d
     if (i0 < i1) pool.emplace_back(rows, i0, i1);
   }
   for (auto& th : pool) th.join();
+}
+
+// The quadrant of the last few geometries, so that plans of a geometry seen
+// before (a pool of solvers of one size) skip the extended-precision pass.
+struct LoveKey {
+  int tx, ty;
+  double dx, dy, young;
+  bool operator==(const LoveKey& o) const {
+    return tx == o.tx && ty == o.ty && dx == o.dx && dy == o.dy && young == o.young;
+  }
+};
+#define CM_LOVE_CACHE 16
+static std::mutex g_love_mu;
+static std::vector<std::pair<LoveKey, std::shared_ptr<const std::vector<double>>>> g_love_cache;
+
+static std::shared_ptr<const std::vector<double>> love_quadrant(int tx, int ty, double dx, double dy,
+                                                                 double young) {
+  const LoveKey key{tx, ty, dx, dy, young};
+  {
+    std::lock_guard<std::mutex> g(g_love_mu);
+    for (size_t i = 0; i < g_love_cache.size(); ++i)
+      if (g_love_cache[i].first == key) {
+        auto hit = g_love_cache[i];
+        g_love_cache.erase(g_love_cache.begin() + i);
+        g_love_cache.push_back(hit);  // most recently used last
+        return hit.second;
+      }
+  }
+  auto q = std::make_shared<std::vector<double>>();
+  love_quadrant_compute(*q, tx, ty, dx, dy, young);
+  std::lock_guard<std::mutex> g(g_love_mu);
+  g_love_cache.emplace_back(key, q);
+  if (g_love_cache.size() > CM_LOVE_CACHE) g_love_cache.erase(g_love_cache.begin());
+  return q;
 }
 
 // out[i][j] of the doubled (nxd, nyd) domain = quadrant value at
@@ -1482,10 +1517,9 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
   } else {
     double *love = nullptr, *quad = nullptr;
     if ((rc = dalloc(p, &love, (long)p->nx * p->ny)) != CM_OK) return fail(rc);
-    std::vector<double> hq;
-    love_quadrant(hq, p->tx, p->ty, desc->sx / p->tx, desc->sy / p->ty, desc->young);
-    if ((rc = dalloc(p, &quad, (long)hq.size())) != CM_OK) return fail(rc);
-    if (cudaMemcpyAsync(quad, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, s) !=
+    const auto hq = love_quadrant(p->tx, p->ty, desc->sx / p->tx, desc->sy / p->ty, desc->young);
+    if ((rc = dalloc(p, &quad, (long)hq->size())) != CM_OK) return fail(rc);
+    if (cudaMemcpyAsync(quad, hq->data(), hq->size() * sizeof(double), cudaMemcpyHostToDevice, s) !=
         cudaSuccess)
       return fail(CM_ERR_CUDA);
     k_love_expand<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, quad, p->tx, p->ty, p->nx, p->ny);
