@@ -10,6 +10,14 @@ in-flight solve by a few iterations in one batched launch sequence
 to the FP64 refinement, and retires finished solves.  A solve's result does
 not depend on which other solves share its steps.
 
+Large requests (at least ``large_points`` domain points) skip the lockstep
+batch: a worker thread solves them one at a time with the single-solve path
+(``constrained_conjugate_gradients``, which on power-of-two domains runs the
+by-value passes of a CUDA graph on the plan's own stream) while the loop
+keeps stepping the small ones; their results are those of
+``constrained_conjugate_gradients`` for the same arguments.  Without a
+running loop thread, ``step`` solves a waiting large request itself.
+
 Each request returns the same ``OptimizeResult`` as
 ``constrained_conjugate_gradients`` (numpy arrays), plus ``latency_s`` from
 arrival to completion.
@@ -24,7 +32,8 @@ import scipy.optimize as optim
 
 from . import _lib
 from .FFTElasticHalfSpace import FreeFFTElasticHalfSpace, PeriodicFFTElasticHalfSpace
-from .Optimization.ConstrainedConjugateGradients import _device_f64, _params
+from .Optimization.ConstrainedConjugateGradients import (_device_f64, _params,
+                                                        constrained_conjugate_gradients)
 
 
 def _torch():
@@ -91,10 +100,13 @@ class ContactServer:
     mem_info         callable returning (free, total) device bytes
                      (default: torch.cuda.mem_get_info)
     precision        "mixed", "fp64" or "fp32"
+    large_points     requests with at least this many domain points are
+                     solved one at a time by the single-solve path
+                     (None: every request is batched)
     """
 
     def __init__(self, max_active=512, iters_per_step=8, hbm_reserve=1 << 30, mem_info=None,
-                 precision="mixed"):
+                 precision="mixed", large_points=1 << 20):
         torch = _torch()
         self._L = _lib.lib()
         self._torch = torch
@@ -107,6 +119,10 @@ class ContactServer:
         self.mem_info = mem_info or torch.cuda.mem_get_info
         self.precision = precision
         self._pending = collections.deque()
+        self._large = collections.deque()
+        self.large_points = large_points
+        self._large_busy = False
+        self._worker = None
         self._active = []
         self._pool = collections.defaultdict(list)
         self._lock = threading.Lock()
@@ -114,6 +130,7 @@ class ContactServer:
         self._thread = None
         self._stop = threading.Event()
         self._wake = threading.Event()
+        self._large_wake = threading.Event()
         self.completed = []
         self.steps = 0
 
@@ -129,8 +146,12 @@ class ContactServer:
             req = Request(self._next_id, kind, nb_grid_pts, physical_sizes, young, heights,
                           solver_kwargs, time.perf_counter() if arrival is None else arrival)
             self._next_id += 1
-            self._pending.append(req)
+            if self._is_large(req):
+                self._large.append(req)
+            else:
+                self._pending.append(req)
         self._wake.set()
+        self._large_wake.set()
         return req
 
     def cancel(self, req):
@@ -139,7 +160,10 @@ class ContactServer:
             try:
                 self._pending.remove(req)
             except ValueError:
-                return False
+                try:
+                    self._large.remove(req)
+                except ValueError:
+                    return False
         req.error = RuntimeError("cancelled")
         req.finished = time.perf_counter()
         req.done_event.set()
@@ -147,7 +171,7 @@ class ContactServer:
 
     @property
     def n_pending(self):
-        return len(self._pending)
+        return len(self._pending) + len(self._large)
 
     @property
     def n_active(self):
@@ -156,6 +180,8 @@ class ContactServer:
     def step(self):
         """One scheduling round: admit, advance, hand over, retire.
         Returns the number of solves in flight after the round."""
+        if self._worker is None and self._large:
+            self._solve_next_large()  # no worker thread: solve it here
         self._admit()
         if not self._active:
             return 0
@@ -185,8 +211,9 @@ class ContactServer:
 
     def run_until_idle(self, timeout=None):
         t0 = time.perf_counter()
-        while self._pending or self._active:
-            self.step()
+        while self._pending or self._active or self._large or self._large_busy:
+            if not self.step() and self._worker is not None:
+                time.sleep(0.0005)
             if timeout is not None and time.perf_counter() - t0 > timeout:
                 raise TimeoutError("server did not drain")
 
@@ -196,26 +223,48 @@ class ContactServer:
             return
         self._stop.clear()
 
+        # each thread works on a stream of its own (torch streams do not wait
+        # for other streams), so the loop's and the worker's small tensor
+        # operations do not serialise against each other's solves
+        device = self._torch.cuda.current_device()
+
         def loop():
             torch = self._torch
-            torch.cuda.set_device(torch.cuda.current_device())
-            while not self._stop.is_set():
-                if not self._pending and not self._active:
-                    self._wake.wait(0.001)
-                    self._wake.clear()
-                    continue
-                self.step()
+            torch.cuda.set_device(device)
+            with torch.cuda.stream(torch.cuda.Stream()):
+                while not self._stop.is_set():
+                    if not self._pending and not self._active:
+                        self._wake.wait(0.001)
+                        self._wake.clear()
+                        continue
+                    self.step()
 
         self._thread = threading.Thread(target=loop, daemon=True)
         self._thread.start()
+
+        def large_loop():
+            torch = self._torch
+            torch.cuda.set_device(device)
+            with torch.cuda.stream(torch.cuda.Stream()):
+                while not self._stop.is_set():
+                    if not self._solve_next_large():
+                        self._large_wake.wait(0.001)
+                        self._large_wake.clear()
+
+        self._worker = threading.Thread(target=large_loop, daemon=True)
+        self._worker.start()
 
     def stop(self):
         if self._thread is None:
             return
         self._stop.set()
         self._wake.set()
+        self._large_wake.set()
         self._thread.join()
         self._thread = None
+        if self._worker is not None:
+            self._worker.join()
+            self._worker = None
 
     def close(self):
         self.stop()
@@ -224,6 +273,46 @@ class ContactServer:
             self._stepper = None
 
     # -------------------------------------------------------------- internals
+    def _is_large(self, req):
+        if self.large_points is None:
+            return False
+        f = 2 if req.kind == "free" else 1
+        return f * f * int(np.prod(req.nb_grid_pts)) >= self.large_points
+
+    def _solve_next_large(self):
+        """Solve the oldest waiting large request with the single-solve path;
+        False if there was none."""
+        with self._lock:
+            if not self._large:
+                return False
+            req = self._large.popleft()
+            self._large_busy = True
+        try:
+            with self._lock:
+                sub = self._substrate(req)
+            kw = dict(req.solver_kwargs)
+            kw.setdefault("precision", self.precision)
+            try:
+                r = constrained_conjugate_gradients(sub, req.heights, **kw)
+                for key in ("x", "jac", "active_set", "plastic"):
+                    v = getattr(r, key, None)
+                    if v is not None and hasattr(v, "cpu"):
+                        setattr(r, key, v.cpu().numpy())
+                req.result_value = r
+                req.finished = time.perf_counter()
+                r.latency_s = req.latency_s
+                self.completed.append(req)
+            except Exception as exc:  # invalid request: report it, keep serving
+                req.error = exc
+                req.finished = time.perf_counter()
+            finally:
+                with self._lock:
+                    self._pool[req.key].append(sub)
+            req.done_event.set()
+        finally:
+            self._large_busy = False
+        return True
+
     def _substrate(self, req):
         pool = self._pool[req.key]
         if pool:

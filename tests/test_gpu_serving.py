@@ -106,3 +106,41 @@ def test_cancel_pending_request(cm):
         assert srv.n_pending == 0
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("threaded", [True, False])
+def test_large_requests_take_the_single_solve_path(cm, threaded):
+    """Requests of at least ``large_points`` domain points are solved one at a
+    time by the single-solve path, concurrently with the batched small ones
+    (or inline without the loop thread): their results equal
+    constrained_conjugate_gradients bit for bit; the small ones stay within
+    1e-6 of the FP64 single solve."""
+    from contactmechanics_b200.Serving import ContactServer
+    reqs = _requests()
+    srv = ContactServer(iters_per_step=4, large_points=6000)
+    try:
+        if threaded:
+            srv.start()
+        handles = [srv.submit(k, nb, (1.0, 1.0), h, **kw) for k, nb, h, kw in reqs]
+        if not threaded:
+            srv.run_until_idle(timeout=120)
+        results = [r.result(timeout=120) for r in handles]
+    finally:
+        srv.close()
+    n_large = 0
+    for (kind, nb, h, kw), rm in zip(reqs, results):
+        assert rm.success and rm.latency_s > 0
+        cls = cm.FreeFFTElasticHalfSpace if kind == "free" else cm.PeriodicFFTElasticHalfSpace
+        sub = cls(nb, 1.0, (1.0, 1.0))
+        points = (4 if kind == "free" else 1) * nb[0] * nb[1]
+        if points >= 6000:
+            n_large += 1
+            rs = cm.constrained_conjugate_gradients(sub, h, precision="mixed", **kw)
+            assert np.array_equal(rs.x, rm.x) and np.array_equal(rs.jac, rm.jac)
+            assert rs.nit == rm.nit
+        else:
+            rs = cm.constrained_conjugate_gradients(sub, h, precision="fp64", **kw)
+            xs = rs.x[:nb[0], :nb[1]]
+            rel = np.linalg.norm(rm.x[:nb[0], :nb[1]] - xs) / np.linalg.norm(xs)
+            assert rel < 1e-6, rel
+    assert 0 < n_large < len(reqs)
