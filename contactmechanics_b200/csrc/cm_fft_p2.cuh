@@ -131,3 +131,156 @@ CM_DEVINL void fft_p2(C (&v)[8], C* sA, C* sB, int base, int estride, int tt, co
     Ns *= 8;
   }
 }
+
+// ---------------------------------------------------------------------------
+// 2^LR elements per thread (LR = 3 or 4): the same scheme with radix-16
+// stages for LR = 4, fewer stages and exchanges per transform.
+// ---------------------------------------------------------------------------
+template <int LOGN, int LR>
+struct P2PlanR {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int RAD = 1 << LR;
+  static constexpr int TPS = N / RAD;  // threads per sequence
+  static constexpr int LTPS = LOGN - LR;
+  static constexpr int FL = (LOGN % LR == 0) ? LR : LOGN % LR;
+  static constexpr int FIRST = 1 << FL;
+  static constexpr int NST = 1 + (LOGN - FL) / LR;
+};
+
+// a * W16^M (W16 = exp(-2 pi i / 16); conjugate for the inverse), M in
+// {1, 2, 3, 4, 6, 9}: the internal twiddles of the length-16 DFT
+template <bool INV, int M, typename C>
+CM_DEVINL C w16(C a) {
+  typedef decltype(a.x) R;
+  const R c1 = (R)0.92387953251128675613;  // cos(pi/8)
+  const R s1 = (R)0.38268343236508977173;  // sin(pi/8)
+  const R h = (R)0.70710678118654752440;   // sqrt(1/2)
+  if (M == 4) return mul_mi<INV>(a);
+  R wr, wi;  // forward W16^M = wr + i wi
+  if (M == 1) { wr = c1; wi = -s1; }
+  else if (M == 2) { wr = h; wi = -h; }
+  else if (M == 3) { wr = s1; wi = -c1; }
+  else if (M == 6) { wr = -h; wi = -h; }
+  else { wr = -c1; wi = s1; }  // M == 9
+  if (INV) wi = -wi;
+  return cmake<C>(a.x * wr - a.y * wi, a.x * wi + a.y * wr);
+}
+
+// Length-16 DFT in place, as 4 x 4: X[k1 + 4 k2] =
+// sum_n2 W4^(n2 k2) W16^(n2 k1) sum_n1 x[4 n1 + n2] W4^(n1 k1).
+template <bool INV, typename C>
+CM_DEVINL void dft16(C (&v)[16]) {
+  C y[4][4];  // y[n2][k1]
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    C a = v[n2], b = v[4 + n2], c = v[8 + n2], d = v[12 + n2];
+    dft4<INV>(a, b, c, d);
+    y[n2][0] = a; y[n2][1] = b; y[n2][2] = c; y[n2][3] = d;
+  }
+  y[1][1] = w16<INV, 1>(y[1][1]);
+  y[1][2] = w16<INV, 2>(y[1][2]);
+  y[1][3] = w16<INV, 3>(y[1][3]);
+  y[2][1] = w16<INV, 2>(y[2][1]);
+  y[2][2] = w16<INV, 4>(y[2][2]);
+  y[2][3] = w16<INV, 6>(y[2][3]);
+  y[3][1] = w16<INV, 3>(y[3][1]);
+  y[3][2] = w16<INV, 6>(y[3][2]);
+  y[3][3] = w16<INV, 9>(y[3][3]);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C a = y[0][k1], b = y[1][k1], c = y[2][k1], d = y[3][k1];
+    dft4<INV>(a, b, c, d);
+    v[k1] = a; v[k1 + 4] = b; v[k1 + 8] = c; v[k1 + 12] = d;
+  }
+}
+
+template <bool INV, int R, typename C>
+CM_DEVINL void dft_rr(C* v) {
+  if constexpr (R == 16) dft16<INV>(*reinterpret_cast<C(*)[16]>(v));
+  else dft_r<INV, R>(v);
+}
+
+// Per-stage twiddle tables for 2^LR elements per thread: stage s (Ns butterfly
+// groups) holds tw[toff(s) + (q-1)*Ns + k] = W^(q k N/(RAD Ns)), q = 1..RAD-1,
+// k < Ns; at most N entries in all.  Entries of the table tw_n[m] = W^m.
+template <int LOGN, int LR, typename C>
+CM_DEVINL void stage_tw_p2r(C* tws, const C* __restrict__ tw_n) {
+  typedef P2PlanR<LOGN, LR> P;
+  constexpr int N = P::N, RAD = P::RAD;
+  int toff = 0;
+#pragma unroll
+  for (int s = 1, Ns = P::FIRST; s < P::NST; ++s, Ns *= RAD) {
+    const int step = N / (Ns * RAD);
+    for (int i = threadIdx.x; i < (RAD - 1) * Ns; i += blockDim.x) {
+      const int q = 1 + i / Ns, k = i & (Ns - 1);
+      tws[toff + i] = __ldg(tw_n + ((q * k * step) & (N - 1)));
+    }
+    toff += (RAD - 1) * Ns;
+  }
+}
+
+// Transform the thread's RAD elements {tt + q N/RAD} of one sequence in
+// place (same contract as fft_p2, tables of stage_tw_p2r).
+template <typename C, bool INV, int LOGN, int LR>
+CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int tt,
+                       const C* tw) {
+  typedef P2PlanR<LOGN, LR> P;
+  constexpr int RAD = P::RAD;
+  {
+    constexpr int R = P::FIRST;
+    constexpr int B = RAD / R;
+    C o[RAD];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+      C g[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) g[q] = v[i + B * q];
+      dft_rr<INV, R>(g);
+#pragma unroll
+      for (int q = 0; q < R; ++q) o[i * R + q] = g[q];
+    }
+    if (P::NST == 1) {
+#pragma unroll
+      for (int i = 0; i < RAD; ++i) v[i] = o[i];
+      return;
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+      const int j = tt + i * P::TPS;
+#pragma unroll
+      for (int q = 0; q < R; ++q) sA[spad(base + (j * R + q) * estride)] = o[i * R + q];
+    }
+  }
+  __syncthreads();
+  C* src = sA;
+  C* dst = sB;
+  int Ns = P::FIRST;
+  int toff = 0;
+#pragma unroll
+  for (int s = 1; s < P::NST; ++s) {
+    const int k = tt & (Ns - 1);
+    C g[RAD];
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) g[q] = src[spad(base + (tt + q * P::TPS) * estride)];
+#pragma unroll
+    for (int q = 1; q < RAD; ++q) {
+      const C w = tw[toff + (q - 1) * Ns + k];
+      g[q] = INV ? cmulc(g[q], w) : cmul(g[q], w);
+    }
+    toff += (RAD - 1) * Ns;
+    dft_rr<INV, RAD>(g);
+    if (s == P::NST - 1) {
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) v[q] = g[q];
+    } else {
+      const int ob = (tt - k) * RAD + k;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) dst[spad(base + (ob + q * Ns) * estride)] = g[q];
+      __syncthreads();
+      C* t = src;
+      src = dst;
+      dst = t;
+    }
+    Ns *= RAD;
+  }
+}

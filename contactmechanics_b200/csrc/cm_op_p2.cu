@@ -56,8 +56,44 @@ int row_fwd(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   return 0;
 }
 
+template <typename R, int LOGN, typename K>
+int prepare16(K kernel, KernelInfo& info) {
+  typedef OpShape16<R, LOGN> Sh;
+  if (info.ready) return info.grid_per_sm > 0 ? 0 : -1;
+  const size_t smem = Sh::smem();
+  if (cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 1;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, Sh::THREADS, smem) != cudaSuccess)
+    return 1;
+  info.grid_per_sm = per_sm;
+  info.ready = true;
+  return per_sm > 0 ? 0 : -1;
+}
+
+// FP32 column pass with 16 elements per thread
+template <typename R, int LOGN>
+int col16(const OpArgs<R>& a, cudaStream_t s, bool launch) {
+  typedef OpShape16<R, LOGN> Sh;
+  static KernelInfo info;
+  if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(g_op_mu);
+    rc = prepare16<R, LOGN>(k_op_col16<R, LOGN>, info);
+  }
+  if (rc || !launch) return rc;
+  const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
+  const int groups = (a.ntile_cols + per_block - 1) / per_block;
+  const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
+  k_op_col16<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  return 0;
+}
+
 template <typename R, int LOGN>
 int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
+  if constexpr (sizeof(R) == 4) return col16<R, LOGN>(a, s, launch);
   typedef OpShape<R, LOGN> Sh;
   static KernelInfo info;
   if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;  // a column tile wider than a block

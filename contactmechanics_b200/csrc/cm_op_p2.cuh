@@ -146,6 +146,71 @@ k_op_col(OpArgs<R> a) {
   }
 }
 
+// Column pass with 16 elements per thread (radix-16 stages, fft_p2r): two
+// shared-memory exchanges per transform of length 2048 instead of three.
+template <typename R, int LOGN>
+struct OpShape16 {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int TPS = N / 16;
+  static constexpr int THREADS = TPS > 256 ? TPS : 256;
+  static constexpr int NP = THREADS / TPS;  // columns per block
+  static size_t smem() {
+    return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
+  }
+};
+
+template <typename R, int LOGN>
+__global__ void __launch_bounds__(OpShape16<R, LOGN>::THREADS, 2)
+k_op_col16(OpArgs<R> a) {
+  typedef typename CT<R>::C C;
+  typedef P2PlanR<LOGN, 4> P;
+  typedef OpShape16<R, LOGN> Sh;
+  constexpr int N = P::N;
+  if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(Sh::NP * N);
+  stage_tw_p2r<LOGN, 4>(tws, a.twx);
+  __syncthreads();
+  const int lw = a.lw, W = 1 << lw;
+  const int c = threadIdx.x & (W - 1);
+  const int tt = (threadIdx.x >> lw) & (P::TPS - 1);
+  const int j = threadIdx.x >> (lw + P::LTPS);
+  const int tiles_per_block = blockDim.x >> (lw + P::LTPS);
+  const int ngroups = (a.ntile_cols + tiles_per_block - 1) / tiles_per_block;
+  const int base = j * N * W + c;
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int tile = grp * tiles_per_block + j;
+    const bool tile_ok = tile < a.ntile_cols;
+    const int wc = tile_ok ? min(W, a.nyh - tile * W) : 0;
+    const bool col_ok = c < wc;
+    C* __restrict__ blk = a.spec + (size_t)tile * N * W;
+    const R* __restrict__ tblk = a.tab + (size_t)tile * N * W;
+    C v[16];
+    R g[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int x = tt + q * P::TPS;
+      v[q] = (col_ok && x < a.in_rows) ? blk[x * W + c] : czero<C>();
+      g[q] = col_ok ? __ldg(tblk + x * W + c) : (R)0;
+    }
+    fft_p2r<C, false, LOGN, 4>(v, bufA, bufB, base, W, tt, tws);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = cscale(v[q], g[q]);
+    __syncthreads();
+    fft_p2r<C, true, LOGN, 4>(v, bufA, bufB, base, W, tt, tws);
+    if (col_ok) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int x = tt + q * P::TPS;
+        if (x < a.out_rows) blk[x * W + c] = v[q];
+      }
+    }
+    __syncthreads();  // buffers free for the next group
+  }
+}
+
 template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_op_row_inv(OpArgs<R> a) {
