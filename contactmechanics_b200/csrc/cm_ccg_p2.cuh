@@ -11,9 +11,12 @@
 //                          and maximum;
 //   k_ccg_row_inv<MODE_T>  r = G t, sum r t -> step length (:287-294);
 //   k_ccg_row_inv<MODE_F>  u = G f on the whole domain, max |du|, maximum
-//                          penetration, convergence test (:391-434).
+//                          penetration, convergence test (:391-434), and the
+//                          next iteration's start (the statistics of
+//                          k_ccg_begin, :239-270, 300-318), so an iteration
+//                          after the first launches no k_ccg_begin.
 //
-// The column pass between them is k_op_col with the solve's state attached.
+// The column pass between them is k_op_col16 with the solve's state attached.
 // Each tile writes its reduction partials and the last tile to finish runs
 // the scalar step (tile_finish), as in the per-pass kernels.
 #pragma once
@@ -166,7 +169,6 @@ k_ccg_row_inv(CcgArgs<R> a) {
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, nx = a.op.nx;
   const int rows_total = (MODE == MODE_T) ? tx : nx;
-  const int lw = a.op.lw, W = 1 << lw, nkb = (a.op.nyh + W - 1) >> lw;
   const int ntiles = (rows_total + ROWS - 1) / ROWS;
   const R off = (R)cv.offset;
   const R hdn = neg_down<R>(cv.H);
@@ -177,22 +179,8 @@ k_ccg_row_inv(CcgArgs<R> a) {
   const unsigned char* __restrict__ gneg = a.gneg;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS;
-    // gather the row pairs' half spectra; e = ((kb * NP) + p) * W + kw
-    const int total = nkb * NP * W;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int kw = e & (W - 1);
-      const int p = (e >> lw) & (NP - 1);
-      const int kb = e >> (lw + Sh::LNP);
-      const int k = kb * W + kw, xa = x0 + 2 * p;
-      if (k >= a.op.nyh || xa >= rows_total) continue;
-      const size_t ia = ((size_t)kb * nx + xa) * W + kw;
-      C X = a.op.spec[ia];
-      C Y = (xa + 1 < rows_total) ? a.op.spec[ia + W] : czero<C>();
-      const bool selfconj = (k == 0) || (2 * k == N);
-      if (selfconj) { X.y = 0; Y.y = 0; }
-      bufA[spad(p * N + k)] = cmake<C>(X.x - Y.y, X.y + Y.x);
-      if (!selfconj) bufA[spad(p * N + N - k)] = cmake<C>(X.x + Y.y, Y.x - X.y);
-    }
+    gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.op.spec, nx, a.op.nyh, a.op.lw, x0,
+                                                      rows_total);
     __syncthreads();
     C v[8];
 #pragma unroll
@@ -213,51 +201,70 @@ k_ccg_row_inv(CcgArgs<R> a) {
       tile_finish<1>(a.partials, a.counter, tile, ntiles, vr, kinds,
                      [&](double (&r)[1]) { fin_tau(*st, r); });
     } else {
+      // u on the whole domain, max |du| and the maximum penetration; on the
+      // topography also the start-of-iteration statistics of the next
+      // iteration (k_ccg_begin: contact areas, sum of the gaps over the CG
+      // area, extreme gaps; ConstrainedConjugateGradients.py:239-270) from
+      // the new displacement and the iteration's final force f[par ^ 1]
       R du = 0, pmax = -INFINITY;  // extrema, exact in R
-      // every input of the thread's 16 elements first, then the stores
-      R uo[2][8], hv[2][8];
-      bool cc[2][8];
-#pragma unroll
-      for (int w = 0; w < 2; ++w) {
-        const int x = xa + w;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int y = tt + q * P::TPS;
-          uo[w][q] = 0; hv[w][q] = 0; cc[w][q] = false;
-          if (x >= rows_total) continue;
-          uo[w][q] = u_io[(size_t)x * N + y];
-          if (x < tx && y < ty) {
-            const size_t ic = (size_t)x * ty + y;
-            hv[w][q] = h_in[ic];
-            if (cv.branch == 0) {
-              const R fa = fa_buf[ic];
-              cc[w][q] = (fa < 0) && (!cv.has_h || fa > hdn);
-            } else {
-              cc[w][q] = gneg[ic] != 0;
-            }
-          }
-        }
-      }
+      R gmax = -INFINITY, gmin = INFINITY;
+      int n_c = 0, n_cg = 0;  // counts, exact in int
+      double s_cg = 0;
+      const R* __restrict__ fn_buf = a.f[cv.par ^ 1];
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w;
         if (x >= rows_total) continue;
+        // every input of the row's 8 elements first, then the stores
+        R uo[8], hv[8], fn[8];
+        bool cc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          hv[q] = 0; fn[q] = 0; cc[q] = false;
+          uo[q] = u_io[(size_t)x * N + y];
+          if (x < tx && y < ty) {
+            const size_t ic = (size_t)x * ty + y;
+            hv[q] = h_in[ic];
+            fn[q] = fn_buf[ic];
+            if (cv.branch == 0) {
+              const R fa = fa_buf[ic];
+              cc[q] = (fa < 0) && (!cv.has_h || fa > hdn);
+            } else {
+              cc[q] = gneg[ic] != 0;
+            }
+          }
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int y = tt + q * P::TPS;
           const R val = w ? v[q].y : v[q].x;
-          du = fmax(du, fabs(val - uo[w][q]));
+          du = fmax(du, fabs(val - uo[q]));
           u_io[(size_t)x * N + y] = val;
           if (x < tx && y < ty) {
-            const R pen = (hv[w][q] + off) - val;
-            pmax = fmax(pmax, cc[w][q] ? pen : (R)0);
+            const R pen = (hv[q] + off) - val;
+            pmax = fmax(pmax, cc[q] ? pen : (R)0);
+            const bool c0 = fn[q] < 0;
+            const bool c = c0 && (!cv.has_h || fn[q] > hdn);
+            const R g = val - hv[q];
+            n_c += c0;
+            n_cg += c;
+            if (c) s_cg += (double)g;
+            gmax = fmax(gmax, g);
+            gmin = fmin(gmin, g);
           }
         }
       }
-      double vr[2] = {(double)du, (double)pmax};
-      const int kinds[2] = {RED_MAX, RED_MAX};
-      tile_finish<2>(a.partials, a.counter, tile, ntiles, vr, kinds,
-                     [&](double (&r)[2]) { ccg_converge(*st, r[0], r[1]); });
+      double vr[7] = {(double)du, (double)pmax, (double)n_c, (double)n_cg, s_cg, (double)gmax,
+                      (double)gmin};
+      const int kinds[7] = {RED_MAX, RED_MAX, RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
+      tile_finish<7>(a.partials, a.counter, tile, ntiles, vr, kinds, [&](double (&r)[7]) {
+        ccg_converge(*st, r[0], r[1]);
+        if (!st->done) {
+          double b[5] = {r[2], r[3], r[4], r[5], r[6]};
+          fin_begin(*st, b);
+        }
+      });
     }
     __syncthreads();  // buffers free for the next tile
   }

@@ -72,9 +72,9 @@ int prepare16(K kernel, KernelInfo& info) {
   return per_sm > 0 ? 0 : -1;
 }
 
-// FP32 column pass with 16 elements per thread
+// column pass: 16 elements per thread (k_op_col16)
 template <typename R, int LOGN>
-int col16(const OpArgs<R>& a, cudaStream_t s, bool launch) {
+int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   typedef OpShape16<R, LOGN> Sh;
   static KernelInfo info;
   if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;
@@ -88,25 +88,6 @@ int col16(const OpArgs<R>& a, cudaStream_t s, bool launch) {
   const int groups = (a.ntile_cols + per_block - 1) / per_block;
   const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
   k_op_col16<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
-  return 0;
-}
-
-template <typename R, int LOGN>
-int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
-  if constexpr (sizeof(R) == 4) return col16<R, LOGN>(a, s, launch);
-  typedef OpShape<R, LOGN> Sh;
-  static KernelInfo info;
-  if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;  // a column tile wider than a block
-  int rc;
-  {
-    std::lock_guard<std::mutex> g(g_op_mu);
-    rc = prepare<R, LOGN>(k_op_col<R, LOGN>, info);
-  }
-  if (rc || !launch) return rc;
-  const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
-  const int groups = (a.ntile_cols + per_block - 1) / per_block;
-  const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
-  k_op_col<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
   return 0;
 }
 

@@ -5,7 +5,7 @@
 //   k_op_row_fwd  rows x < in_rows: packed real-to-complex row transforms
 //                 (two rows per complex transform), half spectrum written
 //                 into the plan's column-tiled spectrum;
-//   k_op_col      every column tile: forward transform along x (input rows
+//   k_op_col16    every column tile: forward transform along x (input rows
 //                 >= in_rows are zero), times the real Green's table,
 //                 inverse transform, rows < out_rows written back;
 //   k_op_row_inv  rows x < out_rows: complex-to-real row transforms, output
@@ -14,9 +14,9 @@
 // Arguments travel by value (no descriptor upload), so a call is a plain
 // sequence of three launches on the caller's stream.  Blocks walk their
 // tiles with a grid stride, so the twiddle tables are staged once per block.
-// A block covers 2*NP rows (row passes) or several column tiles (column
-// pass) with N/8 threads per transform, the register-resident engine of
-// cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
+// A block covers 2*NP rows (row passes, N/8 threads per transform) or
+// several column tiles (column pass, N/16 threads per transform), the
+// register-resident engines of cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
 // touches whole rows-of-a-tile runs: (row, column-in-tile) fastest, which in
 // the plan's layout ((k >> lw) * nx + x) * W + (k & (W-1)) are contiguous.
 #pragma once
@@ -33,12 +33,62 @@ struct OpShape {
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
   static constexpr int MINB = sizeof(R) == 8 ? 1 : 2;
+  // block strides of a row-pair gather whose loads are issued together (the
+  // gather of a row tile with column tiles W <= N/8 takes at most five); the
+  // FP64 passes have the registers to spare, the FP32 ones do not
+  static constexpr int GATHER = sizeof(R) == 8 ? 5 : 1;
   static constexpr int LNP = NP >= 512 ? 9 : NP >= 256 ? 8 : NP >= 128 ? 7 : NP >= 64 ? 6 : NP >= 32 ? 5
                              : NP >= 16 ? 4 : NP >= 8 ? 3 : NP >= 4 ? 2 : NP >= 2 ? 1 : 0;
   static size_t smem() {
     return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
   }
 };
+
+// Gathers the half spectra of the row pairs x0 + 2p, x0 + 2p + 1 (p < NP,
+// rows >= rows_total read as zero) from the column-tiled spectrum and packs
+// each pair into one full-length complex sequence in buf (Z = X + iY with the
+// Hermitian halves filled in).  Element e = ((kb * NP) + p) * W + kw; the
+// loads of U consecutive strides are issued before any of them is used, so a
+// thread has 2U loads in flight.
+template <typename C, int LOGN, int NP, int LNP, int U>
+CM_DEVINL void gather_row_pairs(C* buf, const C* __restrict__ spec, int nx, int nyh, int lw,
+                                int x0, int rows_total) {
+  constexpr int N = 1 << LOGN;
+  const int W = 1 << lw, nkb = (nyh + W - 1) >> lw;
+  const int total = nkb * NP * W;
+  const int T = blockDim.x;
+  for (int e0 = threadIdx.x; e0 < total; e0 += U * T) {
+    C X[U], Y[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = e0 + i * T;
+      const int kw = e & (W - 1);
+      const int p = (e >> lw) & (NP - 1);
+      const int kb = e >> (lw + LNP);
+      const int k = kb * W + kw, xa = x0 + 2 * p;
+      X[i] = czero<C>();
+      Y[i] = czero<C>();
+      if (e >= total || k >= nyh || xa >= rows_total) continue;
+      const size_t ia = ((size_t)kb * nx + xa) * W + kw;
+      X[i] = spec[ia];
+      if (xa + 1 < rows_total) Y[i] = spec[ia + W];
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = e0 + i * T;
+      const int kw = e & (W - 1);
+      const int p = (e >> lw) & (NP - 1);
+      const int kb = e >> (lw + LNP);
+      const int k = kb * W + kw, xa = x0 + 2 * p;
+      if (e >= total || k >= nyh || xa >= rows_total) continue;
+      C x = X[i], y = Y[i];
+      const bool selfconj = (k == 0) || (2 * k == N);
+      if (selfconj) { x.y = 0; y.y = 0; }
+      buf[spad(p * N + k)] = cmake<C>(x.x - y.y, x.y + y.x);
+      if (!selfconj) buf[spad(p * N + N - k)] = cmake<C>(x.x + y.y, y.x - x.y);
+    }
+  }
+}
 
 template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
@@ -93,74 +143,23 @@ k_op_row_fwd(OpArgs<R> a) {
   }
 }
 
-template <typename R, int LOGN>
-__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
-k_op_col(OpArgs<R> a) {
-  typedef typename CT<R>::C C;
-  typedef P2Plan<LOGN> P;
-  typedef OpShape<R, LOGN> Sh;
-  constexpr int N = P::N;
-  if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
-  C* bufB = bufA + smem_padded(Sh::NP * N);
-  stage_tw_p2<LOGN>(tws, a.twx);
-  __syncthreads();
-  const int lw = a.lw, W = 1 << lw;
-  // thread -> (tile of the block j, column c of the tile, element group tt)
-  const int c = threadIdx.x & (W - 1);
-  const int tt = (threadIdx.x >> lw) & (P::TPS - 1);
-  const int j = threadIdx.x >> (lw + P::LTPS);
-  const int tiles_per_block = blockDim.x >> (lw + P::LTPS);
-  const int ngroups = (a.ntile_cols + tiles_per_block - 1) / tiles_per_block;
-  const int base = j * N * W + c;
-  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int tile = grp * tiles_per_block + j;
-    const bool tile_ok = tile < a.ntile_cols;
-    const int wc = tile_ok ? min(W, a.nyh - tile * W) : 0;
-    const bool col_ok = c < wc;
-    C* __restrict__ blk = a.spec + (size_t)tile * N * W;
-    const R* __restrict__ tblk = a.tab + (size_t)tile * N * W;
-    C v[8];
-    R g[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int x = tt + q * P::TPS;
-      v[q] = (col_ok && x < a.in_rows) ? blk[x * W + c] : czero<C>();
-      g[q] = col_ok ? __ldg(tblk + x * W + c) : (R)0;
-    }
-    fft_p2<C, false, LOGN>(v, bufA, bufB, base, W, tt, tws);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = cscale(v[q], g[q]);
-    __syncthreads();
-    fft_p2<C, true, LOGN>(v, bufA, bufB, base, W, tt, tws);
-    if (col_ok) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int x = tt + q * P::TPS;
-        if (x < a.out_rows) blk[x * W + c] = v[q];
-      }
-    }
-    __syncthreads();  // buffers free for the next group
-  }
-}
-
 // Column pass with 16 elements per thread (radix-16 stages, fft_p2r): two
-// shared-memory exchanges per transform of length 2048 instead of three.
+// shared-memory exchanges per transform of length 2048 instead of the three
+// of the 8-element engine.
 template <typename R, int LOGN>
 struct OpShape16 {
   static constexpr int N = 1 << LOGN;
   static constexpr int TPS = N / 16;
   static constexpr int THREADS = TPS > 256 ? TPS : 256;
   static constexpr int NP = THREADS / TPS;  // columns per block
+  static constexpr int MINB = sizeof(R) == 4 ? 2 : 1;
   static size_t smem() {
     return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
   }
 };
 
 template <typename R, int LOGN>
-__global__ void __launch_bounds__(OpShape16<R, LOGN>::THREADS, 2)
+__global__ void __launch_bounds__(OpShape16<R, LOGN>::THREADS, OpShape16<R, LOGN>::MINB)
 k_op_col16(OpArgs<R> a) {
   typedef typename CT<R>::C C;
   typedef P2PlanR<LOGN, 4> P;
@@ -225,26 +224,10 @@ k_op_row_inv(OpArgs<R> a) {
   stage_tw_p2<LOGN>(tws, a.twy);
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
-  const int W = 1 << a.lw, nkb = (a.nyh + W - 1) >> a.lw;
   const int ntiles = (a.out_rows + ROWS - 1) / ROWS;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS;
-    // gather the row pairs' half spectra; e = ((kb * NP) + p) * W + kw
-    const int total = nkb * NP * W;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int kw = e & (W - 1);
-      const int p = (e >> a.lw) & (NP - 1);
-      const int kb = e >> (a.lw + Sh::LNP);
-      const int k = kb * W + kw, xa = x0 + 2 * p;
-      if (k >= a.nyh || xa >= a.out_rows) continue;
-      const size_t ia = ((size_t)kb * a.nx + xa) * W + kw;
-      C X = a.spec[ia];
-      C Y = (xa + 1 < a.out_rows) ? a.spec[ia + W] : czero<C>();
-      const bool selfconj = (k == 0) || (2 * k == N);
-      if (selfconj) { X.y = 0; Y.y = 0; }
-      bufA[spad(p * N + k)] = cmake<C>(X.x - Y.y, X.y + Y.x);
-      if (!selfconj) bufA[spad(p * N + N - k)] = cmake<C>(X.x + Y.y, Y.x - X.y);
-    }
+    gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.spec, a.nx, a.nyh, a.lw, x0, a.out_rows);
     __syncthreads();
     C v[8];
 #pragma unroll

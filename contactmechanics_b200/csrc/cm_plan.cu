@@ -631,7 +631,8 @@ static int init_work(cm_plan* p, Work<R>& w) {
   const int nt_max = std::max({(p->tx + w.tiles.comp_rows - 1) / w.tiles.comp_rows,
                                (p->nx + w.tiles.row_tile - 1) / w.tiles.row_tile,
                                w.tiles.ntile_cols, 1});
-  CKS(dalloc(p, &w.partials, (size_t)nt_max * CM_MAX_PARTIAL_VALS));
+  // (the by-value row passes use tiles of at least two rows: at most nx tiles)
+  CKS(dalloc(p, &w.partials, (size_t)std::max(nt_max, p->nx) * CM_MAX_PARTIAL_VALS));
   CKS(dalloc(p, &w.counter, 1));
   CK(cudaMemset(w.counter, 0, sizeof(unsigned int)));
   CKS(dalloc(p, &w.st, 1));
@@ -780,14 +781,16 @@ static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int
 // ---------------------------------------------------------------------------
 // ---- power-of-two specialisations -------------------------------------------
 
-// kernels of one iteration, in launch order (bisection passes excluded)
+// kernels of one iteration, in launch order (bisection passes excluded).  The
+// by-value passes launch no k_ccg_begin after the first iteration: the
+// previous iteration's k_ccg_row_inv<MODE_F> computes its statistics.
 #define CM_ITER_KERNELS 10
 static const char* const k_iter_names[CM_ITER_KERNELS] = {
     "k_ccg_begin", "k_ccg_gsum", "k_row_fwd<T>", "k_col<T>", "k_row_inv<T>",
     "k_ccg_update", "k_row_fwd<F>", "k_col<F>", "k_row_inv<F>", "k_ccg_bisect"};
 
-static int iteration_launches(bool bisect) {
-  return CM_ITER_KERNELS - 1 + (bisect ? CM_BISECT_PASSES : 0);
+static int iteration_launches(bool bisect, bool by_value) {
+  return CM_ITER_KERNELS - (by_value ? 2 : 1) + (bisect ? CM_BISECT_PASSES : 0);
 }
 
 // One CCG iteration.  With `ev` (CM_ITER_KERNELS + 1 events) an event is
@@ -801,7 +804,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], s); };
   mark();
-  k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  if (!w.by_value) k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
   if (bisect)
     for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
   mark();
@@ -985,6 +988,11 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
                    int prof_iters = 0, float* prof_ms = nullptr) {
   cudaStream_t s = p->stream;
   CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
+  if (w.by_value) {
+    // start of the first iteration; later ones come from k_ccg_row_inv<MODE_F>
+    k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items);
+    g_launches += 1;
+  }
   const bool bisect = prm->has_hardness && prm->load_control;
   if (prof_iters > 0 && w.persist) {
     // profiler: one cooperative launch of prof_iters iterations timed with
@@ -1068,7 +1076,7 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   CKS(get_graph<R>(p, w, bisect, every, &g));
   for (int done_iters = 0;; done_iters += every) {
     CK(cudaGraphLaunch(g, s));
-    g_launches += (unsigned long long)every * iteration_launches(bisect);
+    g_launches += (unsigned long long)every * iteration_launches(bisect, w.by_value);
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     ++g_polls;
@@ -1229,7 +1237,7 @@ static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, do
   auto t0 = std::chrono::steady_clock::now();
   for (int done_iters = 0; running > 0; done_iters += every) {
     if (cudaGraphLaunch(ge, s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
-    g_launches += (unsigned long long)every * (iteration_launches(bisect)) + 1;
+    g_launches += (unsigned long long)every * (iteration_launches(bisect, false)) + 1;
     if (cudaMemcpyAsync(&running, b.running, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
     if (polls) ++*polls;
@@ -1349,7 +1357,7 @@ static int stepper_run(cm_stepper* stp, const std::vector<cm_plan*>& plans, int 
   }
   b.slots = (Slot<R>*)stp->d_slots;
   for (int it = 0; it < iters; ++it) launch_iteration_batch<R>(b, bisect, s);
-  g_launches += (unsigned long long)iters * iteration_launches(bisect) + 1;
+  g_launches += (unsigned long long)iters * iteration_launches(bisect, false) + 1;
   k_collect_done<R><<<grid_for(n), 256, 0, s>>>(b.slots, n, stp->d_done);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(stp->h_done, stp->d_done, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
