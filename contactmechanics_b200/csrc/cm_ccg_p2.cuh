@@ -29,16 +29,18 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   typedef P2Plan<LOGN> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  pdl_trigger();
+  stage_tw_p2<LOGN>(tws, a.op.twy);
+  pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
   if (MODE == MODE_T && st->branch != 0) return;
   CcgView cv;
   load_view(st, cv);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
-  C* bufB = bufA + smem_padded(NP * N);
-  stage_tw_p2<LOGN>(tws, a.op.twy);
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, ny = N;
@@ -155,16 +157,18 @@ k_ccg_row_inv(CcgArgs<R> a) {
   typedef P2Plan<LOGN> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* bufA = tws + N;
+  C* bufB = bufA + smem_padded(NP * N);
+  pdl_trigger();
+  stage_tw_p2<LOGN>(tws, a.op.twy);
+  pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
   if (MODE == MODE_T && st->branch != 0) return;
   CcgView cv;
   load_view(st, cv);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
-  C* bufB = bufA + smem_padded(NP * N);
-  stage_tw_p2<LOGN>(tws, a.op.twy);
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, nx = a.op.nx;

@@ -43,6 +43,16 @@ template <bool INV, typename C> CM_DEVINL C mul_mi(C a) {
 template <typename C> CM_DEVINL C czero() { C r; r.x = 0; r.y = 0; return r; }
 template <typename C, typename R> CM_DEVINL C cmake(R x, R y) { C r; r.x = x; r.y = y; return r; }
 
+// Programmatic dependent launch.  pdl_trigger lets the next kernel of the
+// stream start launching (its blocks are placed as this grid's blocks leave
+// room); pdl_wait blocks until every preceding grid the launch depends on has
+// completed and its memory is visible.  A kernel launched without the
+// programmatic-serialization attribute was already ordered behind its
+// predecessor, and both are no-ops for it.  Kernels read only constant
+// inputs (twiddle tables, launch arguments) before pdl_wait.
+CM_DEVINL void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+CM_DEVINL void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 enum { RED_SUM = 0, RED_MAX = 1, RED_MIN = 2 };
 
 CM_DEVINL double red_neutral(int kind) {

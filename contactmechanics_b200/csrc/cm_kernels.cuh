@@ -667,6 +667,8 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  pdl_trigger();
+  pdl_wait();
   if (st->done) return;
   const int has_h = st->p.has_h;
   const R hdn = neg_down<R>(st->p.H);
@@ -704,6 +706,8 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  pdl_trigger();
+  pdl_wait();
   if (st->done || st->branch != 0) return;
   const int has_h = st->p.has_h;
   const R hdn = neg_down<R>(st->p.H);
@@ -737,6 +741,8 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  pdl_trigger();
+  pdl_wait();
   if (st->done || st->branch != 1 || !st->bs_active) return;
   __shared__ double cand[CM_BIS_CAND];
   __shared__ double cand_lo, cand_hi;
@@ -796,6 +802,8 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  pdl_trigger();
+  pdl_wait();
   if (st->done) return;
   const int par = st->parity, has_h = st->p.has_h, branch = st->branch;
   const double H = st->p.H;

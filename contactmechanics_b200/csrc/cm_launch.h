@@ -93,6 +93,26 @@ struct CcgArgs {
   unsigned int* counter;
   int tx, ty;
 };
+// Launch with programmatic stream serialization: the kernel may start while
+// its predecessor on the stream finishes, and calls pdl_wait before reading
+// anything an earlier kernel wrote.  Off when the environment sets CM_PDL=0.
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem,
+                              cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw);
 template <typename R>

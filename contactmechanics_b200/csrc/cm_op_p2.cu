@@ -1,9 +1,21 @@
-// Launcher of the power-of-two operator passes (cm_op_p2.cuh).
+// Launcher of the power-of-two operator passes (cm_op_p2.cuh).  The first
+// pass of a sequence (k_op_row_fwd of the operator) launches plainly; every
+// later one with programmatic stream serialization (launch_pdl).
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "cm_ccg_p2.cuh"
 #include "cm_launch.h"
 #include "cm_op_p2.cuh"
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("CM_PDL");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
 
 namespace {
 
@@ -87,7 +99,7 @@ int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
   const int groups = (a.ntile_cols + per_block - 1) / per_block;
   const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
-  k_op_col16<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  launch_pdl(k_op_col16<R, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);
   return 0;
 }
 
@@ -103,7 +115,7 @@ int row_inv(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   if (rc || !launch) return rc;
   const int tiles = (a.out_rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
-  k_op_row_inv<R, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  launch_pdl(k_op_row_inv<R, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);
   return 0;
 }
 
@@ -147,7 +159,7 @@ int ccg_row_fwd(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
   if (rc || !launch) return rc;
   const int tiles = (a.tx + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
-  k_ccg_row_fwd<R, MODE, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  launch_pdl(k_ccg_row_fwd<R, MODE, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);
   return 0;
 }
 
@@ -164,7 +176,7 @@ int ccg_row_inv(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
   const int rows = MODE == MODE_T ? a.tx : a.op.nx;
   const int tiles = (rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
-  k_ccg_row_inv<R, MODE, LOGN><<<grid, Sh::THREADS, Sh::smem(), s>>>(a);
+  launch_pdl(k_ccg_row_inv<R, MODE, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);
   return 0;
 }
 

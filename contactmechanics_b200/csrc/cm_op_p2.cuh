@@ -101,7 +101,9 @@ k_op_row_fwd(OpArgs<R> a) {
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
+  pdl_trigger();
   stage_tw_p2<LOGN>(tws, a.twy);
+  pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int W = 1 << a.lw, nkb = (a.nyh + W - 1) >> a.lw;
@@ -165,12 +167,14 @@ k_op_col16(OpArgs<R> a) {
   typedef P2PlanR<LOGN, 4> P;
   typedef OpShape16<R, LOGN> Sh;
   constexpr int N = P::N;
-  if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(Sh::NP * N);
+  pdl_trigger();
   stage_tw_p2r<LOGN, 4>(tws, a.twx);
+  pdl_wait();
+  if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   __syncthreads();
   const int lw = a.lw, W = 1 << lw;
   const int c = threadIdx.x & (W - 1);
@@ -221,7 +225,9 @@ k_op_row_inv(OpArgs<R> a) {
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
+  pdl_trigger();
   stage_tw_p2<LOGN>(tws, a.twy);
+  pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int ntiles = (a.out_rows + ROWS - 1) / ROWS;

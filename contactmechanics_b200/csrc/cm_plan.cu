@@ -795,20 +795,29 @@ static int iteration_launches(bool bisect, bool by_value) {
 
 // One CCG iteration.  With `ev` (CM_ITER_KERNELS + 1 events) an event is
 // recorded before the first and after every kernel, for the profiler.
+// The by-value passes launch with programmatic stream serialization, all but
+// the first kernel of a sequence (`first`: nothing of ours precedes it).
 template <typename R>
 static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s,
-                             cudaEvent_t* ev = nullptr) {
+                             cudaEvent_t* ev = nullptr, bool first = true) {
   const Slot<R>* S = w.d_ccg;
   const int2* it = p->items;
   const Tiles& T = w.tiles;
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], s); };
+  // an element-wise kernel: chained behind the previous pass in the by-value path
+  bool chain = w.by_value && !first;
+  auto elementwise = [&](void (*kern)(const Slot<R>*, const int2*)) {
+    if (chain) launch_pdl(kern, w.nt_comp, CM_THREADS, 0, s, S, it);
+    else kern<<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+    chain = w.by_value;
+  };
   mark();
-  if (!w.by_value) k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  if (!w.by_value) elementwise(k_ccg_begin<R>);
   if (bisect)
-    for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+    for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>);
   mark();
-  k_ccg_gsum<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  elementwise(k_ccg_gsum<R>);
   mark();
   const bool p2 = T.p2;
   const int ly = p->fy.n, lx = p->fx.n;
@@ -826,7 +835,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     mark();
     ccg_p2_row_inv<R, MODE_T>(a, ry, s);
     mark();
-    k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+    elementwise(k_ccg_update<R>);
     mark();
     ccg_p2_row_fwd<R, MODE_F>(a, ry, s);
     mark();
@@ -871,7 +880,7 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
   }
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed));
-  for (int i = 0; i < iters; ++i) launch_iteration<R>(p, w, bisect, p->stream);
+  for (int i = 0; i < iters; ++i) launch_iteration<R>(p, w, bisect, p->stream, nullptr, i == 0);
   cudaError_t e = cudaStreamEndCapture(p->stream, &g);
   CK(e);
   e = cudaGraphInstantiate(&w.graph[gi], g, 0);
