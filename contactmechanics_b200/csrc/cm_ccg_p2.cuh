@@ -30,10 +30,15 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long mbar;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+  }
   stage_tw_p2<LOGN>(tws, a.op.twy);
   pdl_wait();
   CcgState* st = a.st;
@@ -44,6 +49,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, ny = N;
+  unsigned mphase = 0;
   const int lw = a.op.lw, W = 1 << lw, nkb = (a.op.nyh + W - 1) >> lw;
   const int ntiles = (tx + ROWS - 1) / ROWS;
   R* __restrict__ fio = a.f[MODE == MODE_T ? cv.par : (cv.par ^ 1)];
@@ -53,65 +59,125 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   const R off = (R)cv.offset;
   const R hdn = neg_down<R>(cv.H);
   const bool need_gap = (MODE == MODE_T) || cv.apply_nc;
+  // The tile's input rows (f, then u and h for the gap, then t) are brought
+  // into the transform buffers by bulk copies when there are at least three
+  // fields and all of them fit (field j of row r at stg[(j * ROWS + r) * ty]);
+  // otherwise they are loaded per element.
+  R* stg = reinterpret_cast<R*>(bufA);
+  const int nfield = 1 + (need_gap ? 2 : 0) + (MODE == MODE_T ? 1 : 0);
+  const int nst = nfield >= 3 && (size_t)nfield * ROWS * ty * sizeof(R) <= 2 * smem_padded(NP * N) * sizeof(C)
+                      ? nfield : 0;
+  const int jt = need_gap ? 3 : 1;  // field index of t
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS, xa = x0 + 2 * s;
     double acc = 0.0;
     R amax = 0;
-    // prologue: every input of the thread's 16 elements first, then the
-    // element-wise step and its stores
-    R fv2[2][8], uv2[2][8], hv2[2][8], tv2[2][8];
+    if (nst > 0) {
+      if (threadIdx.x == 0) {
+        fence_async_shared();
+        fence_async_global();
+        const int nr = min(ROWS, tx - x0);
+        const unsigned rb = (unsigned)(ty * sizeof(R));
+        mbar_expect_tx(&mbar, (unsigned)(nst * nr) * rb);
 #pragma unroll
-    for (int w = 0; w < 2; ++w) {
-      const int x = xa + w;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int y = tt + q * P::TPS;
-        fv2[w][q] = 0; uv2[w][q] = 0; hv2[w][q] = 0; tv2[w][q] = 0;
-        if (x >= tx || y >= ty) continue;
-        const size_t ic = (size_t)x * ty + y;
-        fv2[w][q] = fio[ic];
-        if (need_gap) {
-          uv2[w][q] = u_in[(size_t)x * ny + y];
-          hv2[w][q] = h_in[ic];
+        for (int j = 0; j < 4; ++j) {
+          if (j >= nst) break;
+          const R* src = j == 0 ? fio : j == jt ? t_io : j == 1 ? u_in : h_in;
+          const int ld = (j == 1 && need_gap) ? ny : ty;
+          for (int r = 0; r < nr; ++r)
+            bulk_g2s(stg + (size_t)(j * ROWS + r) * ty, src + (size_t)(x0 + r) * ld, rb, &mbar);
         }
-        if (MODE == MODE_T) tv2[w][q] = t_io[ic];
+      }
+      const bool ok = __syncthreads_and(mbar_wait(&mbar, mphase)) != 0;
+      mphase ^= 1u;
+      if (!ok) {
+        // copies read valid rows and always complete; the wait is bounded all the same
+        if (threadIdx.x == 0) {
+          mbar_wait(&mbar, mphase ^ 1u);
+          st->status = CMS_TIMEOUT;
+          st->done = 1;
+        }
+        return;
       }
     }
-    R out[2][8];
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-      const int x = xa + w;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int y = tt + q * P::TPS;
-        out[w][q] = 0;
-        if (x >= tx || y >= ty) continue;
-        const size_t ic = (size_t)x * ty + y;
-        const R fv = fv2[w][q], uv = uv2[w][q], hv = hv2[w][q];
-        if (MODE == MODE_T) {
-          const bool c = (fv < 0) && (!cv.has_h || fv > hdn);
+    // the element-wise step of element (x, y): search direction t (MODE_T)
+    // or the iteration's final force (MODE_F), stored and returned
+    auto step = [&](int x, int y, R fv, R uv, R hv, R tv) -> R {
+      const size_t ic = (size_t)x * ty + y;
+      if (MODE == MODE_T) {
+        const bool c = (fv < 0) && (!cv.has_h || fv > hdn);
+        const R g = (uv - hv) - off;
+        const R tn = c ? (R)(g + (R)cv.beta * tv) : (R)0;
+        t_io[ic] = tn;
+        if (c) acc += (double)g * (double)tn;
+        return tn;
+      } else {
+        double f = cv.uniform ? cv.funif : cv.scale * (double)fv;
+        const bool flowing = cv.has_h && fv <= hdn;
+        if (flowing) f = -cv.H;
+        if (cv.apply_nc) {
           const R g = (uv - hv) - off;
-          const R tn = c ? (R)(g + (R)cv.beta * tv2[w][q]) : (R)0;
-          t_io[ic] = tn;
-          if (c) acc += (double)g * (double)tn;
-          out[w][q] = tn;
-        } else {
-          double f = cv.uniform ? cv.funif : cv.scale * (double)fv;
-          const bool flowing = cv.has_h && fv <= hdn;
-          if (flowing) f = -cv.H;
-          if (cv.apply_nc) {
-            const R g = (uv - hv) - off;
-            const bool nc = ((fv == (R)0) && g < 0) || (flowing && g > 0);
-            if (nc) f += cv.tau * (double)g;
+          const bool nc = ((fv == (R)0) && g < 0) || (flowing && g > 0);
+          if (nc) f += cv.tau * (double)g;
+        }
+        const R fr = (R)f;
+        fio[ic] = fr;
+        acc += (double)fr;
+        amax = fmax(amax, fabs(fr));
+        return fr;
+      }
+    };
+    R out[2][8];
+    if (nst == nfield) {
+      // every input in shared memory
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = xa + w, r = 2 * s + w;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          out[w][q] = 0;
+          if (x >= tx || y >= ty) continue;
+          const R* row = stg + (size_t)r * ty + y;
+          out[w][q] = step(x, y, row[0], need_gap ? row[(size_t)ROWS * ty] : (R)0,
+                           need_gap ? row[(size_t)2 * ROWS * ty] : (R)0,
+                           MODE == MODE_T ? row[(size_t)jt * ROWS * ty] : (R)0);
+        }
+      }
+    } else {
+      // every input of the thread's 16 elements first, then the
+      // element-wise step and its stores
+      R fv2[2][8], uv2[2][8], hv2[2][8], tv2[2][8];
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = xa + w;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          fv2[w][q] = 0; uv2[w][q] = 0; hv2[w][q] = 0; tv2[w][q] = 0;
+          if (x >= tx || y >= ty) continue;
+          const size_t ic = (size_t)x * ty + y;
+          fv2[w][q] = fio[ic];
+          if (need_gap) {
+            uv2[w][q] = u_in[(size_t)x * ny + y];
+            hv2[w][q] = h_in[ic];
           }
-          const R fr = (R)f;
-          fio[ic] = fr;
-          acc += (double)fr;
-          amax = fmax(amax, fabs(fr));
-          out[w][q] = fr;
+          if (MODE == MODE_T) tv2[w][q] = t_io[ic];
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int x = xa + w;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int y = tt + q * P::TPS;
+          out[w][q] = 0;
+          if (x >= tx || y >= ty) continue;
+          out[w][q] = step(x, y, fv2[w][q], uv2[w][q], hv2[w][q], tv2[w][q]);
         }
       }
     }
+    if (nst > 0) __syncthreads();  // the transform reuses the staging buffers
     C v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);

@@ -6,7 +6,7 @@
 
 #include "cm_slot.cuh"
 
-#define CMS_TIMEOUT 6  // solve status: a grid-barrier wait gave up
+#define CMS_TIMEOUT 6  // solve status: a grid-barrier or bulk-copy wait gave up
 
 // Dynamic shared memory a transform kernel may use (of the 227 KB a block can
 // hold on sm_100, leaving room for its static shared variables).

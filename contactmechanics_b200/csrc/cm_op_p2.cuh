@@ -24,6 +24,12 @@
 #include "cm_kernels.cuh"
 #include "cm_launch.h"
 
+// resident blocks per SM the FP64 row passes are compiled for: two blocks
+// of 256 threads (at most 128 registers a thread) hide more latency than one
+#ifndef CM_FP64_ROW_MINB
+#define CM_FP64_ROW_MINB 2
+#endif
+
 // threads of one block of the operator passes for transform length 2^LOGN
 template <typename R, int LOGN>
 struct OpShape {
@@ -32,7 +38,7 @@ struct OpShape {
   static constexpr int BASE = sizeof(R) == 8 ? 256 : 512;
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
-  static constexpr int MINB = sizeof(R) == 8 ? 1 : 2;
+  static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : 2;
   // block strides of a row-pair gather whose loads are issued together (the
   // gather of a row tile with column tiles W <= N/8 takes at most five); the
   // FP64 passes have the registers to spare, the FP32 ones do not

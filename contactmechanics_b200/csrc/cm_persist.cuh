@@ -23,7 +23,6 @@
 
 #include "cm_launch.h"
 
-#define CM_BARRIER_TIMEOUT_CYCLES 4000000000LL  // about two seconds
 #ifndef CM_BARRIER_SLEEP_NS
 #define CM_BARRIER_SLEEP_NS 32  // back-off between polls of the barrier word
 #endif
@@ -44,56 +43,6 @@ CM_DEVINL unsigned ld_relaxed_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
-}
-
-// ---------------------------------------------------------------------------
-// bulk asynchronous copies global -> shared (TMA engine), completed on an
-// mbarrier.  Sources and destinations 16-byte aligned, sizes multiples of 16.
-// ---------------------------------------------------------------------------
-CM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-CM_DEVINL void mbar_init(unsigned long long* b, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
-}
-
-// make initialised mbarriers visible to the async proxy (before first use)
-CM_DEVINL void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-CM_DEVINL void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
-               : "memory");
-}
-
-// order this thread's view of global memory (written by the generic proxy of
-// any block before the last grid barrier) before its following bulk copies
-CM_DEVINL void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-
-CM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(b))
-      : "memory");
-}
-
-CM_DEVINL bool mbar_try_wait(unsigned long long* b, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(done)
-      : "r"(smem_addr(b)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Wait for the completion of phase `parity` of mbarrier b; false after about
-// two seconds (the copies it tracks read valid device memory and always
-// complete, so this only bounds the wait).
-CM_DEVINL bool mbar_wait(unsigned long long* b, unsigned parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(b, parity))
-    if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) return false;
-  return true;
 }
 
 // All blocks of the grid meet; returns false if the wait gave up.

@@ -1097,6 +1097,7 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     if (done_iters > maxiter + 2 * every) return CM_ERR_CUDA;  // state machine failed to stop
   }
   *fin = *p->h_state;
+  if (fin->status == CMS_TIMEOUT) return CM_ERR_TIMEOUT;
   if (fin->status == CMS_NAN) return CM_ERR_NAN;
   if (fin->status == CMS_BISECT_SIGN) return CM_ERR_BISECT;
   if (fin->status == CMS_BISECT_SIGN + 1) return CM_ERR_BISECT_CONV;
