@@ -463,7 +463,8 @@ def run_operator(reps=50):
                 _lib.check(L.cm_apply(sub._plan.ptr, _lib.CM_OP_DISP, _lib.PRECISIONS[prec],
                                       ctypes.c_void_p(x.data_ptr()), n if kind == "free" else nxd,
                                       n if kind == "free" else nyd, nyd, ctypes.c_void_p(y.data_ptr()),
-                                      nxd, nyd, nyd, ctypes.c_void_p(stream.cuda_stream)))
+                                      nxd, nyd, nyd,
+                                      ctypes.c_void_p(stream.cuda_stream or _lib.CUDA_STREAM_LEGACY)))
             for _ in range(5):
                 call()
             e0 = torch.cuda.Event(enable_timing=True)

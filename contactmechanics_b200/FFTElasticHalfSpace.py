@@ -232,7 +232,9 @@ class PeriodicFFTElasticHalfSpace(ElasticSubstrate):
             src = src.reshape(-1, 1)
         out = torch.empty((out_rows, out_cols), dtype=tdt, device="cuda")
         L = self._plan._L
-        stream = torch.cuda.current_stream().cuda_stream
+        # torch's default stream has the handle 0, which the library reads as
+        # "the plan's stream"; name the legacy default stream explicitly
+        stream = torch.cuda.current_stream().cuda_stream or _lib.CUDA_STREAM_LEGACY
         _lib.check(L.cm_apply(self._plan.ptr, op, _lib.PRECISIONS[prec],
                               ctypes.c_void_p(src.data_ptr()), in_rows, in_cols, src.shape[1],
                               ctypes.c_void_p(out.data_ptr()), out_rows, out_cols, out_cols,

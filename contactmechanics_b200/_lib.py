@@ -34,6 +34,7 @@ CM_OP_DISP = 0
 CM_OP_FORCE = 1
 CM_SOLVE_CONVERGED = 1
 CM_SOLVE_MAXITER = 2
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream
 
 PRECISIONS = {"fp64": CM_FP64, "fp32": CM_FP32, "mixed": CM_MIXED}
 

@@ -640,7 +640,7 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
 // Fields of one comp tile (rows [cx0, cx0+crows) of the topography) in registers.
 template <typename R>
 struct CompTile {
-  int cx0, cn, ty, ny;
+  int cx0, cn, ty, ny, lty;  // lty: log2 of ty when ty is a power of two, else -1
   const R* __restrict__ u;
   const R* __restrict__ h;
   CM_DEVINL CompTile(const Slot<R>* Sp, int tile) {
@@ -650,10 +650,11 @@ struct CompTile {
     cn = min(Sp->comp_rows, Sp->tx - cx0) * ty;
     u = Sp->u;
     h = Sp->h;
+    lty = (ty & (ty - 1)) == 0 ? __ffs(ty) - 1 : -1;
   }
   // topography index and displacement index of element e of the tile
   CM_DEVINL void at(int e, size_t& ic, size_t& iu) const {
-    const int r = e / ty, y = e - r * ty;
+    const int r = lty >= 0 ? e >> lty : e / ty, y = e - r * ty;
     ic = (size_t)cx0 * ty + e;
     iu = (size_t)(cx0 + r) * ny + y;
   }
@@ -667,13 +668,17 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  // the slot (geometry, field pointers) is constant during a solve: read it
+  // before waiting for the previous kernel
+  const CompTile<R> T(Sp, item.y);
+  R* const f0 = Sp->f[0];
+  R* const f1 = Sp->f[1];
   pdl_trigger();
   pdl_wait();
   if (st->done) return;
   const int has_h = st->p.has_h;
   const R hdn = neg_down<R>(st->p.H);
-  const R* __restrict__ f = Sp->f[st->parity];
-  const CompTile<R> T(Sp, item.y);
+  const R* __restrict__ f = (st->parity & 1) ? f1 : f0;
   // counts in int and extrema in R are exact; only the sum is accumulated in FP64
   int a_c = 0, a_cg = 0;
   double s_cg = 0;
@@ -706,14 +711,16 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  const CompTile<R> T(Sp, item.y);
+  R* const f0 = Sp->f[0];
+  R* const f1 = Sp->f[1];
   pdl_trigger();
   pdl_wait();
   if (st->done || st->branch != 0) return;
   const int has_h = st->p.has_h;
   const R hdn = neg_down<R>(st->p.H);
   const R off = (R)st->offset;
-  const R* __restrict__ f = Sp->f[st->parity];
-  const CompTile<R> T(Sp, item.y);
+  const R* __restrict__ f = (st->parity & 1) ? f1 : f0;
   double G = 0;
   struct V3 { R f, u, h; };
   batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
@@ -741,6 +748,7 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  const CompTile<R> T(Sp, item.y);
   pdl_trigger();
   pdl_wait();
   if (st->done || st->branch != 1 || !st->bs_active) return;
@@ -765,7 +773,6 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   // compared one by one
   const double lo = cand_lo, hi = cand_hi;
   int below_all = 0;
-  const CompTile<R> T(Sp, item.y);
   int icnt[CM_BIS_CAND];  // counts: exact in int
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) icnt[i] = 0;
@@ -802,19 +809,21 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
+  const CompTile<R> T(Sp, item.y);
+  R* const f0 = Sp->f[0];
+  R* const f1 = Sp->f[1];
+  const R* __restrict__ t = Sp->t;
+  unsigned char* __restrict__ gneg = Sp->gneg;
   pdl_trigger();
   pdl_wait();
   if (st->done) return;
-  const int par = st->parity, has_h = st->p.has_h, branch = st->branch;
+  const int par = st->parity & 1, has_h = st->p.has_h, branch = st->branch;
   const double H = st->p.H;
   const R off = (R)st->offset;
   const R tau = (R)st->tau;
   const double mix = st->cur_mixfac;
-  const R* __restrict__ f = Sp->f[par];
-  R* __restrict__ fo = Sp->f[par ^ 1];
-  const R* __restrict__ t = Sp->t;
-  unsigned char* __restrict__ gneg = Sp->gneg;
-  const CompTile<R> T(Sp, item.y);
+  const R* __restrict__ f = par ? f1 : f0;
+  R* __restrict__ fo = par ? f0 : f1;
   const R hdn = neg_down<R>(H);
   // counts in int and extrema in R are exact (x -> (double)x + H is monotonic,
   // so the minimum of fn + H is the minimum fn plus H); only the sum is FP64

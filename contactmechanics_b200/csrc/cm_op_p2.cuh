@@ -30,6 +30,12 @@
 #define CM_FP64_ROW_MINB 2
 #endif
 
+// threads of an FP64 column-pass block (at least one transform): 128, so
+// that two blocks fit an SM's shared memory at length 2048
+#ifndef CM_COL16_FP64_BASE
+#define CM_COL16_FP64_BASE 128
+#endif
+
 // threads of one block of the operator passes for transform length 2^LOGN
 template <typename R, int LOGN>
 struct OpShape {
@@ -158,9 +164,10 @@ template <typename R, int LOGN>
 struct OpShape16 {
   static constexpr int N = 1 << LOGN;
   static constexpr int TPS = N / 16;
-  static constexpr int THREADS = TPS > 256 ? TPS : 256;
+  static constexpr int BASE = sizeof(R) == 8 ? CM_COL16_FP64_BASE : 256;
+  static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // columns per block
-  static constexpr int MINB = sizeof(R) == 4 ? 2 : 1;
+  static constexpr int MINB = sizeof(R) == 4 || BASE < 256 ? 2 : 1;
   static size_t smem() {
     return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
   }

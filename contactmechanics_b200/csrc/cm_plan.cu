@@ -622,8 +622,8 @@ static int init_work(cm_plan* p, Work<R>& w) {
   std::vector<C> twx = make_twiddles<C>(p->nx), twy = make_twiddles<C>(p->ny);
   CKS(dalloc(p, &w.twx, p->nx));
   CKS(dalloc(p, &w.twy, p->ny));
-  CK(cudaMemcpy(w.twx, twx.data(), sizeof(C) * p->nx, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(w.twy, twy.data(), sizeof(C) * p->ny, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(w.twx, twx.data(), sizeof(C) * p->nx, cudaMemcpyHostToDevice, p->stream));
+  CK(cudaMemcpyAsync(w.twy, twy.data(), sizeof(C) * p->ny, cudaMemcpyHostToDevice, p->stream));
   CKS(dalloc(p, &w.spec, (size_t)p->nx * w.tiles.ntile_cols * w.tiles.col_tile));
   CKS(dalloc(p, &w.d_plain, 1));
   CKS(dalloc(p, &w.d_ccg, 1));
@@ -634,7 +634,7 @@ static int init_work(cm_plan* p, Work<R>& w) {
   // (the by-value row passes use tiles of at least two rows: at most nx tiles)
   CKS(dalloc(p, &w.partials, (size_t)std::max(nt_max, p->nx) * CM_MAX_PARTIAL_VALS));
   CKS(dalloc(p, &w.counter, 1));
-  CK(cudaMemset(w.counter, 0, sizeof(unsigned int)));
+  CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), p->stream));
   CKS(dalloc(p, &w.st, 1));
   if (nt_max > p->max_items) p->max_items = nt_max;
   return CM_OK;
@@ -1495,7 +1495,10 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
     p->stream = (cudaStream_t)stream;
     p->own_stream = false;
   } else {
-    if (cudaStreamCreate(&p->stream) != cudaSuccess) return fail(CM_ERR_CUDA);
+    // non-blocking: no implicit ordering with the legacy default stream, so
+    // another thread's stream capture is never joined by this plan's work
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(CM_ERR_CUDA);
     p->own_stream = true;
   }
   if (cudaMallocHost(&p->h_state, sizeof(CcgState)) != cudaSuccess) {
@@ -1509,7 +1512,8 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
     std::vector<int2> it(p->max_items);
     for (int i = 0; i < p->max_items; ++i) it[i] = make_int2(0, i);
     if ((rc = dalloc(p, &p->items, it.size())) != CM_OK) return fail(rc);
-    if (cudaMemcpy(p->items, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(p->items, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                        p->stream) != cudaSuccess)
       return fail(CM_ERR_CUDA);
   }
   const long nh = (long)p->nx * p->nyh;
@@ -1519,8 +1523,8 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
   for (int i = 0; i < 2; ++i) {
     if ((rc = dalloc(p, &p->tab64[i], nh64)) != CM_OK) return fail(rc);
     if ((rc = dalloc(p, &p->tab32[i], nh32)) != CM_OK) return fail(rc);
-    cudaMemset(p->tab64[i], 0, nh64 * sizeof(double));
-    cudaMemset(p->tab32[i], 0, nh32 * sizeof(float));
+    cudaMemsetAsync(p->tab64[i], 0, nh64 * sizeof(double), p->stream);
+    cudaMemsetAsync(p->tab32[i], 0, nh32 * sizeof(float), p->stream);
   }
   p->w64.tab[0] = p->tab64[0];
   p->w64.tab[1] = p->tab64[1];
@@ -1771,7 +1775,10 @@ int cm_stepper_create(void* stream, cm_stepper** out) {
   if (stream) {
     st->stream = (cudaStream_t)stream;
   } else {
-    if (cudaStreamCreate(&st->stream) != cudaSuccess) { delete st; return CM_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete st;
+      return CM_ERR_CUDA;
+    }
     st->own_stream = true;
   }
   *out = st;
