@@ -17,8 +17,8 @@
 //                          after the first launches no k_ccg_begin.
 //
 // The column pass between them is k_op_col16 with the solve's state attached.
-// Each tile writes its reduction partials and the last tile to finish runs
-// the scalar step (tile_finish), as in the per-pass kernels.
+// Each block accumulates its tiles' reductions and writes one partial; the
+// last block to finish runs the scalar step (tile_finish).
 #pragma once
 #include "cm_op_p2.cuh"
 
@@ -68,10 +68,11 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   const int nst = nfield >= 3 && (size_t)nfield * ROWS * ty * sizeof(R) <= 2 * smem_padded(NP * N) * sizeof(C)
                       ? nfield : 0;
   const int jt = need_gap ? 3 : 1;  // field index of t
+  // reductions accumulate over the block's tiles; one partial per block
+  double acc = 0.0;
+  R amax = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS, xa = x0 + 2 * s;
-    double acc = 0.0;
-    R amax = 0;
     if (nst > 0) {
       if (threadIdx.x == 0) {
         fence_async_shared();
@@ -201,18 +202,18 @@ k_ccg_row_fwd(CcgArgs<R> a) {
                             : cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
       a.op.spec[((size_t)kb * a.op.nx + x) * W + kw] = val;
     }
-    if (MODE == MODE_T) {
-      double vr[1] = {acc};
-      const int kinds[1] = {RED_SUM};
-      tile_finish<1>(a.partials, a.counter, tile, ntiles, vr, kinds,
-                     [&](double (&r)[1]) { st->sum_cgt = r[0]; });
-    } else {
-      double vr[2] = {acc, (double)amax};
-      const int kinds[2] = {RED_SUM, RED_MAX};
-      tile_finish<2>(a.partials, a.counter, tile, ntiles, vr, kinds,
-                     [&](double (&r)[2]) { fin_force(*st, r); });
-    }
     __syncthreads();  // bufA free for the next tile
+  }
+  if (MODE == MODE_T) {
+    double vr[1] = {acc};
+    const int kinds[1] = {RED_SUM};
+    tile_finish<1>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds,
+                   [&](double (&r)[1]) { st->sum_cgt = r[0]; });
+  } else {
+    double vr[2] = {acc, (double)amax};
+    const int kinds[2] = {RED_SUM, RED_MAX};
+    tile_finish<2>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds,
+                   [&](double (&r)[2]) { fin_force(*st, r); });
   }
 }
 
@@ -247,6 +248,13 @@ k_ccg_row_inv(CcgArgs<R> a) {
   const R* __restrict__ h_in = a.h;
   const R* __restrict__ t_in = a.t;
   const unsigned char* __restrict__ gneg = a.gneg;
+  // reductions accumulate over the block's tiles; one partial per block
+  double a0 = 0.0;                                // MODE_T: sum r t
+  R du = 0, pmax = -INFINITY;                     // MODE_F: extrema, exact in R
+  R gmax = -INFINITY, gmin = INFINITY;
+  int n_c = 0, n_cg = 0;                          // counts, exact in int
+  double s_cg = 0;
+  const R* __restrict__ fn_buf = a.f[cv.par ^ 1];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS;
     gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.op.spec, nx, a.op.nyh, a.op.lw, x0,
@@ -258,7 +266,6 @@ k_ccg_row_inv(CcgArgs<R> a) {
     fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
     const int xa = x0 + 2 * s;
     if (MODE == MODE_T) {
-      double a0 = 0.0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int y = tt + q * P::TPS;
@@ -266,21 +273,12 @@ k_ccg_row_inv(CcgArgs<R> a) {
         if (xa < tx) a0 += (double)v[q].x * (double)t_in[(size_t)xa * ty + y];
         if (xa + 1 < tx) a0 += (double)v[q].y * (double)t_in[(size_t)(xa + 1) * ty + y];
       }
-      double vr[1] = {a0};
-      const int kinds[1] = {RED_SUM};
-      tile_finish<1>(a.partials, a.counter, tile, ntiles, vr, kinds,
-                     [&](double (&r)[1]) { fin_tau(*st, r); });
     } else {
       // u on the whole domain, max |du| and the maximum penetration; on the
       // topography also the start-of-iteration statistics of the next
       // iteration (k_ccg_begin: contact areas, sum of the gaps over the CG
       // area, extreme gaps; ConstrainedConjugateGradients.py:239-270) from
       // the new displacement and the iteration's final force f[par ^ 1]
-      R du = 0, pmax = -INFINITY;  // extrema, exact in R
-      R gmax = -INFINITY, gmin = INFINITY;
-      int n_c = 0, n_cg = 0;  // counts, exact in int
-      double s_cg = 0;
-      const R* __restrict__ fn_buf = a.f[cv.par ^ 1];
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w;
@@ -325,17 +323,24 @@ k_ccg_row_inv(CcgArgs<R> a) {
           }
         }
       }
-      double vr[7] = {(double)du, (double)pmax, (double)n_c, (double)n_cg, s_cg, (double)gmax,
-                      (double)gmin};
-      const int kinds[7] = {RED_MAX, RED_MAX, RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-      tile_finish<7>(a.partials, a.counter, tile, ntiles, vr, kinds, [&](double (&r)[7]) {
-        ccg_converge(*st, r[0], r[1]);
-        if (!st->done) {
-          double b[5] = {r[2], r[3], r[4], r[5], r[6]};
-          fin_begin(*st, b);
-        }
-      });
     }
     __syncthreads();  // buffers free for the next tile
+  }
+  if (MODE == MODE_T) {
+    double vr[1] = {a0};
+    const int kinds[1] = {RED_SUM};
+    tile_finish<1>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds,
+                   [&](double (&r)[1]) { fin_tau(*st, r); });
+  } else {
+    double vr[7] = {(double)du, (double)pmax, (double)n_c, (double)n_cg, s_cg, (double)gmax,
+                    (double)gmin};
+    const int kinds[7] = {RED_MAX, RED_MAX, RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
+    tile_finish<7>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds, [&](double (&r)[7]) {
+      ccg_converge(*st, r[0], r[1]);
+      if (!st->done) {
+        double b[5] = {r[2], r[3], r[4], r[5], r[6]};
+        fin_begin(*st, b);
+      }
+    });
   }
 }
