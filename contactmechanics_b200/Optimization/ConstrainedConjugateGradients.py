@@ -21,6 +21,7 @@ Extra keyword ``precision``: "fp64" (default; reference arithmetic),
 iterations warm-started from the FP32 forces) or "fp32".
 """
 import ctypes
+import threading
 
 import numpy as np
 import scipy.optimize as optim
@@ -34,15 +35,59 @@ def _torch():
     return torch
 
 
-def _device_f64(a, shape=None):
+class _Staging(threading.local):
+    """Pinned host buffers of this thread, one per role (grown on demand), each
+    with the event of the last copy through it."""
+
+    def __init__(self):
+        self.bufs = {}
+
+
+_STAGING = _Staging()
+
+
+def _pinned(role, n, dtype):
+    torch = _torch()
+    ent = _STAGING.bufs.get((role, dtype))
+    if ent is None or ent[0].numel() < n:
+        ent = [torch.empty(max(n, 1), dtype=dtype, pin_memory=True), None]
+        _STAGING.bufs[(role, dtype)] = ent
+    if ent[1] is not None:
+        ent[1].synchronize()  # the previous copy through this buffer has finished
+        ent[1] = None
+    return ent
+
+
+def _device_f64(a, shape=None, role="in"):
+    """A float64 device copy of `a`; host arrays travel through a pinned buffer."""
     torch = _torch()
     if isinstance(a, torch.Tensor):
         t = a.to(device="cuda", dtype=torch.float64).contiguous()
     else:
-        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64))).to("cuda")
+        arr = np.asarray(a, dtype=np.float64)
+        ent = _pinned(role, arr.size, torch.float64)
+        host = ent[0][:arr.size]
+        np.copyto(host.numpy().reshape(arr.shape), arr)
+        t = host.to("cuda", non_blocking=True).reshape(arr.shape)
+        ev = torch.cuda.Event()
+        ev.record()
+        ent[1] = ev
     if shape is not None:
         t = t.reshape(shape)
     return t
+
+
+def _host_arrays(named):
+    """Fresh numpy copies of device tensors [(role, tensor), ...], through pinned buffers."""
+    torch = _torch()
+    staged = []
+    for role, t in named:
+        ent = _pinned(role, t.numel(), t.dtype)
+        host = ent[0][:t.numel()].view(t.shape)
+        host.copy_(t, non_blocking=True)
+        staged.append(host)
+    torch.cuda.current_stream().synchronize()
+    return [h.numpy().copy() for h in staged]
 
 
 def constrained_conjugate_gradients(substrate, topography, hardness=None, external_force=None,
@@ -94,9 +139,10 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
     if precision not in _lib.PRECISIONS:
         raise ValueError("precision must be one of {}".format(sorted(_lib.PRECISIONS)))
 
-    h_dev = _device_f64(heights, tshape)
-    u0 = _device_f64(initial_displacements, dshape) if initial_displacements is not None else None
-    f0 = _device_f64(initial_forces, dshape) if initial_forces is not None else None
+    h_dev = _device_f64(heights, tshape, role="h")
+    u0 = (_device_f64(initial_displacements, dshape, role="u0")
+          if initial_displacements is not None else None)
+    f0 = _device_f64(initial_forces, dshape, role="f0") if initial_forces is not None else None
     x = torch.empty(dshape, dtype=torch.float64, device="cuda")
     jac = torch.empty(tshape, dtype=torch.float64, device="cuda")
     active = torch.empty(tshape, dtype=torch.uint8, device="cuda")
@@ -160,11 +206,13 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
         if plastic is not None and result.success:
             result.plastic = plastic.bool()
     else:
-        result.x = x.cpu().numpy()
-        result.jac = jac.cpu().numpy()
-        result.active_set = act_dom.cpu().numpy()
+        named = [("x", x), ("jac", jac), ("active", act_dom)]
         if plastic is not None and result.success:
-            result.plastic = plastic.bool().cpu().numpy()
+            named.append(("plastic", plastic.bool()))
+        arrays = _host_arrays(named)
+        result.x, result.jac, result.active_set = arrays[:3]
+        if len(arrays) > 3:
+            result.plastic = arrays[3]
 
     log_headers = ["status", "it", "area", "cg area", "total force", "offset"]
     log_values = ["CONVERGED" if result.success else "NOT CONVERGED", res.nit, res.area,

@@ -347,9 +347,10 @@ class ContactServer:
         kw = dict(req.solver_kwargs)
         sub = self._substrate(req)
         req._substrate = sub
-        req._h_dev = _device_f64(req.heights, sub.nb_grid_pts)
+        req._h_dev = _device_f64(req.heights, sub.nb_grid_pts, role="h")
         u0 = kw.pop("initial_displacements", None)
-        req._u0_dev = _device_f64(u0, sub.nb_domain_grid_pts) if u0 is not None else None
+        req._u0_dev = (_device_f64(u0, sub.nb_domain_grid_pts, role="u0")
+                       if u0 is not None else None)
         P = _params(self.precision, kw.get("external_force"), kw.get("offset"), kw.get("hardness"),
                     kw.get("pentol"), kw.get("forcetol", 1e-5), kw.get("thermotol", 1e-6),
                     kw.get("mixfac", 0.1), kw.get("mixdecfac", 0.95), kw.get("minmixsteps", 10),
