@@ -166,7 +166,9 @@ def kernel_bytes(nx, ny, tx, ty, prec_bytes=4):
         "k_ccg_update": 5 * p * N,
         "k_row_fwd<F>": 2 * p * N + c * nh_t,
         "k_col<F>": c * nh_t + p * nh + c * nh,
-        "k_row_inv<F>": c * nh + 2 * p * Nd + 2 * p * N,
+        # u = G f on the domain, with the next iteration's start statistics
+        # (heights, start and final forces of the topography)
+        "k_row_inv<F>": c * nh + 2 * p * Nd + 3 * p * N,
     }
 
 
