@@ -804,7 +804,7 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
 // Force update, projection onto [0, H], constraint bookkeeping
 // (ConstrainedConjugateGradients.py:296, 320-389).
 template <typename R>
-__global__ void __launch_bounds__(CM_THREADS)
+__global__ void __launch_bounds__(CM_THREADS, sizeof(R) == 4 ? 4 : 3)
 k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
