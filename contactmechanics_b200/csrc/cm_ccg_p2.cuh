@@ -26,7 +26,7 @@ template <typename R, int MODE, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_ccg_row_fwd(CcgArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2Plan<LOGN> P;
+  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -39,7 +39,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
     mbar_init(&mbar, 1);
     mbar_init_fence();
   }
-  stage_tw_p2<LOGN>(tws, a.op.twy);
+  stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
@@ -128,14 +128,14 @@ k_ccg_row_fwd(CcgArgs<R> a) {
         return fr;
       }
     };
-    R out[2][8];
+    R out[2][Sh::E];
     if (nst == nfield) {
       // every input in shared memory
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w, r = 2 * s + w;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < Sh::E; ++q) {
           const int y = tt + q * P::TPS;
           out[w][q] = 0;
           if (x >= tx || y >= ty) continue;
@@ -146,14 +146,14 @@ k_ccg_row_fwd(CcgArgs<R> a) {
         }
       }
     } else {
-      // every input of the thread's 16 elements first, then the
+      // every input of the thread's 2E elements first, then the
       // element-wise step and its stores
-      R fv2[2][8], uv2[2][8], hv2[2][8], tv2[2][8];
+      R fv2[2][Sh::E], uv2[2][Sh::E], hv2[2][Sh::E], tv2[2][Sh::E];
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < Sh::E; ++q) {
           const int y = tt + q * P::TPS;
           fv2[w][q] = 0; uv2[w][q] = 0; hv2[w][q] = 0; tv2[w][q] = 0;
           if (x >= tx || y >= ty) continue;
@@ -170,7 +170,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < Sh::E; ++q) {
           const int y = tt + q * P::TPS;
           out[w][q] = 0;
           if (x >= tx || y >= ty) continue;
@@ -179,13 +179,13 @@ k_ccg_row_fwd(CcgArgs<R> a) {
       }
     }
     if (nst > 0) __syncthreads();  // the transform reuses the staging buffers
-    C v[8];
+    C v[Sh::E];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
-    fft_p2<C, false, LOGN>(v, bufA, bufB, s * N, 1, tt, tws);
+    for (int q = 0; q < Sh::E; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
+    fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 8; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
+    for (int q = 0; q < Sh::E; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
     __syncthreads();
     // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
     const int total = nkb * ROWS * W;
@@ -221,7 +221,7 @@ template <typename R, int MODE, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_ccg_row_inv(CcgArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2Plan<LOGN> P;
+  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -229,7 +229,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2<LOGN>(tws, a.op.twy);
+  stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
@@ -260,14 +260,14 @@ k_ccg_row_inv(CcgArgs<R> a) {
     gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.op.spec, nx, a.op.nyh, a.op.lw, x0,
                                                       rows_total);
     __syncthreads();
-    C v[8];
+    C v[Sh::E];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
-    fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
+    for (int q = 0; q < Sh::E; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
+    fft_p2r<C, true, LOGN, Sh::LR>(v, bufB, bufA, s * N, 1, tt, tws);
     const int xa = x0 + 2 * s;
     if (MODE == MODE_T) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < Sh::E; ++q) {
         const int y = tt + q * P::TPS;
         if (y >= ty) continue;
         if (xa < tx) a0 += (double)v[q].x * (double)t_in[(size_t)xa * ty + y];
@@ -283,11 +283,11 @@ k_ccg_row_inv(CcgArgs<R> a) {
       for (int w = 0; w < 2; ++w) {
         const int x = xa + w;
         if (x >= rows_total) continue;
-        // every input of the row's 8 elements first, then the stores
-        R uo[8], hv[8], fn[8];
-        bool cc[8];
+        // every input of the row's E elements first, then the stores
+        R uo[Sh::E], hv[Sh::E], fn[Sh::E];
+        bool cc[Sh::E];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < Sh::E; ++q) {
           const int y = tt + q * P::TPS;
           hv[q] = 0; fn[q] = 0; cc[q] = false;
           uo[q] = u_io[(size_t)x * N + y];
@@ -304,7 +304,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
           }
         }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < Sh::E; ++q) {
           const int y = tt + q * P::TPS;
           const R val = w ? v[q].y : v[q].x;
           du = fmax(du, fabs(val - uo[q]));

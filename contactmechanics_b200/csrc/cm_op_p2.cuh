@@ -36,12 +36,23 @@
 #define CM_COL16_FP64_BASE 128
 #endif
 
-// threads of one block of the operator passes for transform length 2^LOGN
+// log2 of the elements per thread of the row passes' transforms (3: the
+// radix-8 engine, 4: the radix-16 one)
+#ifndef CM_ROW_LR_F32
+#define CM_ROW_LR_F32 3
+#endif
+#ifndef CM_ROW_LR_F64
+#define CM_ROW_LR_F64 3
+#endif
+
+// threads of one block of the row passes for transform length 2^LOGN
 template <typename R, int LOGN>
 struct OpShape {
   static constexpr int N = 1 << LOGN;
-  static constexpr int TPS = N / 8;
-  static constexpr int BASE = sizeof(R) == 8 ? 256 : 512;
+  static constexpr int LR = sizeof(R) == 8 ? CM_ROW_LR_F64 : CM_ROW_LR_F32;
+  static constexpr int E = 1 << LR;  // elements per thread
+  static constexpr int TPS = N >> LR;
+  static constexpr int BASE = (sizeof(R) == 8 ? 256 : 512) >> (LR - 3);
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
   static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : 2;
@@ -106,7 +117,7 @@ template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_op_row_fwd(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2Plan<LOGN> P;
+  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -114,7 +125,7 @@ k_op_row_fwd(OpArgs<R> a) {
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2<LOGN>(tws, a.twy);
+  stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
@@ -122,9 +133,9 @@ k_op_row_fwd(OpArgs<R> a) {
   const int ntiles = (a.in_rows + ROWS - 1) / ROWS;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS, xa = x0 + 2 * s;
-    C v[8];
+    C v[Sh::E];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;
       R ra = 0, rb = 0;
       if (y < a.in_cols) {
@@ -133,10 +144,10 @@ k_op_row_fwd(OpArgs<R> a) {
       }
       v[q] = cmake<C>(ra, rb);
     }
-    fft_p2<C, false, LOGN>(v, bufA, bufB, s * N, 1, tt, tws);
+    fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 8; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
+    for (int q = 0; q < Sh::E; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
     __syncthreads();
     // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
     const int total = nkb * ROWS * W;
@@ -231,7 +242,7 @@ template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_op_row_inv(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2Plan<LOGN> P;
+  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -239,7 +250,7 @@ k_op_row_inv(OpArgs<R> a) {
   C* bufA = tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2<LOGN>(tws, a.twy);
+  stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
@@ -248,13 +259,13 @@ k_op_row_inv(OpArgs<R> a) {
     const int x0 = tile * ROWS;
     gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.spec, a.nx, a.nyh, a.lw, x0, a.out_rows);
     __syncthreads();
-    C v[8];
+    C v[Sh::E];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
-    fft_p2<C, true, LOGN>(v, bufB, bufA, s * N, 1, tt, tws);
+    for (int q = 0; q < Sh::E; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
+    fft_p2r<C, true, LOGN, Sh::LR>(v, bufB, bufA, s * N, 1, tt, tws);
     const int xa = x0 + 2 * s;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;
       if (y >= a.out_cols) continue;
       if (xa < a.out_rows) a.out[(size_t)xa * a.out_ld + y] = v[q].x;
