@@ -973,6 +973,7 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
   st.nfev = 1;
   st.scale = 1.0;
   CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), s));  // a solve that gave up may leave it set
   g_launches += 3;  // heights statistics (2) and the initial field
   k_h_prep<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64);
   k_h_var<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64, prm->pentol <= 0, rel_pentol);
