@@ -660,17 +660,36 @@ struct CompTile {
   }
 };
 
+// The element-wise passes run in one of two shapes.  With strided == 0 a
+// block takes work item items[blockIdx.x] (a (solve, tile) pair: batched
+// solves share a launch) and writes one partial per tile.  With strided = n
+// > 0 every item is a tile of the one solve of items[0], the block walks
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ... < n and writes one partial
+// for all of them (fewer blocks and partials for a single solve).
+struct EwTiles {
+  int first, end, step, part, nparts;
+  CM_DEVINL EwTiles(int2 item, int strided, int nt_comp) {
+    if (strided > 0) {
+      first = blockIdx.x; end = strided; step = gridDim.x;
+      part = blockIdx.x; nparts = gridDim.x;
+    } else {
+      first = item.y; end = item.y + 1; step = 1;
+      part = item.y; nparts = nt_comp;
+    }
+  }
+};
+
 // Start of an iteration: contact areas, raw-gap sums, step kind and offset
 // (ConstrainedConjugateGradients.py:239-270, 300-318).
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
-k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
-  const int2 item = items[blockIdx.x];
+k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, int strided) {
+  const int2 item = items[strided > 0 ? 0 : blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
   // the slot (geometry, field pointers) is constant during a solve: read it
   // before waiting for the previous kernel
-  const CompTile<R> T(Sp, item.y);
+  const EwTiles W(item, strided, Sp->nt_comp);
   R* const f0 = Sp->f[0];
   R* const f1 = Sp->f[1];
   pdl_trigger();
@@ -684,34 +703,37 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   double s_cg = 0;
   R gmax = -INFINITY, gmin = INFINITY;
   struct V3 { R f, u, h; };
-  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-    size_t ic, iu;
-    T.at(e, ic, iu);
-    return V3{f[ic], T.u[iu], T.h[ic]};
-  }, [&](int, V3 v) {
-    const bool c0 = v.f < 0;
-    const bool c = c0 && (!has_h || v.f > hdn);
-    const R g = v.u - v.h;
-    a_c += c0;
-    a_cg += c;
-    if (c) s_cg += (double)g;
-    gmax = fmax(gmax, g);
-    gmin = fmin(gmin, g);
-  });
+  for (int tile = W.first; tile < W.end; tile += W.step) {
+    const CompTile<R> T(Sp, tile);
+    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+      size_t ic, iu;
+      T.at(e, ic, iu);
+      return V3{f[ic], T.u[iu], T.h[ic]};
+    }, [&](int, V3 v) {
+      const bool c0 = v.f < 0;
+      const bool c = c0 && (!has_h || v.f > hdn);
+      const R g = v.u - v.h;
+      a_c += c0;
+      a_cg += c;
+      if (c) s_cg += (double)g;
+      gmax = fmax(gmax, g);
+      gmin = fmin(gmin, g);
+    });
+  }
   double v[5] = {(double)a_c, (double)a_cg, s_cg, (double)gmax, (double)gmin};
   const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+  tile_finish<5>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
                  [&](double (&a)[5]) { fin_begin(*st, a); });
 }
 
 // G = sum over the CG area of g^2 and the conjugation factor (:273-279).
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
-k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
-  const int2 item = items[blockIdx.x];
+k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, int strided) {
+  const int2 item = items[strided > 0 ? 0 : blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
-  const CompTile<R> T(Sp, item.y);
+  const EwTiles W(item, strided, Sp->nt_comp);
   R* const f0 = Sp->f[0];
   R* const f1 = Sp->f[1];
   pdl_trigger();
@@ -723,18 +745,21 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   const R* __restrict__ f = (st->parity & 1) ? f1 : f0;
   double G = 0;
   struct V3 { R f, u, h; };
-  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-    size_t ic, iu;
-    T.at(e, ic, iu);
-    return V3{f[ic], T.u[iu], T.h[ic]};
-  }, [&](int, V3 v) {
-    const bool c = (v.f < 0) && (!has_h || v.f > hdn);
-    const R g = (v.u - v.h) - off;
-    if (c) G += (double)g * (double)g;
-  });
+  for (int tile = W.first; tile < W.end; tile += W.step) {
+    const CompTile<R> T(Sp, tile);
+    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+      size_t ic, iu;
+      T.at(e, ic, iu);
+      return V3{f[ic], T.u[iu], T.h[ic]};
+    }, [&](int, V3 v) {
+      const bool c = (v.f < 0) && (!has_h || v.f > hdn);
+      const R g = (v.u - v.h) - off;
+      if (c) G += (double)g * (double)g;
+    });
+  }
   double v[1] = {G};
   const int kinds[1] = {RED_SUM};
-  tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+  tile_finish<1>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
                  [&](double (&a)[1]) { fin_gsum(*st, a); });
 }
 
@@ -744,11 +769,11 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
 // then replays scipy's bisection on those counts bit for bit.
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
-k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
-  const int2 item = items[blockIdx.x];
+k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, int strided) {
+  const int2 item = items[strided > 0 ? 0 : blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
-  const CompTile<R> T(Sp, item.y);
+  const EwTiles W(item, strided, Sp->nt_comp);
   pdl_trigger();
   pdl_wait();
   if (st->done || st->branch != 1 || !st->bs_active) return;
@@ -777,27 +802,30 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) icnt[i] = 0;
   struct V2 { R u, h; };
-  batched_loop<4>(T.cn, [&](int e) {
-    size_t ic, iu;
-    T.at(e, ic, iu);
-    return V2{T.u[iu], T.h[ic]};
-  }, [&](int, V2 v) {
-    const double g = (double)(v.u - v.h);
-    if (g < lo) {
-      ++below_all;
-    } else if (g < hi) {
+  for (int tile = W.first; tile < W.end; tile += W.step) {
+    const CompTile<R> T(Sp, tile);
+    batched_loop<4>(T.cn, [&](int e) {
+      size_t ic, iu;
+      T.at(e, ic, iu);
+      return V2{T.u[iu], T.h[ic]};
+    }, [&](int, V2 v) {
+      const double g = (double)(v.u - v.h);
+      if (g < lo) {
+        ++below_all;
+      } else if (g < hi) {
 #pragma unroll
-      for (int i = 0; i < CM_BIS_CAND; ++i)
-        if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
-    }
-  });
+        for (int i = 0; i < CM_BIS_CAND; ++i)
+          if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
+      }
+    });
+  }
   double cnt[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = (double)(icnt[i] + (i < ncand ? below_all : 0));
   int kinds[CM_BIS_CAND];
 #pragma unroll
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
-  tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, cnt, kinds,
+  tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, W.part, W.nparts, cnt, kinds,
                            [&](double (&a)[CM_BIS_CAND]) { fin_bisect(*st, a); });
 }
 
@@ -805,11 +833,11 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
 // (ConstrainedConjugateGradients.py:296, 320-389).
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS, sizeof(R) == 4 ? 4 : 3)
-k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
-  const int2 item = items[blockIdx.x];
+k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, int strided) {
+  const int2 item = items[strided > 0 ? 0 : blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
-  const CompTile<R> T(Sp, item.y);
+  const EwTiles W(item, strided, Sp->nt_comp);
   R* const f0 = Sp->f[0];
   R* const f1 = Sp->f[1];
   const R* __restrict__ t = Sp->t;
@@ -831,34 +859,37 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) 
   R min_fn = INFINITY, max_t = 0;
   double s_fp = 0;
   struct V4 { R f, u, h, t; };
-  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-    size_t ic, iu;
-    T.at(e, ic, iu);
-    return V4{f[ic], T.u[iu], T.h[ic], branch == 0 ? t[ic] : (R)0};
-  }, [&](int e, V4 v) {
-    const size_t ic = (size_t)T.cx0 * T.ty + e;
-    const R fa = v.f;
-    const R g = (v.u - v.h) - off;
-    R fn;
-    if (branch == 0) {
-      const bool c = (fa < 0) && (!has_h || fa > hdn);
-      fn = c ? (R)(fa + tau * v.t) : fa;
-    } else {
-      fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
-    }
-    const bool tensile = fn >= 0;
-    const bool flowing = has_h && fn <= hdn;
-    const bool nc = (tensile && g < 0) || (flowing && g > 0);
-    if (tensile) max_t = fmax(max_t, fn);
-    if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
-    const R fp = tensile ? (R)0 : fn;
-    s_fp += (double)fp;
-    n_nc += nc;
-    fo[ic] = fp;
-    if (has_h) gneg[ic] = g < 0;
-  });
+  for (int tile = W.first; tile < W.end; tile += W.step) {
+    const CompTile<R> T(Sp, tile);
+    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+      size_t ic, iu;
+      T.at(e, ic, iu);
+      return V4{f[ic], T.u[iu], T.h[ic], branch == 0 ? t[ic] : (R)0};
+    }, [&](int e, V4 v) {
+      const size_t ic = (size_t)T.cx0 * T.ty + e;
+      const R fa = v.f;
+      const R g = (v.u - v.h) - off;
+      R fn;
+      if (branch == 0) {
+        const bool c = (fa < 0) && (!has_h || fa > hdn);
+        fn = c ? (R)(fa + tau * v.t) : fa;
+      } else {
+        fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
+      }
+      const bool tensile = fn >= 0;
+      const bool flowing = has_h && fn <= hdn;
+      const bool nc = (tensile && g < 0) || (flowing && g > 0);
+      if (tensile) max_t = fmax(max_t, fn);
+      if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
+      const R fp = tensile ? (R)0 : fn;
+      s_fp += (double)fp;
+      n_nc += nc;
+      fo[ic] = fp;
+      if (has_h) gneg[ic] = g < 0;
+    });
+  }
   double v[5] = {(double)a_fl, (double)min_fn + H, (double)max_t, s_fp, (double)n_nc};
   const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
-  tile_finish<5>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+  tile_finish<5>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
                  [&](double (&a)[5]) { fin_update(*st, a); });
 }

@@ -490,6 +490,7 @@ struct Work {
   int persist_grid = 0, persist_threads = 0, persist_logn = 0;
   size_t persist_smem = 0;
   bool by_value = false;    // single solves: the by-value power-of-two passes (cm_ccg_p2.cuh)
+  int ew_grid[4] = {0, 0, 0, 0};  // by-value path: grids of begin, gsum, update, bisect
   CcgArgs<R> ccg_args{};    // their arguments
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
@@ -699,7 +700,21 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
       if (rc > 0) return CM_ERR_CUDA;
       w.by_value = rc == 0;
     }
-    if (w.by_value) w.persist = false;
+    if (w.by_value) {
+      w.persist = false;
+      // the element-wise passes walk the solve's tiles with at most one
+      // resident wave of blocks (one reduction partial per block)
+      int dev = 0, nsm = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      const void* ks[4] = {(const void*)k_ccg_begin<R>, (const void*)k_ccg_gsum<R>,
+                           (const void*)k_ccg_update<R>, (const void*)k_ccg_bisect<R>};
+      for (int k = 0; k < 4; ++k) {
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks[k], CM_THREADS, 0));
+        w.ew_grid[k] = std::max(1, std::min(w.nt_comp, per_sm * nsm));
+      }
+    }
   }
   w.ccg_ready = true;
   return CM_OK;
@@ -805,19 +820,22 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   const Tiles& T = w.tiles;
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], s); };
-  // an element-wise kernel: chained behind the previous pass in the by-value path
+  // element-wise kernel k (0 begin, 1 gsum, 2 update, 3 bisect): chained
+  // behind the previous pass and walking the tiles in the by-value path
   bool chain = w.by_value && !first;
-  auto elementwise = [&](void (*kern)(const Slot<R>*, const int2*)) {
-    if (chain) launch_pdl(kern, w.nt_comp, CM_THREADS, 0, s, S, it);
-    else kern<<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  auto elementwise = [&](void (*kern)(const Slot<R>*, const int2*, int), int k) {
+    const int grid = w.by_value ? w.ew_grid[k] : w.nt_comp;
+    const int strided = w.by_value ? w.nt_comp : 0;
+    if (chain) launch_pdl(kern, grid, CM_THREADS, 0, s, S, it, strided);
+    else kern<<<grid, CM_THREADS, 0, s>>>(S, it, strided);
     chain = w.by_value;
   };
   mark();
-  if (!w.by_value) elementwise(k_ccg_begin<R>);
+  if (!w.by_value) elementwise(k_ccg_begin<R>, 0);
   if (bisect)
-    for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>);
+    for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>, 3);
   mark();
-  elementwise(k_ccg_gsum<R>);
+  elementwise(k_ccg_gsum<R>, 1);
   mark();
   const bool p2 = T.p2;
   const int ly = p->fy.n, lx = p->fx.n;
@@ -835,7 +853,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     mark();
     ccg_p2_row_inv<R, MODE_T>(a, ry, s);
     mark();
-    elementwise(k_ccg_update<R>);
+    elementwise(k_ccg_update<R>, 2);
     mark();
     ccg_p2_row_fwd<R, MODE_F>(a, ry, s);
     mark();
@@ -854,7 +872,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   if (!(p2 && p2_row_inv<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
     k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
-  k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it);
+  k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it, 0);
   mark();
   if (!(p2 && p2_row_fwd<R, MODE_F>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
     k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
@@ -1000,7 +1018,7 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   if (w.by_value) {
     // start of the first iteration; later ones come from k_ccg_row_inv<MODE_F>
-    k_ccg_begin<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items);
+    k_ccg_begin<R><<<w.ew_grid[0], CM_THREADS, 0, s>>>(w.d_ccg, p->items, w.nt_comp);
     g_launches += 1;
   }
   const bool bisect = prm->has_hardness && prm->load_control;
@@ -1211,14 +1229,15 @@ static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_
 template <typename R>
 static void launch_iteration_batch(const BatchDev<R>& b, bool bisect, cudaStream_t s) {
   const Slot<R>* S = b.slots;
-  k_ccg_begin<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  k_ccg_begin<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
   if (bisect)
-    for (int i = 0; i < CM_BISECT_PASSES; ++i) k_ccg_bisect<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
-  k_ccg_gsum<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+    for (int i = 0; i < CM_BISECT_PASSES; ++i)
+      k_ccg_bisect<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
+  k_ccg_gsum<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
   k_row_fwd<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
   k_col<R, MODE_T><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
   k_row_inv<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
-  k_ccg_update<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+  k_ccg_update<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
   k_row_fwd<R, MODE_F><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
   k_col<R, MODE_F><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
   k_row_inv<R, MODE_F><<<b.n_items[2], CM_THREADS, b.smem_row, s>>>(S, b.items[2]);
