@@ -73,6 +73,55 @@ CM_DEVINL void tile_finish(double* __restrict__ partials, unsigned int* counter,
   }
 }
 
+#ifndef CM_BARRIER_SLEEP_NS
+#define CM_BARRIER_SLEEP_NS 32  // back-off between polls of the barrier word
+#endif
+
+CM_DEVINL unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+CM_DEVINL unsigned ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// All blocks of the grid meet; returns false if the wait gave up.
+CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicExch(&bar->gen, g + 1);
+    } else {
+      const long long t0 = clock64();
+      while (true) {
+        if (ld_acquire_gpu(&bar->gen) != g) break;
+        if (ld_relaxed_gpu(&bar->abort) != 0u) { ok = 0; break; }
+        if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) {
+          atomicExch(&bar->abort, 1u);
+          ok = 0;
+          break;
+        }
+        if (CM_BARRIER_SLEEP_NS > 0) __nanosleep(CM_BARRIER_SLEEP_NS);
+      }
+    }
+    __threadfence();
+    gen = g + 1;
+    *ok_sm = ok;
+  }
+  __syncthreads();
+  return *ok_sm != 0;
+}
+
 // stage the FFT descriptor and twiddle table of length n in shared memory
 template <typename C>
 CM_DEVINL void stage_fft(FftDesc& fd, const FftDesc& src, C* tws, const C* __restrict__ tw, int n) {
@@ -827,6 +876,87 @@ k_ccg_bisect(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, 
   for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
   tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, W.part, W.nparts, cnt, kinds,
                            [&](double (&a)[CM_BIS_CAND]) { fin_bisect(*st, a); });
+}
+
+// All the bisection passes of one iteration in one launch (single solves):
+// the blocks walk the solve's tiles as k_ccg_bisect's strided shape does,
+// the last block of each pass advances the bisection (fin_bisect), and a
+// grid barrier separates the passes, so an iteration without a mixing step
+// costs one launch instead of CM_BISECT_PASSES.  Launched cooperatively
+// (every block resident); the barrier's waits are bounded.
+template <typename R>
+__global__ void __launch_bounds__(CM_THREADS)
+k_ccg_bisect_passes(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, int ntiles,
+                    GridBarrier* bar) {
+  const Slot<R>* __restrict__ Sp = slots + items[0].x;
+  CcgState* st = Sp->st;
+  pdl_trigger();
+  pdl_wait();
+  __shared__ double cand[CM_BIS_CAND];
+  __shared__ double cand_lo, cand_hi;
+  __shared__ int go, ncand_s, ok_sm;
+  unsigned gen = 0;
+  if (threadIdx.x == 0) gen = ld_acquire_gpu(&bar->gen);
+  for (int pass = 0; pass < CM_BISECT_PASSES; ++pass) {
+    if (threadIdx.x == 0) {
+      // the state as the previous pass's last block left it, past this SM's L1
+      go = __ldcg(&st->done) == 0 && __ldcg(&st->branch) == 1 && __ldcg(&st->bs_active) != 0;
+      ncand_s = __ldcg(&st->bs_iter) < 0 ? 1 : CM_BIS_CAND;
+    }
+    __syncthreads();
+    if (!go) break;
+    const int ncand = ncand_s;
+    if (threadIdx.x < ncand) cand[threadIdx.x] = __ldcg(&st->bs_cand[threadIdx.x]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double lo = cand[0], hi = cand[0];
+      for (int i = 1; i < ncand; ++i) {
+        lo = fmin(lo, cand[i]);
+        hi = fmax(hi, cand[i]);
+      }
+      cand_lo = lo;
+      cand_hi = hi;
+    }
+    __syncthreads();
+    const double lo = cand_lo, hi = cand_hi;
+    int below_all = 0;
+    int icnt[CM_BIS_CAND];
+#pragma unroll
+    for (int i = 0; i < CM_BIS_CAND; ++i) icnt[i] = 0;
+    struct V2 { R u, h; };
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const CompTile<R> T(Sp, tile);
+      batched_loop<4>(T.cn, [&](int e) {
+        size_t ic, iu;
+        T.at(e, ic, iu);
+        return V2{T.u[iu], T.h[ic]};
+      }, [&](int, V2 v) {
+        const double g = (double)(v.u - v.h);
+        if (g < lo) {
+          ++below_all;
+        } else if (g < hi) {
+#pragma unroll
+          for (int i = 0; i < CM_BIS_CAND; ++i)
+            if (i < ncand) icnt[i] += (g - cand[i] < 0.0) ? 1 : 0;
+        }
+      });
+    }
+    double cnt[CM_BIS_CAND];
+#pragma unroll
+    for (int i = 0; i < CM_BIS_CAND; ++i) cnt[i] = (double)(icnt[i] + (i < ncand ? below_all : 0));
+    int kinds[CM_BIS_CAND];
+#pragma unroll
+    for (int i = 0; i < CM_BIS_CAND; ++i) kinds[i] = RED_SUM;
+    tile_finish<CM_BIS_CAND>(Sp->partials, Sp->counter, blockIdx.x, gridDim.x, cnt, kinds,
+                             [&](double (&a)[CM_BIS_CAND]) { fin_bisect(*st, a); });
+    if (!grid_barrier(bar, gen, &ok_sm)) {
+      if (threadIdx.x == 0) {
+        st->status = CMS_TIMEOUT;
+        st->done = 1;
+      }
+      break;
+    }
+  }
 }
 
 // Force update, projection onto [0, H], constraint bookkeeping

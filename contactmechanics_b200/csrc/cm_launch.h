@@ -6,19 +6,11 @@
 
 #include "cm_slot.cuh"
 
-#define CMS_TIMEOUT 6  // solve status: a grid-barrier or bulk-copy wait gave up
 
 // Dynamic shared memory a transform kernel may use (of the 227 KB a block can
 // hold on sm_100, leaving room for its static shared variables).
 #define CM_SMEM_DYN_MAX (220 * 1024)
 
-// Grid barrier of the persistent kernel (zeroed before every launch).
-struct GridBarrier {
-  unsigned int count;
-  unsigned int gen;
-  unsigned int abort;
-  unsigned int pad;
-};
 
 // Phases of one iteration as timed by the persistent kernel's stamps buffer.
 enum PersistPhase {

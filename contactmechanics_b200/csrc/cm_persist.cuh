@@ -23,60 +23,12 @@
 
 #include "cm_launch.h"
 
-#ifndef CM_BARRIER_SLEEP_NS
-#define CM_BARRIER_SLEEP_NS 32  // back-off between polls of the barrier word
-#endif
 #ifndef CM_PERSIST_MIN_BLOCKS_F
 #define CM_PERSIST_MIN_BLOCKS_F 1  // resident blocks per SM the FP32 kernel is compiled for
 #endif
 #ifndef CM_PERSIST_MIN_BLOCKS_D
 #define CM_PERSIST_MIN_BLOCKS_D 1
 #endif
-
-CM_DEVINL unsigned ld_acquire_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-CM_DEVINL unsigned ld_relaxed_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// All blocks of the grid meet; returns false if the wait gave up.
-CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    const unsigned g = gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicExch(&bar->gen, g + 1);
-    } else {
-      const long long t0 = clock64();
-      while (true) {
-        if (ld_acquire_gpu(&bar->gen) != g) break;
-        if (ld_relaxed_gpu(&bar->abort) != 0u) { ok = 0; break; }
-        if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) {
-          atomicExch(&bar->abort, 1u);
-          ok = 0;
-          break;
-        }
-        if (CM_BARRIER_SLEEP_NS > 0) __nanosleep(CM_BARRIER_SLEEP_NS);
-      }
-    }
-    __threadfence();
-    gen = g + 1;
-    *ok_sm = ok;
-  }
-  __syncthreads();
-  return *ok_sm != 0;
-}
 
 // Reduce ntiles x NV tile partials in a fixed order; result in thread 0.
 template <int NV>

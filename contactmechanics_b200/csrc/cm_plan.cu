@@ -20,7 +20,6 @@
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
 #define CM_SMEM_PERSIST_MAX (212 * 1024)  // dynamic shared memory of the persistent kernel
 #define CM_COMP_ELEMS 2048
-#define CM_BISECT_PASSES 21
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
 #define CM_PERSIST_ITERS 32   // iterations per cooperative launch
@@ -490,7 +489,8 @@ struct Work {
   int persist_grid = 0, persist_threads = 0, persist_logn = 0;
   size_t persist_smem = 0;
   bool by_value = false;    // single solves: the by-value power-of-two passes (cm_ccg_p2.cuh)
-  int ew_grid[4] = {0, 0, 0, 0};  // by-value path: grids of begin, gsum, update, bisect
+  int ew_grid[5] = {0, 0, 0, 0, 0};  // by-value path: grids of begin, gsum, update, bisect,
+                                     // and of the one-launch bisection (0: not used)
   CcgArgs<R> ccg_args{};    // their arguments
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
@@ -714,6 +714,14 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks[k], CM_THREADS, 0));
         w.ew_grid[k] = std::max(1, std::min(w.nt_comp, per_sm * nsm));
       }
+      // all bisection passes of an iteration in one cooperative launch
+      int coop = 0, per_sm = 0;
+      CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ccg_bisect_passes<R>, CM_THREADS, 0));
+      const char* e = std::getenv("CM_BISECT_ONE_LAUNCH");
+      w.ew_grid[4] = (coop && per_sm > 0 && !(e && e[0] == '0'))
+                         ? std::max(1, std::min(w.nt_comp, per_sm * nsm)) : 0;
+      if (w.ew_grid[4] && !w.bar) CKS(dalloc(p, &w.bar, 1));
     }
   }
   w.ccg_ready = true;
@@ -804,8 +812,8 @@ static const char* const k_iter_names[CM_ITER_KERNELS] = {
     "k_ccg_begin", "k_ccg_gsum", "k_row_fwd<T>", "k_col<T>", "k_row_inv<T>",
     "k_ccg_update", "k_row_fwd<F>", "k_col<F>", "k_row_inv<F>", "k_ccg_bisect"};
 
-static int iteration_launches(bool bisect, bool by_value) {
-  return CM_ITER_KERNELS - (by_value ? 2 : 1) + (bisect ? CM_BISECT_PASSES : 0);
+static int iteration_launches(bool bisect, bool by_value, bool one_bisect_launch = false) {
+  return CM_ITER_KERNELS - (by_value ? 2 : 1) + (bisect ? (one_bisect_launch ? 1 : CM_BISECT_PASSES) : 0);
 }
 
 // One CCG iteration.  With `ev` (CM_ITER_KERNELS + 1 events) an event is
@@ -832,8 +840,21 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   };
   mark();
   if (!w.by_value) elementwise(k_ccg_begin<R>, 0);
-  if (bisect)
+  if (bisect && w.by_value && w.ew_grid[4]) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(w.ew_grid[4]);
+    cfg.blockDim = dim3(CM_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_ccg_bisect_passes<R>, S, it, w.nt_comp, w.bar);
+    chain = true;
+  } else if (bisect) {
     for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>, 3);
+  }
   mark();
   elementwise(k_ccg_gsum<R>, 1);
   mark();
@@ -992,6 +1013,7 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
   st.scale = 1.0;
   CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), s));  // a solve that gave up may leave it set
+  if (w.bar && !w.persist) CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
   g_launches += 3;  // heights statistics (2) and the initial field
   k_h_prep<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64);
   k_h_var<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64, prm->pentol <= 0, rel_pentol);
@@ -1104,7 +1126,8 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   CKS(get_graph<R>(p, w, bisect, every, &g));
   for (int done_iters = 0;; done_iters += every) {
     CK(cudaGraphLaunch(g, s));
-    g_launches += (unsigned long long)every * iteration_launches(bisect, w.by_value);
+    g_launches += (unsigned long long)every *
+                   iteration_launches(bisect, w.by_value, w.by_value && w.ew_grid[4] > 0);
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     ++g_polls;

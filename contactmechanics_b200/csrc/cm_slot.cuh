@@ -19,6 +19,8 @@ enum {
 enum { CMM_RESET = 0, CMM_SD = 1, CMM_CG = 2, CMM_MIX = 3 };
 
 #define CM_BIS_CAND 31   // thresholds evaluated per bisection pass (5 levels)
+#define CM_BISECT_PASSES 21  // bisection passes per mixing step: 105 levels >= scipy's 100 iterations
+#define CMS_TIMEOUT 6  // solve status: a grid-barrier or bulk-copy wait gave up
 #define CM_RED_MAX 8     // reduction values per kernel
 
 struct CcgParams {
@@ -58,6 +60,16 @@ struct CcgState {
   // scipy-compatible bisection state (offset of the mixing step)
   double bs_xa, bs_dm, bs_fa;
   double bs_cand[CM_BIS_CAND + 1];
+};
+
+// Grid barrier (count of arrivals, generation, abort flag) of the kernels
+// whose blocks meet inside a launch: the persistent solver and the
+// bisection passes.  Zeroed with the solve's state.
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+  unsigned int abort;
+  unsigned int pad;
 };
 
 template <typename R>
