@@ -108,29 +108,42 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.samples = []
-        self._stop = threading.Event()
+        self._p = None
         self._t = None
+        self._first = threading.Event()
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.QUERY,
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            line = line.strip()
+            if line:
+                self.samples.append([x.strip() for x in line.split(",")])
+                self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        # one nvidia-smi process sampling every 200 ms, started before the
+        # timed region (its start-up stays outside) and stopped after it
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(5.0)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            self._p.wait(timeout=5)
+        except Exception:
+            self._p.kill()
+        self._t.join(timeout=5)
 
     def summary(self):
         if not self.samples:
@@ -640,6 +653,7 @@ def main():
                    "parallelism": f"replicas x{world}", "precision": "mixed (FP32 bulk, FP64 "
                    "reductions, FP64 refinement)"},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "latencies_ms": [round(float(x), 2) for x in lat],
         "fp64_value": r["fp64_value"], "speedup_vs_fp64": r["value"] / r["fp64_value"],
         "rel_err_vs_fp64": r["rel_err"], "area_rel_err_vs_fp64": r["area_err"],
         "iterations": {"mixed": r["iters"], "mixed_fp32_part": r["iters32"], "fp64": r["iters64"]},
