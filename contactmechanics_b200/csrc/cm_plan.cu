@@ -22,6 +22,7 @@
 #define CM_COMP_ELEMS 2048
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
+#define CM_FP32_ITER_CAP_PLASTIC 256
 #define CM_PERSIST_ITERS 32   // iterations per cooperative launch
 #ifndef CM_BY_VALUE_PASSES
 #define CM_BY_VALUE_PASSES 1  // single solves on power-of-two domains use cm_ccg_p2.cuh
@@ -46,9 +47,14 @@ static unsigned long long g_launches = 0;  // kernels launched by this library
 static thread_local int g_polls = 0;        // convergence polls of the current call
 
 // Iterations the FP32 phase of a mixed solve may take: at most
-// CM_FP32_ITER_CAP and half of the solve's maxiter, so that a phase that
-// stalls at FP32 resolution leaves the FP64 refinement at least half.
-static int fp32_cap(int maxiter) { return std::min(CM_FP32_ITER_CAP, std::max(1, maxiter / 2)); }
+// CM_FP32_ITER_CAP (CM_FP32_ITER_CAP_PLASTIC with a hardness) and half of the
+// solve's maxiter, so that a phase that stalls at FP32 resolution leaves the
+// FP64 refinement at least half.  Plastic phases get the lower cap: on
+// plastic requests whose FP64 solve converges in 40-214 iterations, FP32
+// phases were seen to run to 2000 without meeting the load test.
+static int fp32_cap(int maxiter, bool plastic) {
+  return std::min(plastic ? CM_FP32_ITER_CAP_PLASTIC : CM_FP32_ITER_CAP, std::max(1, maxiter / 2));
+}
 
 static cudaError_t& last_cuda_error() {
   static thread_local cudaError_t e = cudaSuccess;
@@ -1673,7 +1679,7 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   const double rf = prm->precision == CM_MIXED ? 1e-5 : 0.0;
   // FP32 phase: tolerances widened to FP32 resolution; a phase that cannot
   // reach them within its iteration cap hands over to the FP64 refinement
-  const int cap32 = prm->precision == CM_MIXED ? fp32_cap(prm->maxiter) : prm->maxiter;
+  const int cap32 = prm->precision == CM_MIXED ? fp32_cap(prm->maxiter, prm->has_hardness) : prm->maxiter;
   CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin));
   const double ms32 = ms_since(t0);
   if (prm->precision == CM_FP32) {
@@ -1746,7 +1752,7 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
     const double rf = prec == CM_MIXED ? 1e-5 : 0.0;
     for (int i = 0; i < n; ++i) {
       SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, plans[i]->ny};
-      const int mi = prec == CM_MIXED ? fp32_cap(params[i].maxiter) : params[i].maxiter;
+      const int mi = prec == CM_MIXED ? fp32_cap(params[i].maxiter, params[i].has_hardness) : params[i].maxiter;
       CKS(ccg_init<float>(plans[i], plans[i]->w32, &params[i], in, rp, rf, mi, s));
     }
     CKS(batch_loop<float>(n, plans, bisect, maxiter, timeout, s, &g_polls));
@@ -1853,7 +1859,7 @@ int cm_ccg_begin(cm_stepper* stp, cm_plan* p, const cm_ccg_params* prm, const do
   } else {
     const bool mixed = prm->precision == CM_MIXED;
     const double rp = mixed ? (prm->fp32_pentol_rel > 0 ? prm->fp32_pentol_rel : 2e-6) : 0.0;
-    const int mi = mixed ? fp32_cap(prm->maxiter) : prm->maxiter;
+    const int mi = mixed ? fp32_cap(prm->maxiter, prm->has_hardness) : prm->maxiter;
     CKS(ccg_init<float>(p, p->w32, prm, in, rp, mixed ? 1e-5 : 0.0, mi, stp->stream));
     p->phase = 1;
   }
