@@ -19,8 +19,9 @@
 // (k & (W-1)), so a column tile is one contiguous block (read and written
 // whole by k_col) and a row tile of R rows touches contiguous R*W runs.
 //
-// Every reduction is deterministic: per-tile partials in a fixed tile
-// order, reduced by the last tile of the slot (atomic ticket, no waiting).
+// Every reduction is deterministic: partials (one per tile, or one per block
+// when the blocks walk several tiles) reduced in a fixed order by the last
+// one to finish (atomic ticket, no waiting).
 #pragma once
 #include "cm_slot.cuh"
 

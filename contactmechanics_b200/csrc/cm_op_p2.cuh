@@ -14,9 +14,10 @@
 // Arguments travel by value (no descriptor upload), so a call is a plain
 // sequence of three launches on the caller's stream.  Blocks walk their
 // tiles with a grid stride, so the twiddle tables are staged once per block.
-// A block covers 2*NP rows (row passes, N/8 threads per transform) or
-// several column tiles (column pass, N/16 threads per transform), the
-// register-resident engines of cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
+// A block covers 2*NP rows (row passes, N/E threads per transform with E =
+// 8 elements per thread by default) or several column tiles (column pass,
+// N/16 threads per transform), the register-resident engines of
+// cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
 // touches whole rows-of-a-tile runs: (row, column-in-tile) fastest, which in
 // the plan's layout ((k >> lw) * nx + x) * W + (k & (W-1)) are contiguous.
 #pragma once
