@@ -2,7 +2,7 @@
 import numpy as np
 
 from .FFTElasticHalfSpace import ElasticSubstrate
-from .Systems import NonSmoothContactSystem
+from .Systems import NonSmoothContactSystem, _host
 from .Topography import PlasticTopography
 
 
@@ -20,5 +20,5 @@ class PlasticNonSmoothContactSystem(NonSmoothContactSystem):
         opt = super().minimize_proxy(hardness=hardness, **kwargs)
         if opt.success:
             self.surface.plastic_displ += np.where(
-                np.asarray(opt.plastic), self.compute_gap(self.disp, self.offset), 0.)
+                _host(opt.plastic), self.compute_gap(self.disp, self.offset), 0.)
         return opt

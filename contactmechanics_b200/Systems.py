@@ -5,6 +5,14 @@ from .FFTElasticHalfSpace import ElasticSubstrate
 from .Optimization import constrained_conjugate_gradients
 
 
+def _host(a):
+    """A numpy view of a result field: torch tensors (CUDA or not) are copied
+    to the host, numpy arrays pass through."""
+    if hasattr(a, "detach") and hasattr(a, "cpu"):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
 class IncompatibleFormulationError(Exception):
     pass
 
@@ -37,8 +45,8 @@ class SystemBase(object):
 
     def compute_gap(self, disp, offset, *profile_args, **profile_kwargs):
         """Gap ``disp - (heights + offset)`` on the topography (Systems.py:123-134)."""
-        return np.asarray(disp)[self.comp_slice] - \
-            (self.surface.heights(*profile_args, **profile_kwargs) + offset)
+        return _host(disp)[self.comp_slice] - \
+            (_host(self.surface.heights(*profile_args, **profile_kwargs)) + offset)
 
     def compute_contact_area(self):
         return self.compute_nb_contact_pts() * self.area_per_pt
@@ -70,13 +78,13 @@ class NonSmoothContactSystem(SystemBase):
         return self.surface.nb_grid_pts
 
     def compute_normal_force(self):
-        return float(np.sum(np.asarray(self.substrate.force)))
+        return float(np.sum(_host(self.substrate.force)))
 
     def compute_nb_contact_pts(self):
-        return int(np.sum(np.asarray(self.contact_zone)))
+        return int(np.sum(_host(self.contact_zone)))
 
     def compute_contact_coordinates(self):
-        return np.argwhere(np.asarray(self.contact_zone))
+        return np.argwhere(_host(self.contact_zone))
 
     def minimize_proxy(self, solver=constrained_conjugate_gradients, **kwargs):
         """Run ``solver(substrate, surface, **kwargs)`` and store the solution

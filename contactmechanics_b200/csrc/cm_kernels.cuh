@@ -90,8 +90,11 @@ CM_DEVINL unsigned ld_relaxed_gpu(const unsigned* p) {
   return v;
 }
 
-// All blocks of the grid meet; returns false if the wait gave up.
-CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
+// All blocks of the grid meet; returns false if the wait gave up (after
+// limit_cycles SM clock cycles, or when another block gave up first and set
+// the abort word).
+CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm,
+                            long long limit_cycles = CM_BARRIER_TIMEOUT_CYCLES) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
@@ -107,7 +110,7 @@ CM_DEVINL bool grid_barrier(GridBarrier* bar, unsigned& gen, int* ok_sm) {
       while (true) {
         if (ld_acquire_gpu(&bar->gen) != g) break;
         if (ld_relaxed_gpu(&bar->abort) != 0u) { ok = 0; break; }
-        if (clock64() - t0 > CM_BARRIER_TIMEOUT_CYCLES) {
+        if (clock64() - t0 > limit_cycles) {
           atomicExch(&bar->abort, 1u);
           ok = 0;
           break;
@@ -804,7 +807,10 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, in
     }, [&](int, V3 v) {
       const bool c = (v.f < 0) && (!has_h || v.f > hdn);
       const R g = (v.u - v.h) - off;
+      // the reference sums c * g^2 over the whole topography, so a NaN gap
+      // outside the contact set makes G NaN as well (0 * NaN)
       if (c) G += (double)g * (double)g;
+      else if (isnan(g)) G += (double)g;
     });
   }
   double v[1] = {G};

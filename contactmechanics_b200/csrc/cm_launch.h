@@ -1,6 +1,6 @@
 // Host-side declarations shared by the translation units of the library:
-// launchers of the power-of-two FFT passes (cm_p2.cu) and the persistent
-// solver kernel (cm_persist.cu), and the types their callers need.
+// launchers of the power-of-two FFT passes (cm_p2.cu, cm_op_p2.cu) and the
+// types their callers need.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -11,12 +11,6 @@
 // hold on sm_100, leaving room for its static shared variables).
 #define CM_SMEM_DYN_MAX (220 * 1024)
 
-
-// Phases of one iteration as timed by the persistent kernel's stamps buffer.
-enum PersistPhase {
-  PH_BEGIN, PH_BISECT, PH_GSUM, PH_ROW_FWD_T, PH_COL_T, PH_ROW_INV_T, PH_UPDATE, PH_ROW_FWD_F,
-  PH_COL_F, PH_ROW_INV_F, PH_COUNT
-};
 
 #define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
@@ -34,20 +28,6 @@ bool p2_row_inv(int logn, int grid, int threads, size_t smem, cudaStream_t s, co
 // Shared-memory attributes of every power-of-two pass (once per process).
 template <typename R>
 void set_p2_attrs();
-
-// Dynamic shared memory of the persistent kernel for sides n: twiddles, the
-// transform's two ping-pong buffers and two column-tile stages (each
-// 128-byte aligned).
-template <typename R>
-inline size_t persist_smem_bytes(int n, int row_tile, int col_tile) {
-  const size_t csize = 2 * sizeof(R);
-  int e = (row_tile / 2) * n;
-  if (col_tile * n > e) e = col_tile * n;
-  const size_t ebuf = (size_t)(e + (e >> 3) + 1);
-  const size_t head = ((n + 2 * ebuf) * csize + 127) & ~(size_t)127;
-  const size_t stage = ((size_t)n * col_tile * (csize + sizeof(R)) + 127) & ~(size_t)127;
-  return head + 2 * stage;
-}
 
 // The plain operator on power-of-two domains (cm_op_p2.cuh): three launches
 // on stream s.  op_p2_supported: whether sides 2^logx x 2^logy with column
@@ -122,8 +102,3 @@ int ccg_p2_row_inv(const CcgArgs<R>& a, int logy, cudaStream_t s);
 template <typename R>
 int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy);
 
-// Host stub of the persistent kernel for square 2^logn domains, or nullptr.
-// Kernel arguments: (const Slot<R>*, GridBarrier*, int max_iters,
-// int bisect_passes, unsigned long long* stamps).
-template <typename R>
-const void* persist_kernel(int logn);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,12 +19,10 @@
 #include "cm_launch.h"
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
-#define CM_SMEM_PERSIST_MAX (212 * 1024)  // dynamic shared memory of the persistent kernel
 #define CM_COMP_ELEMS 2048
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
 #define CM_FP32_ITER_CAP_PLASTIC 256
-#define CM_PERSIST_ITERS 32   // iterations per cooperative launch
 #ifndef CM_BY_VALUE_PASSES
 #define CM_BY_VALUE_PASSES 1  // single solves on power-of-two domains use cm_ccg_p2.cuh
 #endif
@@ -43,7 +42,8 @@
     if (s_ != CM_OK) return s_;      \
   } while (0)
 
-static unsigned long long g_launches = 0;  // kernels launched by this library
+// kernels launched by this library (serving worker threads launch concurrently)
+static std::atomic<unsigned long long> g_launches{0};
 static thread_local int g_polls = 0;        // convergence polls of the current call
 
 // Iterations the FP32 phase of a mixed solve may take: at most
@@ -490,10 +490,7 @@ struct Work {
   double* partials = nullptr;
   unsigned int* counter = nullptr;
   bool ccg_ready = false;
-  GridBarrier* bar = nullptr;   // persistent solver: grid barrier
-  bool persist = false;         // persistent cooperative kernel usable
-  int persist_grid = 0, persist_threads = 0, persist_logn = 0;
-  size_t persist_smem = 0;
+  GridBarrier* bar = nullptr;   // one-launch bisection: grid barrier
   bool by_value = false;    // single solves: the by-value power-of-two passes (cm_ccg_p2.cuh)
   int ew_grid[5] = {0, 0, 0, 0, 0};  // by-value path: grids of begin, gsum, update, bisect,
                                      // and of the one-launch bisection (0: not used)
@@ -666,7 +663,6 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
   w.nt_col = s.nt_col;
   CK(cudaMemcpyAsync(w.d_ccg, &s, sizeof(s), cudaMemcpyHostToDevice, p->stream));
   CK(cudaStreamSynchronize(p->stream));
-  CKS(setup_persist(p, w));
   {
     // by-value passes for power-of-two domains (single solves)
     const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
@@ -707,7 +703,6 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
       w.by_value = rc == 0;
     }
     if (w.by_value) {
-      w.persist = false;
       // the element-wise passes walk the solve's tiles with at most one
       // resident wave of blocks (one reduction partial per block)
       int dev = 0, nsm = 0;
@@ -856,8 +851,16 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_ccg_bisect_passes<R>, S, it, w.nt_comp, w.bar);
-    chain = true;
+    if (cudaLaunchKernelEx(&cfg, k_ccg_bisect_passes<R>, S, it, w.nt_comp, w.bar) == cudaSuccess) {
+      chain = true;
+    } else {
+      // the cooperative launch was refused (for example fewer SMs available
+      // than the occupancy query counted): clear the error and run the
+      // passes as separate launches from now on
+      cudaGetLastError();
+      w.ew_grid[4] = 0;
+      for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>, 3);
+    }
   } else if (bisect) {
     for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>, 3);
   }
@@ -923,59 +926,27 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
     cudaGraphExecDestroy(w.graph[gi]);
     w.graph[gi] = nullptr;
   }
-  cudaGraph_t g;
-  CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed));
-  for (int i = 0; i < iters; ++i) launch_iteration<R>(p, w, bisect, p->stream, nullptr, i == 0);
-  cudaError_t e = cudaStreamEndCapture(p->stream, &g);
-  CK(e);
-  e = cudaGraphInstantiate(&w.graph[gi], g, 0);
-  cudaGraphDestroy(g);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaSuccess;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool coop = bisect && w.ew_grid[4] > 0;
+    CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed));
+    for (int i = 0; i < iters; ++i) launch_iteration<R>(p, w, bisect, p->stream, nullptr, i == 0);
+    e = cudaStreamEndCapture(p->stream, &g);
+    if (e == cudaSuccess) {
+      e = cudaGraphInstantiate(&w.graph[gi], g, 0);
+      cudaGraphDestroy(g);
+    }
+    if (e == cudaSuccess || !coop) break;
+    // a graph with the cooperative bisection launch could not be built:
+    // capture again with the bisection passes as separate launches
+    cudaGetLastError();
+    w.graph[gi] = nullptr;
+    w.ew_grid[4] = 0;
+  }
   CK(e);
   w.graph_iters[gi] = iters;
   *out = w.graph[gi];
-  return CM_OK;
-}
-
-// ---- persistent cooperative solver --------------------------------------------
-// Decide whether the persistent kernel can run this plan and size its grid.
-template <typename R>
-static int setup_persist(cm_plan* p, Work<R>& w) {
-  w.persist = false;
-  const Tiles& T = w.tiles;
-  if (!T.p2 || p->nx != p->ny || T.p2_threads_row != T.p2_threads_col) return CM_OK;
-  const int logn = log2_exact(p->nx);
-  const void* k = persist_kernel<R>(logn);
-  if (!k) return CM_OK;
-  const size_t smem = persist_smem_bytes<R>(p->nx, T.row_tile, T.col_tile);
-  if (smem > CM_SMEM_PERSIST_MAX) return CM_OK;
-  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-  int per_sm = 0, dev = 0, nsm = 0, coop = 0;
-  CK(cudaGetDevice(&dev));
-  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, T.p2_threads_row, smem));
-  if (!coop || per_sm < 1) return CM_OK;
-  const int tiles = std::max({w.nt_comp, w.nt_rowd, w.nt_col});
-  w.persist_grid = std::min(per_sm * nsm, tiles);
-  w.persist_threads = T.p2_threads_row;
-  w.persist_smem = smem;
-  w.persist_logn = logn;
-  if (!w.bar) CKS(dalloc(p, &w.bar, 1));
-  w.persist = true;
-  return CM_OK;
-}
-
-template <typename R>
-static int launch_persist(cm_plan* p, Work<R>& w, int iters, int bisect_passes, cudaStream_t s,
-                          unsigned long long* stamps = nullptr) {
-  CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
-  const Slot<R>* S = w.d_ccg;
-  GridBarrier* bar = w.bar;
-  void* args[] = {(void*)&S, (void*)&bar, (void*)&iters, (void*)&bisect_passes, (void*)&stamps};
-  CK(cudaLaunchCooperativeKernel(persist_kernel<R>(w.persist_logn), dim3(w.persist_grid),
-                                 dim3(w.persist_threads), args, w.persist_smem, s));
-  g_launches += 1;
   return CM_OK;
 }
 
@@ -1019,7 +990,7 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
   st.scale = 1.0;
   CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), s));  // a solve that gave up may leave it set
-  if (w.bar && !w.persist) CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
+  if (w.bar) CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
   g_launches += 3;  // heights statistics (2) and the initial field
   k_h_prep<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64);
   k_h_var<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, in.h64, prm->pentol <= 0, rel_pentol);
@@ -1050,38 +1021,6 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     g_launches += 1;
   }
   const bool bisect = prm->has_hardness && prm->load_control;
-  if (prof_iters > 0 && w.persist) {
-    // profiler: one cooperative launch of prof_iters iterations timed with
-    // events, then a second one with phase stamps
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, s));
-    CKS(launch_persist(p, w, prof_iters, bisect ? CM_BISECT_PASSES : 0, s));
-    CK(cudaEventRecord(e1, s));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    prof_ms[0] = ms / prof_iters;
-    CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
-    unsigned long long* stamps = nullptr;
-    CK(cudaMalloc(&stamps, PH_COUNT * sizeof(unsigned long long)));
-    unsigned long long ns[PH_COUNT];
-    int rc = cudaMemsetAsync(stamps, 0, sizeof(ns), s) == cudaSuccess ? CM_OK : CM_ERR_CUDA;
-    if (rc == CM_OK) rc = launch_persist(p, w, prof_iters, bisect ? CM_BISECT_PASSES : 0, s, stamps);
-    if (rc == CM_OK && cudaMemcpyAsync(ns, stamps, sizeof(ns), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-      rc = CM_ERR_CUDA;
-    if (rc == CM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = CM_ERR_CUDA;
-    cudaFree(stamps);
-    CKS(rc);
-    for (int k = 0; k < PH_COUNT; ++k) prof_ms[1 + k] = (float)(ns[k] * 1e-6 / prof_iters);
-    CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    *fin = *p->h_state;
-    return CM_OK;
-  }
   if (prof_iters > 0) {
     // profiler: eager launches with an event between kernels
     std::vector<cudaEvent_t> ev(CM_ITER_KERNELS + 1);
@@ -1108,26 +1047,6 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     every = work >= (1L << 20) ? (w.by_value ? 8 : 4) : (work >= (1L << 16) ? 8 : 16);
   }
   auto t0 = std::chrono::steady_clock::now();
-  if (w.persist) {
-    for (int done_iters = 0;; done_iters += CM_PERSIST_ITERS) {
-      CKS(launch_persist(p, w, CM_PERSIST_ITERS, bisect ? CM_BISECT_PASSES : 0, s));
-      CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      ++g_polls;
-      if (p->h_state->done) break;
-      if (prm->timeout_s > 0) {
-        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (el > prm->timeout_s) return CM_ERR_TIMEOUT;
-      }
-      if (done_iters > maxiter + 2 * CM_PERSIST_ITERS) return CM_ERR_CUDA;
-    }
-    *fin = *p->h_state;
-    if (fin->status == CMS_TIMEOUT) return CM_ERR_TIMEOUT;
-    if (fin->status == CMS_NAN) return CM_ERR_NAN;
-    if (fin->status == CMS_BISECT_SIGN) return CM_ERR_BISECT;
-    if (fin->status == CMS_BISECT_SIGN + 1) return CM_ERR_BISECT_CONV;
-    return CM_OK;
-  }
   cudaGraphExec_t g;
   CKS(get_graph<R>(p, w, bisect, every, &g));
   for (int done_iters = 0;; done_iters += every) {
@@ -1428,6 +1347,20 @@ static int stepper_run(cm_stepper* stp, const std::vector<cm_plan*>& plans, int 
 }
 
 // ---------------------------------------------------------------------------
+// self-test of the bounded grid barrier
+// ---------------------------------------------------------------------------
+// Every block meets at one grid barrier (cm_kernels.cuh: grid_barrier) with a
+// wait limit of `limit` SM clock cycles; blocks whose wait gave up are counted.
+__global__ void __launch_bounds__(128) k_selftest_barrier(GridBarrier* bar, long long limit,
+                                                          int* gave_up) {
+  __shared__ int ok_sm;
+  unsigned gen = 0;
+  if (threadIdx.x == 0) gen = ld_acquire_gpu(&bar->gen);
+  const bool ok = grid_barrier(bar, gen, &ok_sm, limit);
+  if (threadIdx.x == 0 && !ok) atomicAdd(gave_up, 1);
+}
+
+// ---------------------------------------------------------------------------
 // periodic operator that allocates nothing
 // ---------------------------------------------------------------------------
 // Scratch of cm_apply_periodic_noalloc: a fixed 4 MiB array in the library's
@@ -1439,24 +1372,18 @@ static int stepper_run(cm_stepper* stp, const std::vector<cm_plan*>& plans, int 
 // share the array and race.
 #define CM_NOALLOC_MAX_SIDE 512
 #define CM_NOALLOC_BYTES (4u << 20)
-#define CM_NOALLOC_MAX_DEVICES 64
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CM_NOALLOC_BYTES];
 
-static void* g_noalloc_addr[CM_NOALLOC_MAX_DEVICES] = {};
-static std::mutex g_noalloc_mu;
-
-// device address of the scratch on the current device (resolved once)
+// Device address of the scratch on the current device.  Looked up on every
+// call (cudaGetSymbolAddress allocates nothing and is cheap), so an address
+// never outlives the context it was taken in (cudaDeviceReset, a primary
+// context released and created again).  The first lookup on a device may
+// load the library's module there, which is why the first call should come
+// before any stream capture.
 static int noalloc_scratch(unsigned char** out) {
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= CM_NOALLOC_MAX_DEVICES) return CM_ERR_ARG;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* ptr = nullptr;
-    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    g_noalloc_addr[dev] = ptr;
-  }
-  *out = (unsigned char*)g_noalloc_addr[dev];
+  void* ptr = nullptr;
+  CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+  *out = (unsigned char*)ptr;
   return CM_OK;
 }
 
@@ -1815,7 +1742,7 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
   return CM_OK;
 }
 
-unsigned long long cm_launch_count(void) { return g_launches; }
+unsigned long long cm_launch_count(void) { return g_launches.load(); }
 
 int cm_stepper_create(void* stream, cm_stepper** out) {
   if (!out) return CM_ERR_ARG;
@@ -1998,6 +1925,43 @@ int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young
   return CM_OK;
 }
 
+int cm_selftest_grid_barrier(int blocks, int phantom, double limit_us, int* gave_up) {
+  if (blocks < 1 || phantom < 0 || !(limit_us > 0) || limit_us > 1e7 || !gave_up) return CM_ERR_ARG;
+  int dev = 0, nsm = 0, coop = 0, per_sm = 0, khz = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  CK(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_selftest_barrier, 128, 0));
+  if (!coop || blocks > per_sm * nsm) return CM_ERR_ARG;  // every block must be resident
+  const long long limit = (long long)(limit_us * 1e-3 * khz) + 1;
+  struct Buf {
+    GridBarrier bar;
+    int gave_up;
+  };
+  Buf* d = nullptr;
+  CK(cudaMalloc(&d, sizeof(Buf)));
+  Buf h;
+  memset(&h, 0, sizeof(h));
+  h.bar.count = (unsigned)phantom;
+  int rc = CM_OK;
+  if (cudaMemcpy(d, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) rc = CM_ERR_CUDA;
+  if (rc == CM_OK) {
+    GridBarrier* bar = &d->bar;
+    int* out = &d->gave_up;
+    void* args[] = {(void*)&bar, (void*)&limit, (void*)&out};
+    g_launches += 1;
+    if (cudaLaunchCooperativeKernel((const void*)k_selftest_barrier, dim3(blocks), dim3(128), args, 0,
+                                    nullptr) != cudaSuccess ||
+        cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = CM_ERR_CUDA;
+  }
+  if (rc != CM_OK) last_cuda_error() = cudaGetLastError();
+  cudaFree(d);
+  *gave_up = h.gave_up;
+  return rc;
+}
+
 int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int iters,
                    float* ms_per_kernel, int* n_kernels, const char** names) {
   if (!p || !prm || !h || iters < 1 || !ms_per_kernel) return CM_ERR_ARG;
@@ -2009,23 +1973,9 @@ int cm_ccg_profile(cm_plan* p, const cm_ccg_params* prm, const double* h, int it
     CKS(run_ccg<double>(p, p->w64, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
   else
     CKS(run_ccg<float>(p, p->w32, &q, in, 0.0, 0.0, q.maxiter, &fin, iters, ms_per_kernel));
-  const bool persist = prm->precision == CM_FP64 ? p->w64.persist : p->w32.persist;
-  if (persist) {
-    static const char* phase_names[PH_COUNT] = {
-        "k_ccg_persist:begin",   "k_ccg_persist:bisect",    "k_ccg_persist:gsum",
-        "k_ccg_persist:row_fwd_t", "k_ccg_persist:col_t",   "k_ccg_persist:row_inv_t",
-        "k_ccg_persist:update",  "k_ccg_persist:row_fwd_f", "k_ccg_persist:col_f",
-        "k_ccg_persist:row_inv_f"};
-    if (n_kernels) *n_kernels = 1 + PH_COUNT;
-    if (names) {
-      names[0] = "k_ccg_persist";
-      for (int k = 0; k < PH_COUNT; ++k) names[1 + k] = phase_names[k];
-    }
-  } else {
-    if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
-    if (names)
-      for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) names[k] = k_iter_names[k];
-  }
+  if (n_kernels) *n_kernels = CM_ITER_KERNELS - 1;
+  if (names)
+    for (int k = 0; k < CM_ITER_KERNELS - 1; ++k) names[k] = k_iter_names[k];
   return fin.done && fin.it < iters ? CM_ERR_ARG : CM_OK;
 }
 

@@ -236,14 +236,30 @@ int cm_ccg_end(cm_stepper* stepper, cm_plan* plan, double* x_dev, double* jac_de
  * memory (each GPU that loads the library holds it until the process exits),
  * so nx and ny are limited to 512; larger grids return CM_ERR_SIZE.  in_dev
  * and out_dev are caller-owned (nx, ny) FP64 device arrays; work is enqueued
- * on `stream` (NULL: the legacy default stream).  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array: calls
+ * on `stream` (NULL: the legacy default stream).  Every call looks up that
+ * array's device address on the current device (cudaGetSymbolAddress); the
+ * first lookup on a device may load the library's code there, so make the
+ * first call on each device before any stream capture.  All calls share the array: calls
  * that overlap on the GPU race and corrupt each other's results.
  * This entry point has no counterpart in the reference.
  */
 int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young, double poisson,
                               int op, const double* in_dev, double* out_dev, void* stream);
+
+/*
+ * Self-test of the bounded grid barrier that separates the passes of the
+ * solver's one-launch offset bisection (and every other wait on another
+ * block inside a launch): `blocks` blocks, launched cooperatively, meet at
+ * one barrier whose arrival count starts at `phantom`.  With phantom = 0 the
+ * barrier completes; with phantom >= blocks the count never reaches the
+ * release value (arrivals that never come), so every block waits until its
+ * limit of `limit_us` microseconds of SM clock runs out, the first to give up
+ * raises the barrier's abort word and the others leave.  *gave_up receives
+ * the number of blocks whose wait gave up.  The launch ends by itself either
+ * way and leaves the context usable.  Instrumentation; no reference
+ * counterpart.
+ */
+int cm_selftest_grid_barrier(int blocks, int phantom, double limit_us, int* gave_up);
 
 /*
  * Number of kernels this library has launched in the process (graph nodes

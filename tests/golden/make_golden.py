@@ -1,9 +1,9 @@
 """Generate golden vectors by running the reference's own code.
 
-Run in a container that has the reference checkout (read-only) at
-``/root/reference``::
+Run where a checkout of the reference is available (read-only is enough)::
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
+    # or: CM_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 
 It imports ContactMechanics unmodified over the serial stand-ins of
 ``refstubs.py`` and writes ``tests/golden/*.npz``.  The fixtures are small
@@ -206,4 +206,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py /path/to/reference (or set CM_REFERENCE)")
+    main(ref)
