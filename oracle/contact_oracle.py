@@ -547,6 +547,22 @@ def self_affine(nb_grid_pts, physical_sizes, hurst, rms_slope, seed,
 # Automated sweeps (PipelineFunction.py:37-449)
 # ---------------------------------------------------------------------------
 
+def auto_offset(step, mean_displacements, total_contact_areas, heights):
+    """Offset of automatic step `step` of a sweep from the offsets and contact
+    areas of the steps before it (PipelineFunction.py:138-226)."""
+    top, middle, bot = np.max(heights), np.mean(heights), np.min(heights)
+    if step == 0:
+        return -middle
+    if step == 1:
+        return -top + 0.01 * (top - middle)
+    sd, sa = np.transpose(sorted(zip(mean_displacements, total_contact_areas),
+                                 key=lambda pair: pair[1]))
+    ref_area = np.log10(np.array(sa + 1 / np.prod(np.shape(heights))))
+    darea = np.append(ref_area[1:] - ref_area[:-1], -ref_area[-1])
+    i = np.argmax(darea)
+    return bot + 2 * (sd[-1] - bot) if i == step - 1 else (sd[i] + sd[i + 1]) / 2
+
+
 def contact_mechanics(heights, physical_sizes, periodic=True, nsteps=None, offsets=None,
                       pressures=None, hardness=None, maxiter=100, results_callback=None,
                       **solver_kwargs):
@@ -605,18 +621,6 @@ def contact_mechanics(heights, physical_sizes, periodic=True, nsteps=None, offse
     else:
         for step in range(nsteps):
             state["pd"] = np.zeros(nb)
-            h = cur_heights()
-            top, middle, bot = np.max(h), np.mean(h), np.min(h)
-            if step == 0:
-                off = -middle
-            elif step == 1:
-                off = -top + 0.01 * (top - middle)
-            else:
-                sd, sa = np.transpose(sorted(zip(md, ta), key=lambda pair: pair[1]))
-                ref_area = np.log10(np.array(sa + 1 / np.prod(nb)))
-                darea = np.append(ref_area[1:] - ref_area[:-1], -ref_area[-1])
-                i = np.argmax(darea)
-                off = bot + 2 * (sd[-1] - bot) if i == step - 1 else (sd[i] + sd[i + 1]) / 2
-            calc(offset=off)
+            calc(offset=auto_offset(step, md, ta, cur_heights()))
     return np.array(mp), np.array(ta), np.array(md), np.array(mg), np.array(conv)
 
