@@ -37,6 +37,23 @@
 #define CM_COL16_FP64_BASE 128
 #endif
 
+// threads of an FP32 row-pass block (at least one transform) and the
+// resident blocks per SM it is compiled for
+#ifndef CM_ROW_F32_BASE
+#define CM_ROW_F32_BASE 512
+#endif
+#ifndef CM_ROW_F32_MINB
+#define CM_ROW_F32_MINB 2
+#endif
+
+// threads of an FP32 column-pass block and its resident blocks per SM
+#ifndef CM_COL16_F32_BASE
+#define CM_COL16_F32_BASE 256
+#endif
+#ifndef CM_COL16_F32_MINB
+#define CM_COL16_F32_MINB 2
+#endif
+
 // log2 of the elements per thread of the row passes' transforms (3: the
 // radix-8 engine, 4: the radix-16 one)
 #ifndef CM_ROW_LR_F32
@@ -53,10 +70,10 @@ struct OpShape {
   static constexpr int LR = sizeof(R) == 8 ? CM_ROW_LR_F64 : CM_ROW_LR_F32;
   static constexpr int E = 1 << LR;  // elements per thread
   static constexpr int TPS = N >> LR;
-  static constexpr int BASE = (sizeof(R) == 8 ? 256 : 512) >> (LR - 3);
+  static constexpr int BASE = (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
-  static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : 2;
+  static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : CM_ROW_F32_MINB;
   // block strides of a row-pair gather whose loads are issued together (the
   // gather of a row tile with column tiles W <= N/8 takes at most five); the
   // FP64 passes have the registers to spare, the FP32 ones do not
@@ -176,10 +193,10 @@ template <typename R, int LOGN>
 struct OpShape16 {
   static constexpr int N = 1 << LOGN;
   static constexpr int TPS = N / 16;
-  static constexpr int BASE = sizeof(R) == 8 ? CM_COL16_FP64_BASE : 256;
+  static constexpr int BASE = sizeof(R) == 8 ? CM_COL16_FP64_BASE : CM_COL16_F32_BASE;
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // columns per block
-  static constexpr int MINB = sizeof(R) == 4 || BASE < 256 ? 2 : 1;
+  static constexpr int MINB = sizeof(R) == 4 ? CM_COL16_F32_MINB : (BASE < 256 ? 2 : 1);
   static size_t smem() {
     return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
   }
