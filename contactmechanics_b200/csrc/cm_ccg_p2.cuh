@@ -344,3 +344,183 @@ k_ccg_row_inv(CcgArgs<R> a) {
     });
   }
 }
+
+// ---------------------------------------------------------------------------
+// Element-wise passes of the single-solve path, vectorised.  The topography
+// fields (h, f, t: tx x ty, rows of a power-of-two length ty >= 64) and the
+// displacement (u: rows of length ny on the domain) are read in 16-byte
+// vectors of V = 16 / sizeof(R) consecutive elements of one row; every
+// thread has U vectors of each field in flight, the grid is one resident
+// wave that strides over the vectors, and each block writes one reduction
+// partial.  The arithmetic per element is that of the per-tile kernels of
+// cm_kernels.cuh (same formulas, same precision).
+// ---------------------------------------------------------------------------
+template <typename R>
+struct alignas(16) Vec16 {
+  static constexpr int V = 16 / sizeof(R);
+  R v[V];
+};
+
+#define CM_EW_THREADS 256
+
+// vector j of the topography: element index (topography) and displacement index
+struct EwIndex {
+  int lvr;      // log2 of the vectors per topography row
+  int ny;       // displacement row length
+  int V;
+  CM_DEVINL void at(long j, size_t& ic, size_t& iu) const {
+    const long x = j >> lvr;
+    const long y = (j - (x << lvr)) * V;
+    ic = (size_t)j * V;
+    iu = (size_t)x * ny + y;
+  }
+};
+
+template <typename R>
+CM_DEVINL EwIndex ew_index(const CcgArgs<R>& a) {
+  EwIndex e;
+  e.V = Vec16<R>::V;
+  e.lvr = (__ffs(a.ty) - 1) - (__ffs(Vec16<R>::V) - 1);
+  e.ny = a.ny;
+  return e;
+}
+
+// G = sum over the CG area of g^2 (ConstrainedConjugateGradients.py:273-279)
+template <typename R, int U>
+__global__ void __launch_bounds__(CM_EW_THREADS) k_ew_gsum(CcgArgs<R> a) {
+  typedef Vec16<R> VR;
+  constexpr int V = VR::V;
+  const EwIndex ix = ew_index(a);
+  const long nvec = (long)a.tx * a.ty / V;
+  pdl_trigger();
+  pdl_wait();
+  CcgState* st = a.st;
+  if (st->done || st->branch != 0) return;
+  const int has_h = st->p.has_h;
+  const R hdn = neg_down<R>(st->p.H);
+  const R off = (R)st->offset;
+  const R* __restrict__ f = a.f[st->parity & 1];
+  const R* __restrict__ u = a.u;
+  const R* __restrict__ h = a.h;
+  double G = 0;
+  const long step = (long)gridDim.x * blockDim.x * U;
+  for (long j0 = (long)blockIdx.x * blockDim.x * U + threadIdx.x; j0 < nvec; j0 += step) {
+    VR fv[U], uv[U], hv[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const long j = j0 + (long)i * blockDim.x;
+      if (j >= nvec) continue;
+      size_t ic, iu;
+      ix.at(j, ic, iu);
+      fv[i] = *reinterpret_cast<const VR*>(f + ic);
+      uv[i] = *reinterpret_cast<const VR*>(u + iu);
+      hv[i] = *reinterpret_cast<const VR*>(h + ic);
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      if (j0 + (long)i * blockDim.x >= nvec) continue;
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const R fa = fv[i].v[e];
+        const bool c = (fa < 0) && (!has_h || fa > hdn);
+        const R g = (uv[i].v[e] - hv[i].v[e]) - off;
+        // the reference sums c * g^2 over the whole topography, so a NaN gap
+        // outside the contact set makes G NaN as well (0 * NaN)
+        if (c) G += (double)g * (double)g;
+        else if (isnan(g)) G += (double)g;
+      }
+    }
+  }
+  double v[1] = {G};
+  const int kinds[1] = {RED_SUM};
+  tile_finish<1>(a.partials, a.counter, blockIdx.x, gridDim.x, v, kinds,
+                 [&](double (&r)[1]) { fin_gsum(*st, r); });
+}
+
+// Force update, projection onto [0, H] and the constraint bookkeeping
+// (ConstrainedConjugateGradients.py:296, 320-389)
+template <typename R, int U>
+__global__ void __launch_bounds__(CM_EW_THREADS) k_ew_update(CcgArgs<R> a) {
+  typedef Vec16<R> VR;
+  constexpr int V = VR::V;
+  const EwIndex ix = ew_index(a);
+  const long nvec = (long)a.tx * a.ty / V;
+  pdl_trigger();
+  pdl_wait();
+  CcgState* st = a.st;
+  if (st->done) return;
+  const int par = st->parity & 1, has_h = st->p.has_h, branch = st->branch;
+  const double H = st->p.H;
+  const R off = (R)st->offset;
+  const R tau = (R)st->tau;
+  const double mix = st->cur_mixfac;
+  const R* __restrict__ f = a.f[par];
+  R* __restrict__ fo = a.f[par ^ 1];
+  const R* __restrict__ t = a.t;
+  const R* __restrict__ u = a.u;
+  const R* __restrict__ h = a.h;
+  unsigned char* __restrict__ gneg = const_cast<unsigned char*>(a.gneg);
+  const R hdn = neg_down<R>(H);
+  // counts in int and extrema in R are exact (x -> (double)x + H is
+  // monotonic, so the minimum of fn + H is the minimum fn plus H); only the
+  // force sum is accumulated in FP64
+  int a_fl = 0, n_nc = 0;
+  R min_fn = INFINITY, max_t = 0;
+  double s_fp = 0;
+  const long step = (long)gridDim.x * blockDim.x * U;
+  for (long j0 = (long)blockIdx.x * blockDim.x * U + threadIdx.x; j0 < nvec; j0 += step) {
+    VR fv[U], uv[U], hv[U], tv[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const long j = j0 + (long)i * blockDim.x;
+      if (j >= nvec) continue;
+      size_t ic, iu;
+      ix.at(j, ic, iu);
+      fv[i] = *reinterpret_cast<const VR*>(f + ic);
+      uv[i] = *reinterpret_cast<const VR*>(u + iu);
+      hv[i] = *reinterpret_cast<const VR*>(h + ic);
+      if (branch == 0) tv[i] = *reinterpret_cast<const VR*>(t + ic);
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const long j = j0 + (long)i * blockDim.x;
+      if (j >= nvec) continue;
+      VR out;
+      unsigned char gn[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const R fa = fv[i].v[e];
+        const R g = (uv[i].v[e] - hv[i].v[e]) - off;
+        R fn;
+        if (branch == 0) {
+          const bool c = (fa < 0) && (!has_h || fa > hdn);
+          fn = c ? (R)(fa + tau * tv[i].v[e]) : fa;
+        } else {
+          fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
+        }
+        const bool tensile = fn >= 0;
+        const bool flowing = has_h && fn <= hdn;
+        const bool nc = (tensile && g < 0) || (flowing && g > 0);
+        if (tensile) max_t = fmax(max_t, fn);
+        if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
+        const R fp = tensile ? (R)0 : fn;
+        s_fp += (double)fp;
+        n_nc += nc;
+        out.v[e] = fp;
+        gn[e] = g < 0;
+      }
+      const size_t ic = (size_t)j * V;
+      *reinterpret_cast<VR*>(fo + ic) = out;
+      if (has_h) {
+        if constexpr (V == 4)
+          *reinterpret_cast<uchar4*>(gneg + ic) = make_uchar4(gn[0], gn[1], gn[2], gn[3]);
+        else
+          *reinterpret_cast<uchar2*>(gneg + ic) = make_uchar2(gn[0], gn[1]);
+      }
+    }
+  }
+  double v[5] = {(double)a_fl, (double)min_fn + H, (double)max_t, s_fp, (double)n_nc};
+  const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
+  tile_finish<5>(a.partials, a.counter, blockIdx.x, gridDim.x, v, kinds,
+                 [&](double (&r)[5]) { fin_update(*st, r); });
+}

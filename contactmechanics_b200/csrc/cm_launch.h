@@ -64,14 +64,26 @@ struct CcgArgs {
   double* partials;
   unsigned int* counter;
   int tx, ty;
+  int ny;        // row length of u (domain columns)
+  int ew_grid;   // blocks of the vectorised element-wise passes
 };
 // Launch with programmatic stream serialization: the kernel may start while
 // its predecessor on the stream finishes, and calls pdl_wait before reading
 // anything an earlier kernel wrote.  Off when the environment sets CM_PDL=0.
 bool pdl_enabled();
 template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(bool chained, void (*kernel)(KArgs...), int grid, int block,
+                                  size_t smem, cudaStream_t s, Args... args);
+template <typename... KArgs, typename... Args>
 inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem,
                               cudaStream_t s, Args... args) {
+  return launch_chained(true, kernel, grid, block, smem, s, args...);
+}
+// launch_pdl when `chained` (a kernel of ours precedes it on the stream),
+// else a plain launch
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(bool chained, void (*kernel)(KArgs...), int grid, int block,
+                                  size_t smem, cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(block);
@@ -81,7 +93,7 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, siz
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cfg.numAttrs = chained && pdl_enabled() ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
@@ -101,4 +113,13 @@ int ccg_p2_row_inv(const CcgArgs<R>& a, int logy, cudaStream_t s);
 // may be inside a stream capture): 0, -1 unsupported, 1 CUDA error.
 template <typename R>
 int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy);
+// The vectorised element-wise passes of the single-solve path (gsum, force
+// update), chained behind the previous pass; grid a.ew_grid.
+template <typename R>
+int ccg_p2_gsum(const CcgArgs<R>& a, cudaStream_t s, bool chained);
+template <typename R>
+int ccg_p2_update(const CcgArgs<R>& a, cudaStream_t s, bool chained);
+// Resident blocks per SM of those passes (for sizing a.ew_grid), or -1.
+template <typename R>
+int ccg_p2_ew_blocks_per_sm();
 

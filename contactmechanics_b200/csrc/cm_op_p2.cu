@@ -1,6 +1,7 @@
 // Launcher of the power-of-two operator passes (cm_op_p2.cuh).  The first
 // pass of a sequence (k_op_row_fwd of the operator) launches plainly; every
 // later one with programmatic stream serialization (launch_pdl).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -231,6 +232,34 @@ int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy) {
   }
 }
 
+// loads of each field in flight per thread in the element-wise passes
+#define CM_EW_UNROLL 2
+
+template <typename R>
+int ccg_p2_gsum(const CcgArgs<R>& a, cudaStream_t s, bool chained) {
+  return launch_chained(chained, k_ew_gsum<R, CM_EW_UNROLL>, a.ew_grid, CM_EW_THREADS, 0, s, a) ==
+                 cudaSuccess
+             ? 0 : 1;
+}
+
+template <typename R>
+int ccg_p2_update(const CcgArgs<R>& a, cudaStream_t s, bool chained) {
+  return launch_chained(chained, k_ew_update<R, CM_EW_UNROLL>, a.ew_grid, CM_EW_THREADS, 0, s, a) ==
+                 cudaSuccess
+             ? 0 : 1;
+}
+
+template <typename R>
+int ccg_p2_ew_blocks_per_sm() {
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_ew_gsum<R, CM_EW_UNROLL>, CM_EW_THREADS, 0) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ew_update<R, CM_EW_UNROLL>, CM_EW_THREADS, 0) !=
+          cudaSuccess)
+    return -1;
+  return std::min(a, b);
+}
+
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw) {
   if (logx < 6 || logx > 12 || logy < 6 || logy > 12) return 0;
@@ -265,3 +294,9 @@ template int ccg_p2_row_inv<double, MODE_T>(const CcgArgs<double>&, int, cudaStr
 template int ccg_p2_row_inv<double, MODE_F>(const CcgArgs<double>&, int, cudaStream_t);
 template int ccg_p2_prepare<float>(const CcgArgs<float>&, int, int);
 template int ccg_p2_prepare<double>(const CcgArgs<double>&, int, int);
+template int ccg_p2_gsum<float>(const CcgArgs<float>&, cudaStream_t, bool);
+template int ccg_p2_gsum<double>(const CcgArgs<double>&, cudaStream_t, bool);
+template int ccg_p2_update<float>(const CcgArgs<float>&, cudaStream_t, bool);
+template int ccg_p2_update<double>(const CcgArgs<double>&, cudaStream_t, bool);
+template int ccg_p2_ew_blocks_per_sm<float>();
+template int ccg_p2_ew_blocks_per_sm<double>();

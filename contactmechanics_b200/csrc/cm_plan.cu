@@ -498,6 +498,7 @@ struct Work {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
   int nt_comp = 0, nt_rowt = 0, nt_rowd = 0, nt_col = 0;
+  int partial_blocks = 0;   // blocks whose reduction partials fit the partials buffer
 };
 
 struct cm_plan {
@@ -637,6 +638,7 @@ static int init_work(cm_plan* p, Work<R>& w) {
                                w.tiles.ntile_cols, 1});
   // (the by-value row passes use tiles of at least two rows: at most nx tiles)
   CKS(dalloc(p, &w.partials, (size_t)std::max(nt_max, p->nx) * CM_MAX_PARTIAL_VALS));
+  w.partial_blocks = std::max(nt_max, p->nx);
   CKS(dalloc(p, &w.counter, 1));
   CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), p->stream));
   CKS(dalloc(p, &w.st, 1));
@@ -696,6 +698,8 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
     a.counter = w.counter;
     a.tx = p->tx;
     a.ty = p->ty;
+    a.ny = p->ny;
+    a.ew_grid = 0;
     w.by_value = CM_BY_VALUE_PASSES && lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw);
     if (w.by_value) {
       const int rc = ccg_p2_prepare<R>(a, lx, ly);
@@ -723,6 +727,13 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
       w.ew_grid[4] = (coop && per_sm > 0 && !(e && e[0] == '0'))
                          ? std::max(1, std::min(w.nt_comp, per_sm * nsm)) : 0;
       if (w.ew_grid[4] && !w.bar) CKS(dalloc(p, &w.bar, 1));
+      // the vectorised element-wise passes (gsum, force update): one resident
+      // wave, no more blocks than vectors to walk or reduction partials
+      const int ew_per_sm = ccg_p2_ew_blocks_per_sm<R>();
+      if (ew_per_sm < 1) return CM_ERR_CUDA;
+      const long nvec = (long)p->tx * p->ty / (16 / (long)sizeof(R));
+      const long need = (nvec + 2L * 256 - 1) / (2L * 256);
+      a.ew_grid = (int)std::max(1L, std::min({(long)ew_per_sm * nsm, need, (long)w.partial_blocks}));
     }
   }
   w.ccg_ready = true;
@@ -865,7 +876,12 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     for (int i = 0; i < CM_BISECT_PASSES; ++i) elementwise(k_ccg_bisect<R>, 3);
   }
   mark();
-  elementwise(k_ccg_gsum<R>, 1);
+  if (w.by_value) {
+    ccg_p2_gsum<R>(w.ccg_args, s, chain);
+    chain = true;
+  } else {
+    elementwise(k_ccg_gsum<R>, 1);
+  }
   mark();
   const bool p2 = T.p2;
   const int ly = p->fy.n, lx = p->fx.n;
@@ -883,7 +899,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     mark();
     ccg_p2_row_inv<R, MODE_T>(a, ry, s);
     mark();
-    elementwise(k_ccg_update<R>, 2);
+    ccg_p2_update<R>(a, s, true);
     mark();
     ccg_p2_row_fwd<R, MODE_F>(a, ry, s);
     mark();
