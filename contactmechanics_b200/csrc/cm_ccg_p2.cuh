@@ -1,7 +1,8 @@
 // Row passes of one CCG iteration for a single solve on a power-of-two
 // domain, in the shape of the operator passes of cm_op_p2.cuh: arguments by
-// value, blocks of 2*NP rows walking their tiles with a grid stride,
-// spectrum stores and gathers in whole (row, column-in-tile) runs.  The
+// value, blocks of 2*NP rows walking their tiles with a grid stride, the
+// pair-major spectrum stored and loaded straight from the transform
+// registers (the column pass splits and packs the row pairs).  The
 // solver's element-wise work rides on the transforms as in the per-pass
 // kernels of cm_kernels_p2.cuh (same formulas):
 //
@@ -16,7 +17,7 @@
 //                          k_ccg_begin, :239-270, 300-318), so an iteration
 //                          after the first launches no k_ccg_begin.
 //
-// The column pass between them is k_op_col16 with the solve's state attached.
+// The column pass between them is k_op_col with the solve's state attached.
 // Each block accumulates its tiles' reductions and writes one partial; the
 // last block to finish runs the scalar step (tile_finish).
 #pragma once
@@ -50,7 +51,6 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, ny = N;
   unsigned mphase = 0;
-  const int lw = a.op.lw, W = 1 << lw, nkb = (a.op.nyh + W - 1) >> lw;
   const int ntiles = (tx + ROWS - 1) / ROWS;
   R* __restrict__ fio = a.f[MODE == MODE_T ? cv.par : (cv.par ^ 1)];
   const R* __restrict__ u_in = a.u;
@@ -183,26 +183,12 @@ k_ccg_row_fwd(CcgArgs<R> a) {
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
     fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
-    __syncthreads();
+    if (xa < tx) {
+      C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N + tt;
 #pragma unroll
-    for (int q = 0; q < Sh::E; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
-    __syncthreads();
-    // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
-    const int total = nkb * ROWS * W;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int kw = e & (W - 1);
-      const int r = (e >> lw) & (ROWS - 1);
-      const int kb = e >> (lw + Sh::LNP + 1);
-      const int k = kb * W + kw, x = x0 + r;
-      if (k >= a.op.nyh || x >= tx) continue;
-      const int p = r >> 1;
-      const C z = bufA[spad(p * N + k)];
-      const C zm = bufA[spad(p * N + ((N - k) & (N - 1)))];
-      const C val = (r & 1) ? cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5)
-                            : cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
-      a.op.spec[((size_t)kb * a.op.nx + x) * W + kw] = val;
+      for (int q = 0; q < Sh::E; ++q) srow[q * P::TPS] = v[q];
     }
-    __syncthreads();  // bufA free for the next tile
+    __syncthreads();  // buffers free for the next tile
   }
   if (MODE == MODE_T) {
     double vr[1] = {acc};
@@ -257,14 +243,15 @@ k_ccg_row_inv(CcgArgs<R> a) {
   const R* __restrict__ fn_buf = a.f[cv.par ^ 1];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS;
-    gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.op.spec, nx, a.op.nyh, a.op.lw, x0,
-                                                      rows_total);
-    __syncthreads();
-    C v[Sh::E];
-#pragma unroll
-    for (int q = 0; q < Sh::E; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
-    fft_p2r<C, true, LOGN, Sh::LR>(v, bufB, bufA, s * N, 1, tt, tws);
     const int xa = x0 + 2 * s;
+    C v[Sh::E];
+    {
+      const C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N + tt;
+      const bool have = xa < rows_total;
+#pragma unroll
+      for (int q = 0; q < Sh::E; ++q) v[q] = have ? srow[q * P::TPS] : czero<C>();
+    }
+    fft_p2r<C, true, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
     if (MODE == MODE_T) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) {

@@ -41,7 +41,8 @@ struct OpArgs {
   R* out;
   int in_rows, in_cols, in_ld;
   int out_rows, out_cols, out_ld;
-  int nx, nyh, lw;  // domain rows, half-spectrum columns, log2 of the column-tile width
+  int nx, nyh, lw;  // domain rows, half-spectrum columns, log2 of the table's column tiles
+  int ny;           // domain columns (row length of the pair-major spectrum)
   int ntile_cols;
   C* spec;
   const R* tab;     // the selected Green's table, tiled like the spectrum

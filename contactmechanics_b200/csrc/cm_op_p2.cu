@@ -69,11 +69,12 @@ int row_fwd(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
   return 0;
 }
 
-template <typename R, int LOGN, typename K>
-int prepare16(K kernel, KernelInfo& info) {
-  typedef OpShape16<R, LOGN> Sh;
+template <typename R, int LOGX, typename K>
+int prepare_col(K kernel, KernelInfo& info) {
+  typedef ColShape<R, LOGX> Sh;
   if (info.ready) return info.grid_per_sm > 0 ? 0 : -1;
   const size_t smem = Sh::smem();
+  if (smem > CM_SMEM_DYN_MAX) return -1;
   if (cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return 1;
@@ -85,22 +86,23 @@ int prepare16(K kernel, KernelInfo& info) {
   return per_sm > 0 ? 0 : -1;
 }
 
-// column pass: 16 elements per thread (k_op_col16)
-template <typename R, int LOGN>
+// column pass on the pair-major spectrum (k_op_col); LOGX: log2 of the
+// column length (domain rows)
+template <typename R, int LOGX>
 int col(const OpArgs<R>& a, cudaStream_t s, bool launch = true) {
-  typedef OpShape16<R, LOGN> Sh;
+  typedef ColShape<R, LOGX> Sh;
   static KernelInfo info;
-  if (((1 << a.lw) * Sh::TPS) > Sh::THREADS) return -1;
   int rc;
   {
     std::lock_guard<std::mutex> g(g_op_mu);
-    rc = prepare16<R, LOGN>(k_op_col16<R, LOGN>, info);
+    rc = prepare_col<R, LOGX>(k_op_col<R, LOGX>, info);
   }
   if (rc || !launch) return rc;
-  const int per_block = Sh::THREADS / ((1 << a.lw) * Sh::TPS);
-  const int groups = (a.ntile_cols + per_block - 1) / per_block;
-  const int grid = std::max(1, std::min(groups, info.grid_per_sm * sm_count()));
-  launch_pdl(k_op_col16<R, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);
+  const int units = a.ny / 2 + 1;
+  const int groups = (units + Sh::W - 1) / Sh::W;
+  const int blocks = (groups + Sh::NG - 1) / Sh::NG;
+  const int grid = std::max(1, std::min(blocks, info.grid_per_sm * sm_count()));
+  launch_pdl(k_op_col<R, LOGX>, grid, Sh::THREADS, Sh::smem(), s, a);
   return 0;
 }
 
@@ -262,10 +264,8 @@ int ccg_p2_ew_blocks_per_sm() {
 
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw) {
-  if (logx < 6 || logx > 12 || logy < 6 || logy > 12) return 0;
-  const int tps = 1 << (logx - 3);
-  const int threads = std::max(tps, sizeof(R) == 8 ? 256 : 512);
-  return ((1 << lw) * tps) <= threads;
+  (void)lw;  // the column pass reads the tables in any column tiling
+  return logx >= 6 && logx <= 12 && logy >= 6 && logy <= 12;
 }
 
 template <typename R>

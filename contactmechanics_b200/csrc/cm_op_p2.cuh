@@ -1,25 +1,37 @@
 // The elastic operator u = IFFT(T . FFT(f)) (FFTElasticHalfSpace.py:573-611,
 // free :1141-1197) for power-of-two domains (sides 64..4096), as three
-// bandwidth-oriented passes over caller buffers:
+// passes over caller buffers:
 //
-//   k_op_row_fwd  rows x < in_rows: packed real-to-complex row transforms
-//                 (two rows per complex transform), half spectrum written
-//                 into the plan's column-tiled spectrum;
-//   k_op_col16    every column tile: forward transform along x (input rows
-//                 >= in_rows are zero), times the real Green's table,
-//                 inverse transform, rows < out_rows written back;
-//   k_op_row_inv  rows x < out_rows: complex-to-real row transforms, output
-//                 columns < out_cols written to the caller's buffer.
+//   k_op_row_fwd  row pairs (2p, 2p+1) with rows < in_rows: one complex
+//                 transform of z = f[2p] + i f[2p+1] per pair, stored as it
+//                 comes out of the registers: Z_p(k), k = 0..ny-1, at
+//                 spec[p * ny + k] (the pair-major spectrum);
+//   k_op_col      every column k = 0..ny/2 of the half spectrum: the column
+//                 X_x(k) of row x = 2p + b is split off the pair transforms
+//                 in registers (X_2p(k) = (Z_p(k) + conj Z_p(ny-k)) / 2,
+//                 X_2p+1(k) = (Z_p(k) - conj Z_p(ny-k)) / 2i; rows >= in_rows
+//                 are zero), transformed along x, multiplied by the real
+//                 Green's table, transformed back, and packed again for the
+//                 inverse row transforms: W_p(k) = Xh_2p(k) + i Xh_2p+1(k) and
+//                 W_p(ny-k) = conj Xh_2p(k) + i conj Xh_2p+1(k), pairs with rows
+//                 < out_rows written back in place;
+//   k_op_row_inv  row pairs with rows < out_rows: one inverse complex
+//                 transform of W_p per pair straight from the spectrum; the
+//                 real part is row 2p, the imaginary part row 2p+1.
+//
+// The row passes thus read and write the spectrum in whole rows from the
+// transform registers, with no shared-memory split or pack pass; the split
+// and the pack are arithmetic in the column pass, whose two rows of a pair
+// sit in neighbouring threads (a shuffle exchanges them).  A column group
+// covers W consecutive columns (W = 32 bytes of complex values, so every
+// spectrum access of a warp fills whole 32-byte sectors; fewer when the
+// shared memory of a long column does not allow it).
 //
 // Arguments travel by value (no descriptor upload), so a call is a plain
 // sequence of three launches on the caller's stream.  Blocks walk their
-// tiles with a grid stride, so the twiddle tables are staged once per block.
-// A block covers 2*NP rows (row passes, N/E threads per transform with E =
-// 8 elements per thread by default) or several column tiles (column pass,
-// N/16 threads per transform), the register-resident engines of
-// cm_fft_p2.cuh.  Spectrum stores and gathers are ordered so that a warp
-// touches whole rows-of-a-tile runs: (row, column-in-tile) fastest, which in
-// the plan's layout ((k >> lw) * nx + x) * W + (k & (W-1)) are contiguous.
+// tiles with a grid stride, so the twiddle tables are staged once per block;
+// the transforms are the register-resident engines of cm_fft_p2.cuh (row
+// passes 2^LR elements per thread, column pass 16).
 #pragma once
 #include "cm_fft_p2.cuh"
 #include "cm_kernels.cuh"
@@ -31,12 +43,6 @@
 #define CM_FP64_ROW_MINB 2
 #endif
 
-// threads of an FP64 column-pass block (at least one transform): 128, so
-// that two blocks fit an SM's shared memory at length 2048
-#ifndef CM_COL16_FP64_BASE
-#define CM_COL16_FP64_BASE 128
-#endif
-
 // threads of an FP32 row-pass block (at least one transform) and the
 // resident blocks per SM it is compiled for
 #ifndef CM_ROW_F32_BASE
@@ -46,18 +52,24 @@
 #define CM_ROW_F32_MINB 2
 #endif
 
-// threads of an FP32 column-pass block and its resident blocks per SM
-#ifndef CM_COL16_F32_BASE
-#define CM_COL16_F32_BASE 256
+// threads of a column-pass block when a column group is smaller
+#ifndef CM_COL_BASE
+#define CM_COL_BASE 256
 #endif
-#ifndef CM_COL16_F32_MINB
-#define CM_COL16_F32_MINB 2
+
+// log2 of the columns of a column group (at most; fewer when its shared
+// memory does not fit): 32 bytes of complex values
+#ifndef CM_COL_LW_F32
+#define CM_COL_LW_F32 2
+#endif
+#ifndef CM_COL_LW_F64
+#define CM_COL_LW_F64 1
 #endif
 
 // log2 of the elements per thread of the row passes' transforms (3: the
 // radix-8 engine, 4: the radix-16 one)
 #ifndef CM_ROW_LR_F32
-#define CM_ROW_LR_F32 3
+#define CM_ROW_LR_F32 4
 #endif
 #ifndef CM_ROW_LR_F64
 #define CM_ROW_LR_F64 3
@@ -72,64 +84,34 @@ struct OpShape {
   static constexpr int TPS = N >> LR;
   static constexpr int BASE = (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
-  static constexpr int NP = THREADS / TPS;  // sequences (row pairs, columns) per block
+  static constexpr int NP = THREADS / TPS;  // row pairs per block
   static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : CM_ROW_F32_MINB;
-  // block strides of a row-pair gather whose loads are issued together (the
-  // gather of a row tile with column tiles W <= N/8 takes at most five); the
-  // FP64 passes have the registers to spare, the FP32 ones do not
-  static constexpr int GATHER = sizeof(R) == 8 ? 5 : 1;
-  static constexpr int LNP = NP >= 512 ? 9 : NP >= 256 ? 8 : NP >= 128 ? 7 : NP >= 64 ? 6 : NP >= 32 ? 5
-                             : NP >= 16 ? 4 : NP >= 8 ? 3 : NP >= 4 ? 2 : NP >= 2 ? 1 : 0;
   static size_t smem() {
     return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
   }
 };
 
-// Gathers the half spectra of the row pairs x0 + 2p, x0 + 2p + 1 (p < NP,
-// rows >= rows_total read as zero) from the column-tiled spectrum and packs
-// each pair into one full-length complex sequence in buf (Z = X + iY with the
-// Hermitian halves filled in).  Element e = ((kb * NP) + p) * W + kw; the
-// loads of U consecutive strides are issued before any of them is used, so a
-// thread has 2U loads in flight.
-template <typename C, int LOGN, int NP, int LNP, int U>
-CM_DEVINL void gather_row_pairs(C* buf, const C* __restrict__ spec, int nx, int nyh, int lw,
-                                int x0, int rows_total) {
-  constexpr int N = 1 << LOGN;
-  const int W = 1 << lw, nkb = (nyh + W - 1) >> lw;
-  const int total = nkb * NP * W;
-  const int T = blockDim.x;
-  for (int e0 = threadIdx.x; e0 < total; e0 += U * T) {
-    C X[U], Y[U];
-#pragma unroll
-    for (int i = 0; i < U; ++i) {
-      const int e = e0 + i * T;
-      const int kw = e & (W - 1);
-      const int p = (e >> lw) & (NP - 1);
-      const int kb = e >> (lw + LNP);
-      const int k = kb * W + kw, xa = x0 + 2 * p;
-      X[i] = czero<C>();
-      Y[i] = czero<C>();
-      if (e >= total || k >= nyh || xa >= rows_total) continue;
-      const size_t ia = ((size_t)kb * nx + xa) * W + kw;
-      X[i] = spec[ia];
-      if (xa + 1 < rows_total) Y[i] = spec[ia + W];
-    }
-#pragma unroll
-    for (int i = 0; i < U; ++i) {
-      const int e = e0 + i * T;
-      const int kw = e & (W - 1);
-      const int p = (e >> lw) & (NP - 1);
-      const int kb = e >> (lw + LNP);
-      const int k = kb * W + kw, xa = x0 + 2 * p;
-      if (e >= total || k >= nyh || xa >= rows_total) continue;
-      C x = X[i], y = Y[i];
-      const bool selfconj = (k == 0) || (2 * k == N);
-      if (selfconj) { x.y = 0; y.y = 0; }
-      buf[spad(p * N + k)] = cmake<C>(x.x - y.y, x.y + y.x);
-      if (!selfconj) buf[spad(p * N + N - k)] = cmake<C>(x.x + y.y, y.x - x.y);
-    }
+// Column pass for columns of length 2^LOGX: 16 elements per thread, groups of
+// W = 2^LW columns with the column index fastest across threads.
+template <typename R, int LOGX>
+struct ColShape {
+  typedef typename CT<R>::C C;
+  static constexpr int NX = 1 << LOGX;
+  static constexpr int TPS = NX / 16;
+  static constexpr size_t smem_for(int lw) {
+    return (size_t)(NX + 2 * (((NX << lw)) + ((NX << lw) >> 3) + 1)) * sizeof(C);
   }
-}
+  // 32 bytes of complex values per column group, fewer if the group's
+  // ping-pong buffers do not fit
+  static constexpr int LW_PREF = sizeof(C) == 8 ? CM_COL_LW_F32 : CM_COL_LW_F64;
+  static constexpr int LW = smem_for(LW_PREF) <= CM_SMEM_DYN_MAX ? LW_PREF
+                            : smem_for(LW_PREF - 1) <= CM_SMEM_DYN_MAX ? LW_PREF - 1 : 0;
+  static constexpr int W = 1 << LW;
+  static constexpr int GROUP = W * TPS;
+  static constexpr int THREADS = GROUP > CM_COL_BASE ? GROUP : CM_COL_BASE;
+  static constexpr int NG = THREADS / GROUP;  // column groups per block
+  static size_t smem() { return (size_t)(NX + 2 * smem_padded(NG * NX * W)) * sizeof(C); }
+};
 
 template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
@@ -137,7 +119,7 @@ k_op_row_fwd(OpArgs<R> a) {
   typedef typename CT<R>::C C;
   typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
-  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
@@ -147,10 +129,9 @@ k_op_row_fwd(OpArgs<R> a) {
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
-  const int W = 1 << a.lw, nkb = (a.nyh + W - 1) >> a.lw;
-  const int ntiles = (a.in_rows + ROWS - 1) / ROWS;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int x0 = tile * ROWS, xa = x0 + 2 * s;
+  const int npairs = (a.in_rows + 1) >> 1;
+  for (int p0 = blockIdx.x * NP; p0 < npairs; p0 += gridDim.x * NP) {
+    const int p = p0 + s, xa = 2 * p;
     C v[Sh::E];
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) {
@@ -163,95 +144,114 @@ k_op_row_fwd(OpArgs<R> a) {
       v[q] = cmake<C>(ra, rb);
     }
     fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
-    __syncthreads();
+    if (p < npairs) {
+      C* __restrict__ row = a.spec + (size_t)p * N + tt;
 #pragma unroll
-    for (int q = 0; q < Sh::E; ++q) bufA[spad(s * N + tt + q * P::TPS)] = v[q];
-    __syncthreads();
-    // split the packed transforms; e = ((kb * ROWS) + r) * W + kw
-    const int total = nkb * ROWS * W;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int kw = e & (W - 1);
-      const int r = (e >> a.lw) & (ROWS - 1);
-      const int kb = e >> (a.lw + Sh::LNP + 1);
-      const int k = kb * W + kw, x = x0 + r;
-      if (k >= a.nyh || x >= a.in_rows) continue;
-      const int p = r >> 1;
-      const C z = bufA[spad(p * N + k)];
-      const C zm = bufA[spad(p * N + ((N - k) & (N - 1)))];
-      const C val = (r & 1) ? cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5)
-                            : cmake<C>((z.x + zm.x) * (R)0.5, (z.y - zm.y) * (R)0.5);
-      a.spec[((size_t)kb * a.nx + x) * W + kw] = val;
+      for (int q = 0; q < Sh::E; ++q) row[q * P::TPS] = v[q];
     }
-    __syncthreads();  // bufA free for the next tile
+    __syncthreads();  // buffers free for the next pairs
   }
 }
 
-// Column pass with 16 elements per thread (radix-16 stages, fft_p2r): two
-// shared-memory exchanges per transform of length 2048 instead of the three
-// of the 8-element engine.
-template <typename R, int LOGN>
-struct OpShape16 {
-  static constexpr int N = 1 << LOGN;
-  static constexpr int TPS = N / 16;
-  static constexpr int BASE = sizeof(R) == 8 ? CM_COL16_FP64_BASE : CM_COL16_F32_BASE;
-  static constexpr int THREADS = TPS > BASE ? TPS : BASE;
-  static constexpr int NP = THREADS / TPS;  // columns per block
-  static constexpr int MINB = sizeof(R) == 4 ? CM_COL16_F32_MINB : (BASE < 256 ? 2 : 1);
-  static size_t smem() {
-    return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
+// Loads of one column unit k of the pair-major spectrum (rows x = 2p + b of
+// the thread's elements x = tt + q TPS, b = tt & 1): both rows of a pair load
+// Z_p(k) and Z_p(ny - k) (neighbouring lanes, one request) and each splits
+// off its own row.  Rows >= in_rows are zero.
+template <typename C, int TPS>
+CM_DEVINL void col_split_load(C (&v)[16], const C* __restrict__ spec, int ny, int k, int km, int tt,
+                              int in_rows, bool ok) {
+  typedef decltype(v[0].x) R;
+  const int b = tt & 1;
+  const C* __restrict__ sk = spec + k + (size_t)(tt >> 1) * ny;
+  const C* __restrict__ skm = spec + km + (size_t)(tt >> 1) * ny;
+  const int pstep = (TPS / 2) * ny;
+#pragma unroll
+  for (int h = 0; h < 16; h += 8) {
+    C z[8], zm[8];
+#pragma unroll
+    for (int q = h; q < h + 8; ++q) {
+      const int x = tt + q * TPS;
+      z[q - h] = czero<C>();
+      zm[q - h] = czero<C>();
+      if (ok && x < in_rows) {
+        z[q - h] = sk[(size_t)q * pstep];
+        zm[q - h] = skm[(size_t)q * pstep];
+      }
+    }
+#pragma unroll
+    for (int q = h; q < h + 8; ++q) {
+      const C zk = z[q - h], zn = zm[q - h];
+      v[q] = b ? cmake<C>((zk.y + zn.y) * (R)0.5, (zn.x - zk.x) * (R)0.5)
+               : cmake<C>((zk.x + zn.x) * (R)0.5, (zk.y - zn.y) * (R)0.5);
+    }
   }
-};
+}
 
-template <typename R, int LOGN>
-__global__ void __launch_bounds__(OpShape16<R, LOGN>::THREADS, OpShape16<R, LOGN>::MINB)
-k_op_col16(OpArgs<R> a) {
+// Pack the filtered column back into the pair-major spectrum: the even row of
+// a pair writes W_p(k) = Xh_2p + i Xh_2p+1 (real parts only for the
+// self-conjugate columns 0 and ny/2), the odd row W_p(ny - k); pairs with
+// rows < out_rows.
+template <typename C, int TPS, int W>
+CM_DEVINL void col_pack_store(const C (&v)[16], C* __restrict__ spec, int ny, int k, int km, int tt,
+                              int out_rows, bool ok) {
+  const int b = tt & 1;
+  const int pairs_out = (out_rows + 1) >> 1;
+  const bool selfc = (k == 0) || (2 * k == ny);
+  const bool writes = ok && !(b && selfc);
+  C* __restrict__ dst = spec + (b ? km : k) + (size_t)(tt >> 1) * ny;
+  const int pstep = (TPS / 2) * ny;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const C a = v[q];
+    C o;
+    o.x = __shfl_xor_sync(0xffffffffu, a.x, W);
+    o.y = __shfl_xor_sync(0xffffffffu, a.y, W);
+    const int pp = (tt >> 1) + q * (TPS / 2);
+    if (!writes || pp >= pairs_out) continue;
+    dst[(size_t)q * pstep] = !b ? (selfc ? cmake<C>(a.x, o.x) : cmake<C>(a.x - o.y, a.y + o.x))
+                                : cmake<C>(o.x + a.y, a.x - o.y);
+  }
+}
+
+template <typename R, int LOGX>
+__global__ void __launch_bounds__(ColShape<R, LOGX>::THREADS, 1)
+k_op_col(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGN, 4> P;
-  typedef OpShape16<R, LOGN> Sh;
-  constexpr int N = P::N;
+  typedef P2PlanR<LOGX, 4> P;
+  typedef ColShape<R, LOGX> Sh;
+  constexpr int NX = P::N, W = Sh::W, LW = Sh::LW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
-  C* bufB = bufA + smem_padded(Sh::NP * N);
+  C* bufA = tws + NX;
+  C* bufB = bufA + smem_padded(Sh::NG * NX * W);
   pdl_trigger();
-  stage_tw_p2r<LOGN, 4>(tws, a.twx);
+  stage_tw_p2r<LOGX, 4>(tws, a.twx);
   pdl_wait();
   if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   __syncthreads();
-  const int lw = a.lw, W = 1 << lw;
+  const int ny = a.ny;
   const int c = threadIdx.x & (W - 1);
-  const int tt = (threadIdx.x >> lw) & (P::TPS - 1);
-  const int j = threadIdx.x >> (lw + P::LTPS);
-  const int tiles_per_block = blockDim.x >> (lw + P::LTPS);
-  const int ngroups = (a.ntile_cols + tiles_per_block - 1) / tiles_per_block;
-  const int base = j * N * W + c;
-  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int tile = grp * tiles_per_block + j;
-    const bool tile_ok = tile < a.ntile_cols;
-    const int wc = tile_ok ? min(W, a.nyh - tile * W) : 0;
-    const bool col_ok = c < wc;
-    C* __restrict__ blk = a.spec + (size_t)tile * N * W;
-    const R* __restrict__ tblk = a.tab + (size_t)tile * N * W;
+  const int tt = (threadIdx.x >> LW) & (P::TPS - 1);
+  const int j = threadIdx.x >> (LW + P::LTPS);
+  const int units = ny / 2 + 1;
+  const int ngroups = (units + W - 1) >> LW;
+  const int base = j * NX * W + c;
+  const int tlw = a.lw, tW = 1 << tlw;  // the table's column tiles
+  for (int g0 = blockIdx.x * Sh::NG; g0 < ngroups; g0 += gridDim.x * Sh::NG) {
+    const int k = (g0 + j) * W + c;
+    const bool ok = k < units;
+    const int km = (ny - k) & (ny - 1);
     C v[16];
-    R g[16];
+    col_split_load<C, P::TPS>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
+    fft_p2r<C, false, LOGX, 4>(v, bufA, bufB, base, W, tt, tws);
+    const R* __restrict__ tb =
+        a.tab + ((size_t)(k >> tlw) * NX << tlw) + (k & (tW - 1)) + ((size_t)tt << tlw);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int x = tt + q * P::TPS;
-      v[q] = (col_ok && x < a.in_rows) ? blk[x * W + c] : czero<C>();
-      g[q] = col_ok ? __ldg(tblk + x * W + c) : (R)0;
-    }
-    fft_p2r<C, false, LOGN, 4>(v, bufA, bufB, base, W, tt, tws);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = cscale(v[q], g[q]);
+    for (int q = 0; q < 16; ++q)
+      v[q] = cscale(v[q], ok ? __ldg(tb + ((size_t)(q * P::TPS) << tlw)) : (R)0);
     __syncthreads();
-    fft_p2r<C, true, LOGN, 4>(v, bufA, bufB, base, W, tt, tws);
-    if (col_ok) {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int x = tt + q * P::TPS;
-        if (x < a.out_rows) blk[x * W + c] = v[q];
-      }
-    }
+    fft_p2r<C, true, LOGX, 4>(v, bufA, bufB, base, W, tt, tws);
+    col_pack_store<C, P::TPS, W>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
     __syncthreads();  // buffers free for the next group
   }
 }
@@ -262,7 +262,7 @@ k_op_row_inv(OpArgs<R> a) {
   typedef typename CT<R>::C C;
   typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
-  constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
+  constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + N;
@@ -272,16 +272,14 @@ k_op_row_inv(OpArgs<R> a) {
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
-  const int ntiles = (a.out_rows + ROWS - 1) / ROWS;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int x0 = tile * ROWS;
-    gather_row_pairs<C, LOGN, NP, Sh::LNP, Sh::GATHER>(bufA, a.spec, a.nx, a.nyh, a.lw, x0, a.out_rows);
-    __syncthreads();
+  const int npairs = (a.out_rows + 1) >> 1;
+  for (int p0 = blockIdx.x * NP; p0 < npairs; p0 += gridDim.x * NP) {
+    const int p = p0 + s, xa = 2 * p;
     C v[Sh::E];
+    const C* __restrict__ row = a.spec + (size_t)p * N + tt;
 #pragma unroll
-    for (int q = 0; q < Sh::E; ++q) v[q] = bufA[spad(s * N + tt + q * P::TPS)];
-    fft_p2r<C, true, LOGN, Sh::LR>(v, bufB, bufA, s * N, 1, tt, tws);
-    const int xa = x0 + 2 * s;
+    for (int q = 0; q < Sh::E; ++q) v[q] = p < npairs ? row[q * P::TPS] : czero<C>();
+    fft_p2r<C, true, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;
@@ -289,6 +287,6 @@ k_op_row_inv(OpArgs<R> a) {
       if (xa < a.out_rows) a.out[(size_t)xa * a.out_ld + y] = v[q].x;
       if (xa + 1 < a.out_rows) a.out[(size_t)(xa + 1) * a.out_ld + y] = v[q].y;
     }
-    __syncthreads();  // buffers free for the next tile
+    __syncthreads();  // buffers free for the next pairs
   }
 }

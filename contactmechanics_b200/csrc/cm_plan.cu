@@ -680,6 +680,7 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
     a.op.nx = p->nx;
     a.op.nyh = p->nyh;
     a.op.lw = w.tiles.lw;
+    a.op.ny = p->ny;
     a.op.ntile_cols = w.tiles.ntile_cols;
     a.op.spec = w.spec;
     a.op.tab = w.tab[0];
@@ -771,6 +772,7 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
       a.nx = p->nx;
       a.nyh = p->nyh;
       a.lw = w.tiles.lw;
+      a.ny = p->ny;
       a.ntile_cols = w.tiles.ntile_cols;
       a.spec = w.spec;
       a.tab = w.tab[table_sel];
