@@ -291,13 +291,17 @@ class FreeFFTElasticHalfSpace(PeriodicFFTElasticHalfSpace):
                  communicator=None, check_boundaries=False, fftengine=None, precision="fp64"):
         if not hasattr(nb_grid_pts, "__iter__"):
             nb_grid_pts = (nb_grid_pts,)
-        self._comp_nb_grid_pts = tuple(2 * int(r) for r in nb_grid_pts)
+        self._comp_nb_grid_pts = self._domain_of(tuple(int(r) for r in nb_grid_pts))
         super().__init__(nb_grid_pts, young, physical_sizes, superclass=False, fft=fft,
                          communicator=communicator, fftengine=fftengine, precision=precision)
         if self.dim != 2:
             raise self.Error("FreeFFTElasticHalfSpace is implemented for 2D only")
         self._plan = _Plan(self._plan_desc())
         self._check_boundaries = check_boundaries
+
+    def _domain_of(self, nb_grid_pts):
+        """Computational grid: doubled along every axis (:950-951)."""
+        return tuple(2 * n for n in nb_grid_pts)
 
     def _plan_desc(self):
         d = super()._plan_desc()
@@ -376,3 +380,76 @@ class FreeFFTElasticHalfSpace(PeriodicFFTElasticHalfSpace):
     def check(self, force=None):
         if self._check_boundaries:
             self.check_boundaries(force)
+
+
+class SemiPeriodicFFTElasticHalfSpace(FreeFFTElasticHalfSpace):
+    """Half-space that is periodic along some axes and free along the others
+    (FFTElasticHalfSpace.py:1286-1615).  A periodic axis keeps its n points
+    and the Love kernel is summed over its periodic images
+    -n_images..n_images; a free axis is padded to 2n - 1 points.  The kernel
+    and its table are built by the library (extended-precision sum of the
+    images on the host, FP64 transform on the device); evaluate_disp pads
+    like FreeFFTElasticHalfSpace, evaluate_force zero-pads displacements that
+    do not cover the domain."""
+
+    name = "semi_periodic_fft_elastic_halfspace"
+
+    def __init__(self, nb_grid_pts, young, physical_sizes=(2 * np.pi, 2 * np.pi),
+                 periodicity=(False, True), n_images=10, fft="serial", communicator=None,
+                 check_boundaries=False, fftengine=None, precision="fp64"):
+        self.periodicity = tuple(bool(p) for p in periodicity)
+        self.n_images = int(n_images)
+        self._G_real = None
+        super().__init__(nb_grid_pts, young, physical_sizes, fft=fft, communicator=communicator,
+                         check_boundaries=check_boundaries, fftengine=fftengine,
+                         precision=precision)
+
+    def _domain_of(self, nb_grid_pts):
+        """n points along a periodic axis, 2n - 1 along a free one (:1343-1353)."""
+        return tuple(n if per else 2 * n - 1 for n, per in zip(nb_grid_pts, self.periodicity))
+
+    def _plan_desc(self):
+        d = super()._plan_desc()
+        d.kind = _lib.CM_SEMI
+        d.periodic_x = int(self.periodicity[0])
+        d.periodic_y = int(self.periodicity[1])
+        d.n_images = self.n_images
+        return d
+
+    def spawn_child(self, nb_grid_pts):
+        size = tuple(nb_grid_pts[i] / float(self.nb_grid_pts[i]) * self.physical_sizes[i]
+                     for i in range(self.dim))
+        return type(self)(nb_grid_pts, self.young, size, periodicity=self.periodicity,
+                          n_images=self.n_images)
+
+    def evaluate_force(self, disp):
+        """Forces due to displacements (:1541-1565); displacements that do not
+        cover the domain are zero padded."""
+        shape = self._shape(disp)
+        nxd, nyd = self.nb_domain_grid_pts
+        if shape == (nxd, nyd):
+            return super().evaluate_force(disp)
+        if len(shape) != 2 or shape[0] > nxd or shape[1] > nyd:
+            raise self.Error("displacements array has a different shape ({0}) than this "
+                             "halfspace's domain ({1})".format(shape, (nxd, nyd)))
+        return self._apply(_lib.CM_OP_FORCE, disp, (nxd, nyd), shape[0], shape[1], nxd, nyd)
+
+    @property
+    def G_real(self):
+        """Real-space kernel of the domain (sum over the periodic images)."""
+        if self._G_real is None:
+            nxd, nyd = self.nb_domain_grid_pts
+            self._G_real = np.fft.irfftn(self.greens_function, s=(nyd, nxd), axes=(1, 0))
+        return self._G_real
+
+    def get_G_real(self):
+        """The real-space kernel with the zero offset at the array centre (:1567-1596)."""
+        nxd, nyd = self.nb_domain_grid_pts
+        mx = np.round(np.fft.fftfreq(nxd) * nxd).astype(int)
+        my = np.round(np.fft.fftfreq(nyd) * nyd).astype(int)
+        return self.G_real[np.ix_(np.argsort(mx), np.argsort(my))]
+
+    def get_G_real_slices(self):
+        """Middle slices of get_G_real() along x and along y (:1598-1615)."""
+        g = self.get_G_real()
+        return g[:, g.shape[1] // 2], g[g.shape[0] // 2, :]

@@ -7,7 +7,8 @@ reference's Substrates / Systems / Optimization call signatures.
 """
 from .Substrates import ElasticSubstrate, PlasticSubstrate, Substrate  # noqa: F401
 from .FFTElasticHalfSpace import (FreeFFTElasticHalfSpace,  # noqa: F401
-                                  PeriodicFFTElasticHalfSpace)
+                                  PeriodicFFTElasticHalfSpace,
+                                  SemiPeriodicFFTElasticHalfSpace)
 from .Optimization import (constrained_conjugate_gradients,  # noqa: F401
                            constrained_conjugate_gradients_batch)
 from .Systems import NonSmoothContactSystem  # noqa: F401

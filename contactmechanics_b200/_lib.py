@@ -24,6 +24,7 @@ CM_ERR_TIMEOUT = 9
 
 CM_PERIODIC = 0
 CM_FREE = 1
+CM_SEMI = 2
 CM_FP64 = 0
 CM_FP32 = 1
 CM_MIXED = 2
@@ -45,7 +46,8 @@ class PlanDesc(ctypes.Structure):
                 ("sx", ctypes.c_double), ("sy", ctypes.c_double),
                 ("young", ctypes.c_double), ("poisson", ctypes.c_double),
                 ("q0_mode", ctypes.c_int), ("stiffness_q0", ctypes.c_double),
-                ("thickness", ctypes.c_double)]
+                ("thickness", ctypes.c_double), ("periodic_x", ctypes.c_int),
+                ("periodic_y", ctypes.c_int), ("n_images", ctypes.c_int)]
 
 
 class CcgParams(ctypes.Structure):

@@ -203,12 +203,19 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   }
 }
 
+// shape of the inverse row passes: the displacement pass (MODE_F) of FP32
+// solves has its own elements per thread
 template <typename R, int MODE, int LOGN>
-__global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
+using InvShape = OpShape<R, LOGN,
+                         (MODE == MODE_F && sizeof(R) == 4) ? CM_ROW_LR_INVF_F32
+                                                            : OpShape<R, LOGN>::LR>;
+
+template <typename R, int MODE, int LOGN>
+__global__ void __launch_bounds__(InvShape<R, MODE, LOGN>::THREADS, InvShape<R, MODE, LOGN>::MINB)
 k_ccg_row_inv(CcgArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
-  typedef OpShape<R, LOGN> Sh;
+  typedef InvShape<R, MODE, LOGN> Sh;
+  typedef P2PlanR<LOGN, Sh::LR> P;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);

@@ -25,9 +25,8 @@ struct KernelInfo {
   int grid_per_sm = 0;
 };
 
-template <typename R, int LOGN, typename K>
+template <typename R, int LOGN, typename K, typename Sh = OpShape<R, LOGN>>
 int prepare(K kernel, KernelInfo& info) {
-  typedef OpShape<R, LOGN> Sh;
   if (info.ready) return info.grid_per_sm > 0 ? 0 : -1;
   const size_t smem = Sh::smem();
   if (cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -168,12 +167,13 @@ int ccg_row_fwd(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
 
 template <typename R, int MODE, int LOGN>
 int ccg_row_inv(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
-  typedef OpShape<R, LOGN> Sh;
+  typedef InvShape<R, MODE, LOGN> Sh;
   static KernelInfo info;
   int rc;
   {
     std::lock_guard<std::mutex> g(g_op_mu);
-    rc = prepare<R, LOGN>(k_ccg_row_inv<R, MODE, LOGN>, info);
+    rc = prepare<R, LOGN, decltype(&k_ccg_row_inv<R, MODE, LOGN>), Sh>(k_ccg_row_inv<R, MODE, LOGN>,
+                                                                       info);
   }
   if (rc || !launch) return rc;
   const int rows = MODE == MODE_T ? a.tx : a.op.nx;

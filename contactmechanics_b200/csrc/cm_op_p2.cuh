@@ -31,7 +31,7 @@
 // sequence of three launches on the caller's stream.  Blocks walk their
 // tiles with a grid stride, so the twiddle tables are staged once per block;
 // the transforms are the register-resident engines of cm_fft_p2.cuh (row
-// passes 2^LR elements per thread, column pass 16).
+// passes and column pass 2^LR elements per thread).
 #pragma once
 #include "cm_fft_p2.cuh"
 #include "cm_kernels.cuh"
@@ -57,6 +57,14 @@
 #define CM_COL_BASE 256
 #endif
 
+// log2 of the elements per thread of the column pass's transforms
+#ifndef CM_COL_LR_F32
+#define CM_COL_LR_F32 4
+#endif
+#ifndef CM_COL_LR_F64
+#define CM_COL_LR_F64 4
+#endif
+
 // log2 of the columns of a column group (at most; fewer when its shared
 // memory does not fit): 32 bytes of complex values
 #ifndef CM_COL_LW_F32
@@ -64,6 +72,13 @@
 #endif
 #ifndef CM_COL_LW_F64
 #define CM_COL_LW_F64 1
+#endif
+
+// log2 of the elements per thread of the solver's displacement pass
+// (k_ccg_row_inv<MODE_F>): its epilogue reads four fields per element, so it
+// keeps eight elements per thread and twice the resident warps
+#ifndef CM_ROW_LR_INVF_F32
+#define CM_ROW_LR_INVF_F32 3
 #endif
 
 // log2 of the elements per thread of the row passes' transforms (3: the
@@ -75,11 +90,12 @@
 #define CM_ROW_LR_F64 3
 #endif
 
-// threads of one block of the row passes for transform length 2^LOGN
-template <typename R, int LOGN>
+// threads of one block of the row passes for transform length 2^LOGN with
+// 2^LRV elements per thread
+template <typename R, int LOGN, int LRV = (sizeof(R) == 8 ? CM_ROW_LR_F64 : CM_ROW_LR_F32)>
 struct OpShape {
   static constexpr int N = 1 << LOGN;
-  static constexpr int LR = sizeof(R) == 8 ? CM_ROW_LR_F64 : CM_ROW_LR_F32;
+  static constexpr int LR = LRV;
   static constexpr int E = 1 << LR;  // elements per thread
   static constexpr int TPS = N >> LR;
   static constexpr int BASE = (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
@@ -97,7 +113,9 @@ template <typename R, int LOGX>
 struct ColShape {
   typedef typename CT<R>::C C;
   static constexpr int NX = 1 << LOGX;
-  static constexpr int TPS = NX / 16;
+  static constexpr int LR = sizeof(R) == 8 ? CM_COL_LR_F64 : CM_COL_LR_F32;
+  static constexpr int E = 1 << LR;  // elements per thread
+  static constexpr int TPS = NX / E;
   static constexpr size_t smem_for(int lw) {
     return (size_t)(NX + 2 * (((NX << lw)) + ((NX << lw) >> 3) + 1)) * sizeof(C);
   }
@@ -157,8 +175,8 @@ k_op_row_fwd(OpArgs<R> a) {
 // the thread's elements x = tt + q TPS, b = tt & 1): both rows of a pair load
 // Z_p(k) and Z_p(ny - k) (neighbouring lanes, one request) and each splits
 // off its own row.  Rows >= in_rows are zero.
-template <typename C, int TPS>
-CM_DEVINL void col_split_load(C (&v)[16], const C* __restrict__ spec, int ny, int k, int km, int tt,
+template <typename C, int TPS, int E>
+CM_DEVINL void col_split_load(C (&v)[E], const C* __restrict__ spec, int ny, int k, int km, int tt,
                               int in_rows, bool ok) {
   typedef decltype(v[0].x) R;
   const int b = tt & 1;
@@ -166,7 +184,7 @@ CM_DEVINL void col_split_load(C (&v)[16], const C* __restrict__ spec, int ny, in
   const C* __restrict__ skm = spec + km + (size_t)(tt >> 1) * ny;
   const int pstep = (TPS / 2) * ny;
 #pragma unroll
-  for (int h = 0; h < 16; h += 8) {
+  for (int h = 0; h < E; h += 8) {
     C z[8], zm[8];
 #pragma unroll
     for (int q = h; q < h + 8; ++q) {
@@ -191,8 +209,8 @@ CM_DEVINL void col_split_load(C (&v)[16], const C* __restrict__ spec, int ny, in
 // a pair writes W_p(k) = Xh_2p + i Xh_2p+1 (real parts only for the
 // self-conjugate columns 0 and ny/2), the odd row W_p(ny - k); pairs with
 // rows < out_rows.
-template <typename C, int TPS, int W>
-CM_DEVINL void col_pack_store(const C (&v)[16], C* __restrict__ spec, int ny, int k, int km, int tt,
+template <typename C, int TPS, int W, int E>
+CM_DEVINL void col_pack_store(const C (&v)[E], C* __restrict__ spec, int ny, int k, int km, int tt,
                               int out_rows, bool ok) {
   const int b = tt & 1;
   const int pairs_out = (out_rows + 1) >> 1;
@@ -201,7 +219,7 @@ CM_DEVINL void col_pack_store(const C (&v)[16], C* __restrict__ spec, int ny, in
   C* __restrict__ dst = spec + (b ? km : k) + (size_t)(tt >> 1) * ny;
   const int pstep = (TPS / 2) * ny;
 #pragma unroll
-  for (int q = 0; q < 16; ++q) {
+  for (int q = 0; q < E; ++q) {
     const C a = v[q];
     C o;
     o.x = __shfl_xor_sync(0xffffffffu, a.x, W);
@@ -217,15 +235,15 @@ template <typename R, int LOGX>
 __global__ void __launch_bounds__(ColShape<R, LOGX>::THREADS, 1)
 k_op_col(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGX, 4> P;
   typedef ColShape<R, LOGX> Sh;
-  constexpr int NX = P::N, W = Sh::W, LW = Sh::LW;
+  typedef P2PlanR<LOGX, Sh::LR> P;
+  constexpr int NX = P::N, W = Sh::W, LW = Sh::LW, E = Sh::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* bufA = tws + NX;
   C* bufB = bufA + smem_padded(Sh::NG * NX * W);
   pdl_trigger();
-  stage_tw_p2r<LOGX, 4>(tws, a.twx);
+  stage_tw_p2r<LOGX, Sh::LR>(tws, a.twx);
   pdl_wait();
   if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   __syncthreads();
@@ -241,17 +259,17 @@ k_op_col(OpArgs<R> a) {
     const int k = (g0 + j) * W + c;
     const bool ok = k < units;
     const int km = (ny - k) & (ny - 1);
-    C v[16];
-    col_split_load<C, P::TPS>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
-    fft_p2r<C, false, LOGX, 4>(v, bufA, bufB, base, W, tt, tws);
+    C v[E];
+    col_split_load<C, P::TPS, E>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
+    fft_p2r<C, false, LOGX, Sh::LR>(v, bufA, bufB, base, W, tt, tws);
     const R* __restrict__ tb =
         a.tab + ((size_t)(k >> tlw) * NX << tlw) + (k & (tW - 1)) + ((size_t)tt << tlw);
 #pragma unroll
-    for (int q = 0; q < 16; ++q)
+    for (int q = 0; q < E; ++q)
       v[q] = cscale(v[q], ok ? __ldg(tb + ((size_t)(q * P::TPS) << tlw)) : (R)0);
     __syncthreads();
-    fft_p2r<C, true, LOGX, 4>(v, bufA, bufB, base, W, tt, tws);
-    col_pack_store<C, P::TPS, W>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
+    fft_p2r<C, true, LOGX, Sh::LR>(v, bufA, bufB, base, W, tt, tws);
+    col_pack_store<C, P::TPS, W, E>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
     __syncthreads();  // buffers free for the next group
   }
 }

@@ -200,40 +200,56 @@ __global__ void k_table_periodic(double* G, int nx, int ny, int nyh, double sx, 
   }
 }
 
-// Displacement of a uniformly loaded dx x dy pixel (Love / Johnson p.54) on
-// the doubled domain, coordinates wrapped at i > nx.
 // Love's kernel: displacement of a uniformly loaded dx x dy pixel
-// (FFTElasticHalfSpace.py:1033-1137, Johnson 1985 p.54) on the doubled
-// domain.  The formula sums four corner terms that cancel: at a distance of
-// r pixels they exceed the result by about r^2, so evaluated in FP64 it
-// carries relative errors of about r^2 * 1e-16 (1e-9 of the displacement at
-// a 1024^2 topography).  It is therefore evaluated on the host in extended
-// precision, on the quadrant |x| <= tx dx, |y| <= ty dy only (the kernel is
-// even in x and y), and rounded once to FP64.
-static void love_quadrant_compute(std::vector<double>& q, int tx, int ty, double dx_d, double dy_d,
-                                  double young) {
+// (FFTElasticHalfSpace.py:1033-1137, Johnson 1985 p.54).  The formula sums
+// four corner terms that cancel: at a distance of r pixels they exceed the
+// result by about r^2, so evaluated in FP64 it carries relative errors of
+// about r^2 * 1e-16 (1e-9 of the displacement at a 1024^2 topography, more
+// for the far periodic images of a semi-periodic kernel).  It is therefore
+// evaluated on the host in extended precision and rounded once to FP64, on
+// the quadrant of non-negative offsets only (the kernel, and its sum over a
+// symmetric range of periodic images, is even in x and y):
+//   q[a][b] = sum over images (mx, my) of love(a dx + mx Lx, b dy + my Ly),
+// a < qx, b < qy; images -nimx..nimx along x (Lx the period), likewise y.
+struct LoveKey {
+  int qx, qy, nimx, nimy;
+  double dx, dy, young, Lx, Ly;
+  bool operator==(const LoveKey& o) const {
+    return qx == o.qx && qy == o.qy && nimx == o.nimx && nimy == o.nimy && dx == o.dx &&
+           dy == o.dy && young == o.young && Lx == o.Lx && Ly == o.Ly;
+  }
+};
+
+static void love_quadrant_compute(std::vector<double>& q, const LoveKey& k) {
   typedef long double L;
   const L pi = 3.141592653589793238462643383279502884L;
-  const L dx = dx_d, dy = dy_d, a = dx / 2, b = dy / 2, c = 1 / (pi * (L)young);
-  q.assign((size_t)(tx + 1) * (ty + 1), 0.0);
+  const L dx = k.dx, dy = k.dy, a = dx / 2, b = dy / 2, c = 1 / (pi * (L)k.young);
+  const L Lx = k.Lx, Ly = k.Ly;
+  const int qx = k.qx, qy = k.qy;
+  q.assign((size_t)qx * qy, 0.0);
   auto rows = [&](int i0, int i1) {
     for (int i = i0; i < i1; ++i) {
-      const L x = (L)i * dx, xp = x + a, xm = x - a;
-      for (int j = 0; j <= ty; ++j) {
-        const L y = (L)j * dy, yp = y + b, ym = y - b;
-        const L r_pp = sqrtl(yp * yp + xp * xp), r_mp = sqrtl(ym * ym + xp * xp);
-        const L r_pm = sqrtl(yp * yp + xm * xm), r_mm = sqrtl(ym * ym + xm * xm);
-        const L v = xp * logl((yp + r_pp) / (ym + r_mp)) + yp * logl((xp + r_pp) / (xm + r_pm)) +
-                    xm * logl((ym + r_mm) / (yp + r_pm)) + ym * logl((xm + r_mm) / (xp + r_mp));
-        q[(size_t)i * (ty + 1) + j] = (double)(c * v);
+      for (int j = 0; j < qy; ++j) {
+        L v = 0;
+        for (int mx = -k.nimx; mx <= k.nimx; ++mx) {
+          const L x = (L)i * dx + (L)mx * Lx, xp = x + a, xm = x - a;
+          for (int my = -k.nimy; my <= k.nimy; ++my) {
+            const L y = (L)j * dy + (L)my * Ly, yp = y + b, ym = y - b;
+            const L r_pp = sqrtl(yp * yp + xp * xp), r_mp = sqrtl(ym * ym + xp * xp);
+            const L r_pm = sqrtl(yp * yp + xm * xm), r_mm = sqrtl(ym * ym + xm * xm);
+            v += xp * logl((yp + r_pp) / (ym + r_mp)) + yp * logl((xp + r_pp) / (xm + r_pm)) +
+                 xm * logl((ym + r_mm) / (yp + r_pm)) + ym * logl((xm + r_mm) / (xp + r_mp));
+          }
+        }
+        q[(size_t)i * qy + j] = (double)(c * v);
       }
     }
   };
   const int nt = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
   std::vector<std::thread> pool;
-  const int per = (tx + 1 + nt - 1) / nt;
+  const int per = (qx + nt - 1) / nt;
   for (int t = 0; t < nt; ++t) {
-    const int i0 = t * per, i1 = std::min(tx + 1, i0 + per);
+    const int i0 = t * per, i1 = std::min(qx, i0 + per);
     if (i0 < i1) pool.emplace_back(rows, i0, i1);
   }
   for (auto& th : pool) th.join();
@@ -241,20 +257,11 @@ static void love_quadrant_compute(std::vector<double>& q, int tx, int ty, double
 
 // The quadrant of the last few geometries, so that plans of a geometry seen
 // before (a pool of solvers of one size) skip the extended-precision pass.
-struct LoveKey {
-  int tx, ty;
-  double dx, dy, young;
-  bool operator==(const LoveKey& o) const {
-    return tx == o.tx && ty == o.ty && dx == o.dx && dy == o.dy && young == o.young;
-  }
-};
 #define CM_LOVE_CACHE 16
 static std::mutex g_love_mu;
 static std::vector<std::pair<LoveKey, std::shared_ptr<const std::vector<double>>>> g_love_cache;
 
-static std::shared_ptr<const std::vector<double>> love_quadrant(int tx, int ty, double dx, double dy,
-                                                                 double young) {
-  const LoveKey key{tx, ty, dx, dy, young};
+static std::shared_ptr<const std::vector<double>> love_quadrant(const LoveKey& key) {
   {
     std::lock_guard<std::mutex> g(g_love_mu);
     for (size_t i = 0; i < g_love_cache.size(); ++i)
@@ -266,21 +273,22 @@ static std::shared_ptr<const std::vector<double>> love_quadrant(int tx, int ty, 
       }
   }
   auto q = std::make_shared<std::vector<double>>();
-  love_quadrant_compute(*q, tx, ty, dx, dy, young);
+  love_quadrant_compute(*q, key);
   std::lock_guard<std::mutex> g(g_love_mu);
   g_love_cache.emplace_back(key, q);
   if (g_love_cache.size() > CM_LOVE_CACHE) g_love_cache.erase(g_love_cache.begin());
   return q;
 }
 
-// out[i][j] of the doubled (nxd, nyd) domain = quadrant value at
-// (|x|, |y|) = (min(i, nxd - i), min(j, nyd - j)) pixels
-__global__ void k_love_expand(double* out, const double* q, int tx, int ty, int nxd, int nyd) {
+// out[i][j] of the (nxd, nyd) domain = quadrant value at the absolute
+// signed offset (|x|, |y|) = (min(i, nxd - i), min(j, nyd - j)) pixels; the
+// quadrant has rows of qy values
+__global__ void k_love_expand(double* out, const double* q, int qy, int nxd, int nyd) {
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nxd * nyd;
        idx += (long)gridDim.x * blockDim.x) {
     const int i = (int)(idx / nyd), j = (int)(idx % nyd);
     const int ai = min(i, nxd - i), aj = min(j, nyd - j);
-    out[idx] = q[(size_t)ai * (ty + 1) + aj];
+    out[idx] = q[(size_t)ai * qy + aj];
   }
 }
 
@@ -1465,19 +1473,27 @@ const char* cm_status_string(int status) {
 int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
   if (!desc || !out) return CM_ERR_ARG;
   *out = nullptr;
-  if (desc->kind != CM_PERIODIC && desc->kind != CM_FREE) return CM_ERR_ARG;
+  if (desc->kind != CM_PERIODIC && desc->kind != CM_FREE && desc->kind != CM_SEMI) return CM_ERR_ARG;
   if (desc->dim != 1 && desc->dim != 2) return CM_ERR_ARG;
   if (desc->nx < 1 || desc->ny < 1 || (desc->dim == 1 && desc->ny != 1)) return CM_ERR_ARG;
-  if (desc->kind == CM_FREE && desc->dim != 2) return CM_ERR_ARG;
+  if (desc->kind != CM_PERIODIC && desc->dim != 2) return CM_ERR_ARG;
+  if (desc->kind == CM_SEMI && (desc->n_images < 0 || desc->n_images > 10000)) return CM_ERR_ARG;
   if (!(desc->sx > 0) || !(desc->sy > 0)) return CM_ERR_ARG;
   cm_plan* p = new (std::nothrow) cm_plan();
   if (!p) return CM_ERR_OOM;
   p->d = *desc;
   p->tx = desc->nx;
   p->ty = desc->ny;
-  const int f = desc->kind == CM_FREE ? 2 : 1;
-  p->nx = f * desc->nx;
-  p->ny = f * desc->ny;
+  if (desc->kind == CM_SEMI) {
+    // a periodic axis keeps its points, a free one is padded to 2n - 1
+    // (FFTElasticHalfSpace.py:1343-1353)
+    p->nx = desc->periodic_x ? desc->nx : 2 * desc->nx - 1;
+    p->ny = desc->periodic_y ? desc->ny : 2 * desc->ny - 1;
+  } else {
+    const int f = desc->kind == CM_FREE ? 2 : 1;
+    p->nx = f * desc->nx;
+    p->ny = f * desc->ny;
+  }
   p->nyh = p->ny / 2 + 1;
   int rc = CM_OK;
   auto fail = [&](int code) {
@@ -1533,12 +1549,26 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
   } else {
     double *love = nullptr, *quad = nullptr;
     if ((rc = dalloc(p, &love, (long)p->nx * p->ny)) != CM_OK) return fail(rc);
-    const auto hq = love_quadrant(p->tx, p->ty, desc->sx / p->tx, desc->sy / p->ty, desc->young);
+    // the kernel at every absolute offset the domain holds (the free
+    // domain's offsets reach the topography's size, wrapped at i > nx), summed
+    // over the periodic images of a semi-periodic substrate
+    LoveKey key{};
+    key.qx = p->nx / 2 + 1;
+    key.qy = p->ny / 2 + 1;
+    key.dx = desc->sx / p->tx;
+    key.dy = desc->sy / p->ty;
+    key.young = desc->young;
+    key.Lx = desc->sx;
+    key.Ly = desc->sy;
+    const bool semi = desc->kind == CM_SEMI;
+    key.nimx = semi && desc->periodic_x ? desc->n_images : 0;
+    key.nimy = semi && desc->periodic_y ? desc->n_images : 0;
+    const auto hq = love_quadrant(key);
     if ((rc = dalloc(p, &quad, (long)hq->size())) != CM_OK) return fail(rc);
     if (cudaMemcpyAsync(quad, hq->data(), hq->size() * sizeof(double), cudaMemcpyHostToDevice, s) !=
         cudaSuccess)
       return fail(CM_ERR_CUDA);
-    k_love_expand<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, quad, p->tx, p->ty, p->nx, p->ny);
+    k_love_expand<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, quad, key.qy, p->nx, p->ny);
     rc = launch_plain<double>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
                                          0, 0, s);
     if (rc != CM_OK) return fail(rc);

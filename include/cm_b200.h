@@ -47,6 +47,7 @@ extern "C" {
 /* substrate kinds */
 #define CM_PERIODIC 0
 #define CM_FREE 1
+#define CM_SEMI 2   /* free along some axes, periodic (summed images) along others */
 
 /* precisions */
 #define CM_FP64 0   /* everything in FP64 */
@@ -78,6 +79,11 @@ typedef struct {
   int q0_mode;         /* CM_Q0_* (periodic only) */
   double stiffness_q0; /* used when q0_mode == CM_Q0_VALUE */
   double thickness;    /* <= 0: infinitely deep half-space (periodic only) */
+  /* CM_SEMI only (SemiPeriodicFFTElasticHalfSpace): periodicity of each axis;
+     a periodic axis keeps n points and sums the periodic images
+     -n_images..n_images into the kernel, a free axis has 2n - 1 points */
+  int periodic_x, periodic_y;
+  int n_images;
 } cm_plan_desc;
 
 typedef struct {
@@ -119,8 +125,9 @@ const char* cm_version(void);
  * Create a substrate plan: domain geometry, FFT twiddles and the
  * Green's-function tables built on the device in FP64 (with an FP32 copy).
  * Replaces PeriodicFFTElasticHalfSpace.__init__ (FFTElasticHalfSpace.py:169-306,
- * tables :445-571) and FreeFFTElasticHalfSpace.__init__ (:912-964, table
- * :1033-1139).  stream: the stream all work of this plan runs on (NULL: a new
+ * tables :445-571), FreeFFTElasticHalfSpace.__init__ (:912-964, table
+ * :1033-1139) and SemiPeriodicFFTElasticHalfSpace.__init__ (:1295-1363,
+ * table :1365-1500).  stream: the stream all work of this plan runs on (NULL: a new
  * non-blocking stream owned by the plan).
  */
 int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out);

@@ -180,6 +180,53 @@ def love_kernel_extended(nb_grid_pts, physical_sizes, young):
     return (val / (L(np.pi) * L(young))).astype(np.float64)
 
 
+def _love_at(x, y, dx, dy, young, log=np.log, sqrt=np.sqrt, pi=np.pi):
+    """Love's rectangle kernel at offset (x, y) from a uniformly loaded dx x dy
+    pixel (the four corner terms of FFTElasticHalfSpace.py:1064-1137)."""
+    a, b = dx / 2, dy / 2
+    xp, xm, yp, ym = x + a, x - a, y + b, y - b
+
+    def r(p, q):
+        return sqrt(p * p + q * q)
+    val = (xp * log((yp + r(yp, xp)) / (ym + r(ym, xp)))
+           + yp * log((xp + r(yp, xp)) / (xm + r(yp, xm)))
+           + xm * log((ym + r(ym, xm)) / (yp + r(yp, xm)))
+           + ym * log((xm + r(ym, xm)) / (xp + r(ym, xp))))
+    return val / (pi * young)
+
+
+def semi_periodic_domain(nb_grid_pts, periodicity):
+    """Domain of SemiPeriodicFFTElasticHalfSpace: n points along a periodic
+    axis, 2n - 1 along a free one (FFTElasticHalfSpace.py:1343-1353)."""
+    return tuple(n if per else 2 * n - 1 for n, per in zip(nb_grid_pts, periodicity))
+
+
+def semi_periodic_kernel(nb_grid_pts, physical_sizes, young, periodicity, n_images,
+                         extended=False):
+    """Real-space kernel of SemiPeriodicFFTElasticHalfSpace: Love's kernel at
+    the signed grid offsets of the domain (numpy fftfreq order, spacing
+    L / n), summed over the periodic images -n_images..n_images of each
+    periodic axis (FFTElasticHalfSpace.py:1365-1397, 1408-1500).  With
+    `extended` the sum is evaluated in numpy's longdouble and rounded once
+    (test helper: far images cancel by about r^2 eps in FP64)."""
+    nxd, nyd = semi_periodic_domain(nb_grid_pts, periodicity)
+    T = np.longdouble if extended else np.float64
+    L = [T(v) for v in physical_sizes]
+    dx, dy = L[0] / T(nb_grid_pts[0]), L[1] / T(nb_grid_pts[1])
+    xs = (np.round(np.fft.fftfreq(nxd) * nxd).astype(T) * dx).reshape(-1, 1)
+    ys = (np.round(np.fft.fftfreq(nyd) * nyd).astype(T) * dy).reshape(1, -1)
+    imx = range(-n_images, n_images + 1) if periodicity[0] else [0]
+    imy = range(-n_images, n_images + 1) if periodicity[1] else [0]
+    p = np.zeros((nxd, nyd), dtype=T)
+    kw = {}
+    if extended:
+        kw = dict(pi=T(np.pi) if False else T("3.14159265358979323846264338327950288"))
+    for ix in imx:
+        for iy in imy:
+            p += _love_at(xs + T(ix) * L[0], ys + T(iy) * L[1], dx, dy, T(young), **kw)
+    return p.astype(np.float64)
+
+
 def free_greens_function(nb_grid_pts, physical_sizes, young):
     """Hockney table: forward FFT of :func:`love_kernel`
     (FFTElasticHalfSpace.py:1138-1139).  Shape ``(nx+1, 2ny)`` complex."""
@@ -295,6 +342,41 @@ class FreeSubstrate(PeriodicSubstrate):
         if not ok:
             raise FreeBoundaryError(
                 "The forces not zero at the boundary of the active domain.")
+
+
+class SemiPeriodicSubstrate(FreeSubstrate):
+    """Oracle of ``SemiPeriodicFFTElasticHalfSpace``
+    (FFTElasticHalfSpace.py:1286-1539): free substrate whose periodic axes
+    keep n points and sum periodic images into the kernel."""
+
+    def __init__(self, nb_grid_pts, young, physical_sizes=(2 * np.pi, 2 * np.pi),
+                 periodicity=(False, True), n_images=10, check_boundaries=False, workers=1,
+                 extended=False):
+        self.nb_grid_pts = tuple(int(n) for n in nb_grid_pts)
+        self.dim = 2
+        self.physical_sizes = tuple(float(v) for v in physical_sizes)
+        self.young = young
+        self.workers = workers
+        self.periodicity = tuple(bool(p) for p in periodicity)
+        self.n_images = n_images
+        self.check_boundaries_flag = check_boundaries
+        self.G_real = semi_periodic_kernel(self.nb_grid_pts, self.physical_sizes, young,
+                                           self.periodicity, n_images, extended)
+        self.greens_function = fft_forward(self.G_real, workers)
+        self.surface_stiffness = surface_stiffness(self.greens_function)
+
+    @property
+    def nb_domain_grid_pts(self):
+        return semi_periodic_domain(self.nb_grid_pts, self.periodicity)
+
+    def evaluate_force(self, disp):
+        """Displacements that do not cover the domain are zero padded
+        (FFTElasticHalfSpace.py:1541-1565)."""
+        if disp.shape != self.nb_domain_grid_pts:
+            padded = np.zeros(self.nb_domain_grid_pts)
+            padded[:disp.shape[0], :disp.shape[1]] = disp
+            disp = padded
+        return super().evaluate_force(disp)
 
 
 # ---------------------------------------------------------------------------

@@ -2,11 +2,12 @@
 
 Run where a checkout of the reference is available (read-only is enough)::
 
-    python tests/golden/make_golden.py /path/to/reference
+    python tests/golden/make_golden.py /path/to/reference [--semi-only]
     # or: CM_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 
 It imports ContactMechanics unmodified over the serial stand-ins of
-``refstubs.py`` and writes ``tests/golden/*.npz``.  The fixtures are small
+``refstubs.py`` and writes ``tests/golden/reference_vectors.npz`` and
+``tests/golden/semi_vectors.npz`` (``--semi-only``: the second only).  The fixtures are small
 (grids of at most 64x64) so that the CPU test-suite stays fast.  The GPU box
 never runs this script; tests only read the committed ``.npz`` files.
 """
@@ -205,8 +206,64 @@ def main(ref_root):
     print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")
 
 
+def main_semi(ref_root):
+    """Golden vectors of SemiPeriodicFFTElasticHalfSpace (semi_vectors.npz)."""
+    refstubs.install(ref_root)
+    from ContactMechanics.FFTElasticHalfSpace import SemiPeriodicFFTElasticHalfSpace
+    from ContactMechanics.Systems import NonSmoothContactSystem
+    from refstubs import Topography
+
+    rng = np.random.default_rng(20261204)
+    out = {}
+    cases = [
+        ("s16x16_fp", (16, 16), (0.1, 0.1), (False, True), 10, 210e9),
+        ("s12x9_pf", (12, 9), (1.0, 2.0), (True, False), 4, 1.0),
+        ("s8x10_pp", (8, 10), (1.0, 1.0), (True, True), 3, 2.0),
+        ("s9x8_ff", (9, 8), (1.0, 1.0), (False, False), 0, 1.0),
+        ("s33x32_fp", (33, 32), (1.0, 1.0), (False, True), 10, 1.0),
+    ]
+    for name, nb, sizes, per, nim, young in cases:
+        s = SemiPeriodicFFTElasticHalfSpace(nb, young, sizes, periodicity=per, n_images=nim)
+        out[f"op_{name}_config"] = np.array(json.dumps(dict(
+            kind="semi", nb_grid_pts=list(nb), physical_sizes=list(sizes), young=young,
+            periodicity=list(per), n_images=nim, domain=list(s.nb_domain_grid_pts))))
+        f = rng.standard_normal(nb)
+        u = rng.standard_normal(s.nb_domain_grid_pts)
+        out[f"op_{name}_G"] = s.greens_function
+        out[f"op_{name}_f"] = f
+        out[f"op_{name}_disp"] = s.evaluate_disp(f)
+        out[f"op_{name}_disp_full"] = s.evaluate_disp(f, bIncludePadding=True)
+        out[f"op_{name}_u"] = u
+        out[f"op_{name}_force"] = s.evaluate_force(u)
+        out[f"op_{name}_force_topo"] = s.evaluate_force(u[:nb[0], :nb[1]])
+    # a load-controlled solve on a semi-periodic substrate: a cylinder-like
+    # ridge (periodic along y, free along x)
+    nb, sizes = (32, 24), (1.0, 1.0)
+    x = ((np.arange(nb[0]) - nb[0] / 2) * sizes[0] / nb[0]).reshape(-1, 1)
+    h = np.broadcast_to(-(x * x) / (2 * 1.5), nb).copy()
+    h += 1e-3 * rng.standard_normal(nb)
+    sub = SemiPeriodicFFTElasticHalfSpace(nb, 1.0, sizes, periodicity=(False, True), n_images=10)
+    kw = dict(external_force=2e-3, pentol=1e-12, forcetol=1e-14)
+    res = NonSmoothContactSystem(sub, Topography(h, sizes)).minimize_proxy(**kw)
+    out["ccg_semi_ridge_config"] = np.array(json.dumps(dict(
+        kind="semi", nb_grid_pts=list(nb), physical_sizes=list(sizes), young=1.0,
+        periodicity=[False, True], n_images=10, solver_kwargs=kw)))
+    out["ccg_semi_ridge_heights"] = h
+    out["ccg_semi_ridge_x"] = res.x
+    out["ccg_semi_ridge_jac"] = res.jac
+    out["ccg_semi_ridge_active_set"] = res.active_set
+    out["ccg_semi_ridge_scalars"] = np.array(
+        [res.offset, res.fun, res.nit, res.nfev, float(res.success)])
+    path = os.path.join(HERE, "semi_vectors.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")
+
+
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CM_REFERENCE")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else os.environ.get("CM_REFERENCE")
     if not ref:
-        sys.exit("usage: make_golden.py /path/to/reference (or set CM_REFERENCE)")
-    main(ref)
+        sys.exit("usage: make_golden.py /path/to/reference [--semi-only] (or set CM_REFERENCE)")
+    if "--semi-only" not in sys.argv:
+        main(ref)
+    main_semi(ref)

@@ -37,8 +37,8 @@ def test_status_strings():
 
 
 def test_struct_sizes_match_header_layout():
-    # cm_plan_desc: 4 ints, 4 doubles, int, 2 doubles (natural alignment)
-    assert ctypes.sizeof(_lib.PlanDesc) == 4 * 4 + 4 * 8 + 8 + 2 * 8
+    # cm_plan_desc: 4 ints, 4 doubles, int, 2 doubles, 3 ints (natural alignment)
+    assert ctypes.sizeof(_lib.PlanDesc) == 4 * 4 + 4 * 8 + 8 + 2 * 8 + 16
     assert ctypes.sizeof(_lib.CcgResult) % 8 == 0
 
 

@@ -155,10 +155,24 @@ def test_c4_plastic_periodic(cm, c4_case, precision):
         assert rel(pd, pd_ref) < 1e-9
     else:
         assert e < 1e-6, e
-        assert abs(npl - npl_ref) <= 1e-3 * npl_ref, (npl, npl_ref)
         a, ar = np.count_nonzero(res.jac > 0), np.count_nonzero(ref["jac"] > 0)
         assert abs(a - ar) <= 1e-3 * ar
         assert rel(pd, pd_ref) < 1e-5
+        # The plastic flag is the sign of a gap; at the rim of the flowing
+        # region gaps sit at the convergence tolerance, so a solve that
+        # reaches the same tolerances along another path (FP32, then FP64)
+        # may flag a few rim points differently.  Every mismatch lies on the
+        # rim (a point whose 4-neighbourhood holds both flags), and they are
+        # a small fraction of the plastic area.
+        pl, pl_ref = np.asarray(res.plastic, bool), np.asarray(ref["plastic"], bool)
+        rim = np.zeros_like(pl_ref)
+        for m in (pl_ref, pl):
+            for ax in (0, 1):
+                for sh in (1, -1):
+                    rim |= m != np.roll(m, sh, axis=ax)
+        mism = pl != pl_ref
+        assert not np.any(mism & ~rim), int(np.count_nonzero(mism & ~rim))
+        assert abs(npl - npl_ref) <= 5e-3 * npl_ref, (npl, npl_ref)
     assert float(res.jac.max()) <= H * (1.0 / n) ** 2 * (1 + 1e-12)
 
 
