@@ -23,6 +23,12 @@ def _torch():
     return torch
 
 
+def _host(a):
+    if hasattr(a, "detach") and hasattr(a, "cpu"):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
 class _Plan:
     """Owns one ``cm_plan`` (device tables, twiddles, work buffers)."""
 
@@ -269,16 +275,114 @@ class PeriodicFFTElasticHalfSpace(ElasticSubstrate):
 
     def evaluate_elastic_energy(self, forces, disp):
         """``0.5 * dot(disp, -forces)`` (FFTElasticHalfSpace.py:676-684)."""
-        return 0.5 * float(np.dot(np.ravel(np.asarray(disp)), np.ravel(-np.asarray(forces))))
+        return 0.5 * float(np.dot(np.ravel(_host(disp)), np.ravel(-_host(forces))))
+
+    # --- k-space (:613-805, 841-885): half spectra in the reference's
+    # layout, complex (nxd // 2 + 1, nyd), halved along x, unnormalised ----
+    def _kshape(self):
+        return self.nb_fourier_grid_pts
+
+    def _k_device(self, a):
+        """A contiguous complex128 device copy (or view) of a half spectrum."""
+        torch = _torch()
+        if isinstance(a, torch.Tensor):
+            t = a.to(device="cuda", dtype=torch.complex128).contiguous()
+        else:
+            t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128)).cuda()
+        if tuple(t.shape) != self._kshape():
+            raise self.Error("Fourier array has shape {} but this halfspace's half spectrum "
+                             "has shape {}".format(tuple(t.shape), self._kshape()))
+        return t
+
+    def _fft(self, field):
+        """Forward transform of a domain-shaped real field (device FP64)."""
+        torch = _torch()
+        is_np = not isinstance(field, torch.Tensor)
+        src = (torch.from_numpy(np.ascontiguousarray(field, dtype=np.float64)).cuda() if is_np
+               else field.to(device="cuda", dtype=torch.float64).contiguous())
+        nxd = self.nb_domain_grid_pts[0]
+        nyd = self.nb_domain_grid_pts[1] if self.dim == 2 else 1
+        src = src.reshape(nxd, nyd)
+        out = torch.empty(self._kshape(), dtype=torch.complex128, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream or _lib.CUDA_STREAM_LEGACY
+        _lib.check(self._plan._L.cm_fft_forward(self._plan.ptr, ctypes.c_void_p(src.data_ptr()),
+                                                nxd, nyd, nyd, ctypes.c_void_p(out.data_ptr()),
+                                                ctypes.c_void_p(stream)))
+        return out, is_np
+
+    def _kapply(self, op, scale, k, as_numpy):
+        torch = _torch()
+        out = torch.empty_like(k)
+        stream = torch.cuda.current_stream().cuda_stream or _lib.CUDA_STREAM_LEGACY
+        _lib.check(self._plan._L.cm_kspace_apply(self._plan.ptr, op, float(scale),
+                                                 ctypes.c_void_p(k.data_ptr()),
+                                                 ctypes.c_void_p(out.data_ptr()),
+                                                 ctypes.c_void_p(stream)))
+        return out.cpu().numpy() if as_numpy else out
+
+    def evaluate_k_disp(self, forces):
+        """k-space displacements ``G fft(-f) / a`` (FFTElasticHalfSpace.py:613-636)."""
+        if self._shape(forces) != self.nb_subdomain_grid_pts:
+            raise self.Error(
+                ("force array has a different shape ({0}) than this halfspace's "
+                 "nb_grid_pts ({1})").format(self._shape(forces), self.nb_subdomain_grid_pts))
+        k, is_np = self._fft(forces)
+        return self._kapply(_lib.CM_OP_DISP, -1.0 / self.area_per_pt, k, is_np)
+
+    def evaluate_k_force(self, disp):
+        """k-space forces ``-K fft(u) a`` (FFTElasticHalfSpace.py:638-655)."""
+        if self._shape(disp) != self.nb_subdomain_grid_pts:
+            raise self.Error(
+                ("displacements array has a different shape ({0}) than this halfspace's "
+                 "nb_grid_pts ({1})").format(self._shape(disp), self.nb_subdomain_grid_pts))
+        k, is_np = self._fft(disp)
+        return self._kapply(_lib.CM_OP_FORCE, -self.area_per_pt, k, is_np)
+
+    def evaluate_k_force_k(self, disp_k):
+        """k-space forces of k-space displacements ``-K u_k a`` (:657-674)."""
+        torch = _torch()
+        as_np = not isinstance(disp_k, torch.Tensor)
+        return self._kapply(_lib.CM_OP_FORCE, -self.area_per_pt, self._k_device(disp_k), as_np)
+
+    def evaluate_scalar_product_k_space(self, ka, kb):
+        """sum_ij a_ij b_ij from the half spectra of a and b (power theorem,
+        FFTElasticHalfSpace.py:686-805)."""
+        a, b = self._k_device(ka), self._k_device(kb)
+        out = ctypes.c_double()
+        torch = _torch()
+        stream = torch.cuda.current_stream().cuda_stream or _lib.CUDA_STREAM_LEGACY
+        _lib.check(self._plan._L.cm_kspace_dot(self._plan.ptr, ctypes.c_void_p(a.data_ptr()),
+                                               ctypes.c_void_p(b.data_ptr()), ctypes.byref(out),
+                                               ctypes.c_void_p(stream)))
+        return out.value
+
+    def evaluate_elastic_energy_k_space(self, kforces, kdisp):
+        """``-1/2 sum u f`` from half spectra (FFTElasticHalfSpace.py:807-839)."""
+        return -0.5 * self.evaluate_scalar_product_k_space(kdisp, kforces)
 
     def evaluate(self, disp, pot=True, forces=False):
-        """Energy and/or forces of a displacement field (FFTElasticHalfSpace.py:841-885).
+        """Energy and/or forces of a displacement field (FFTElasticHalfSpace.py:841-868):
+        with forces, the energy is the real-space product; without, it is
+        evaluated in k-space from the transform of the displacements."""
+        force = potential = None
+        if forces:
+            force = self.evaluate_force(disp)
+            if pot:
+                potential = self.evaluate_elastic_energy(force, disp)
+        elif pot:
+            dispk, _ = self._fft(disp)
+            kforce = self._kapply(_lib.CM_OP_FORCE, -self.area_per_pt, dispk, False)
+            potential = self.evaluate_elastic_energy_k_space(kforce, dispk)
+        return potential, force
 
-        The energy is evaluated in real space in both branches; by Parseval it
-        equals the reference's k-space energy to rounding."""
-        force = self.evaluate_force(disp)
-        potential = self.evaluate_elastic_energy(force, disp) if pot else None
-        return potential, (force if forces else None)
+    def evaluate_k(self, disp_k, pot=True, forces=False):
+        """Energy and k-space forces of a k-space displacement field (:870-885);
+        like the reference, the forces come back whenever either is asked for."""
+        if not (pot or forces):
+            return None, None
+        force_k = self.evaluate_k_force_k(disp_k)
+        potential = self.evaluate_elastic_energy_k_space(force_k, disp_k) if pot else None
+        return potential, force_k
 
 
 class FreeFFTElasticHalfSpace(PeriodicFFTElasticHalfSpace):

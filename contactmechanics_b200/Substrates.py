@@ -57,6 +57,14 @@ class ElasticSubstrate(Substrate, metaclass=abc.ABCMeta):
     def compute(self, disp, pot=True, forces=False):
         self.energy, self.force = self.evaluate(disp, pot, forces)
 
+    def compute_k(self, disp_k, pot=True, forces=False):
+        """Energy and/or forces from a displacement field in Fourier space
+        (Substrates.py:151-166)."""
+        self.energy, self.force_k = self.evaluate_k(disp_k, pot, forces)
+
+    def evaluate_k(self, disp_k, pot=True, forces=False):
+        raise NotImplementedError()
+
     def evaluate(self, disp, pot=True, forces=False):
         raise NotImplementedError()
 

@@ -1373,6 +1373,70 @@ static int stepper_run(cm_stepper* stp, const std::vector<cm_plan*>& plans, int 
 }
 
 // ---------------------------------------------------------------------------
+// k-space operators on half spectra of the reference's layout
+// ---------------------------------------------------------------------------
+// out[kx][ky] (kx <= nx/2, ky < ny) of the reference's half spectrum, halved
+// along x, from the library's spectrum halved along y (column tiles of
+// width 2^lw): the mirror (-kx, -ky) holds the conjugate of a real field's
+// transform for ky > ny/2.
+__global__ void k_spec_to_ref(const double2* __restrict__ spec, double2* __restrict__ out, int nx,
+                              int ny, int lw) {
+  const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
+  const long n = (long)nxh * ny;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int kx = (int)(i / ny), ky = (int)(i % ny);
+    double2 v;
+    if (ky < nyh) {
+      v = spec[spec_at(kx, ky, nx, lw)];
+    } else {
+      v = spec[spec_at((nx - kx) % nx, ny - ky, nx, lw)];
+      v.y = -v.y;
+    }
+    out[i] = v;
+  }
+}
+
+// k_out = scale T k_in, T = G (op 0) or 1/G (op 1, 0 where G = 0); G is the
+// natural (nx, nyh) table, even in kx and ky
+__global__ void k_kspace_apply(const double* __restrict__ G, const double2* k_in, double2* k_out,
+                               int nx, int ny, int op, double scale) {
+  const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
+  const long n = (long)nxh * ny;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int kx = (int)(i / ny), ky = (int)(i % ny);
+    const double g = G[(size_t)kx * nyh + min(ky, ny - ky)];
+    const double t = op == CM_OP_DISP ? g : (g != 0.0 ? 1.0 / g : 0.0);
+    double2 v = k_in[i];
+    v.x *= scale * t;
+    v.y *= scale * t;
+    k_out[i] = v;
+  }
+}
+
+// per-block partial sums of w_kx Re(conj(a) b) over the reference half spectrum
+__global__ void __launch_bounds__(256) k_kspace_dot(const double2* __restrict__ a,
+                                                    const double2* __restrict__ b, int nx, int ny,
+                                                    double* partial) {
+  const int nxh = nx / 2 + 1;
+  const long n = (long)nxh * ny;
+  double acc = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int kx = (int)(i / ny);
+    const double w = (kx == 0 || (nx % 2 == 0 && 2 * kx == nx)) ? 1.0 : 2.0;
+    const double2 u = a[i], v = b[i];
+    acc += w * (u.x * v.x + u.y * v.y);
+  }
+  __shared__ double sm[256];
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sm[threadIdx.x] += sm[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+// ---------------------------------------------------------------------------
 // self-test of the bounded grid barrier
 // ---------------------------------------------------------------------------
 // Every block meets at one grid barrier (cm_kernels.cuh: grid_barrier) with a
@@ -1970,6 +2034,52 @@ int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young
   k_row_inv<double, MODE_PLAIN><<<nt_row, T.threads_row, T.smem_row, s>>>(d_slot, d_items);
   g_launches += 6;
   CK(cudaGetLastError());
+  return CM_OK;
+}
+
+int cm_fft_forward(cm_plan* p, const double* in, int in_rows, int in_cols, int in_ld, double* out,
+                   void* stream) {
+  if (!p || !in || !out) return CM_ERR_ARG;
+  if (in_rows < 0 || in_rows > p->nx || in_cols < 0 || in_cols > p->ny || in_ld < in_cols)
+    return CM_ERR_SHAPE;
+  cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
+  CKS(launch_plain<double>(p, p->w64, MODE_FWD, 0, in, in_rows, in_cols, in_ld, nullptr, 0, 0, 0, s));
+  const long n = (long)(p->nx / 2 + 1) * p->ny;
+  k_spec_to_ref<<<grid_for(n), 256, 0, s>>>(p->w64.spec, (double2*)out, p->nx, p->ny,
+                                            p->w64.tiles.lw);
+  g_launches += 1;
+  CK(cudaGetLastError());
+  return CM_OK;
+}
+
+int cm_kspace_apply(cm_plan* p, int op, double scale, const double* k_in, double* k_out, void* stream) {
+  if (!p || !k_in || !k_out || (op != CM_OP_DISP && op != CM_OP_FORCE)) return CM_ERR_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
+  const long n = (long)(p->nx / 2 + 1) * p->ny;
+  k_kspace_apply<<<grid_for(n), 256, 0, s>>>(p->G, (const double2*)k_in, (double2*)k_out, p->nx,
+                                             p->ny, op, scale);
+  g_launches += 1;
+  CK(cudaGetLastError());
+  return CM_OK;
+}
+
+int cm_kspace_dot(cm_plan* p, const double* ka, const double* kb, double* out, void* stream) {
+  if (!p || !ka || !kb || !out) return CM_ERR_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
+  const long n = (long)(p->nx / 2 + 1) * p->ny;
+  const int blocks = (int)std::max(1L, std::min((n + 255) / 256, 1184L));
+  // the solver's reduction scratch holds at least max(nx, tiles) * 32 doubles
+  if (blocks > p->w64.partial_blocks * CM_MAX_PARTIAL_VALS) return CM_ERR_SIZE;
+  k_kspace_dot<<<blocks, 256, 0, s>>>((const double2*)ka, (const double2*)kb, p->nx, p->ny,
+                                      p->w64.partials);
+  g_launches += 1;
+  std::vector<double> part(blocks);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(part.data(), p->w64.partials, blocks * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double acc = 0.0;
+  for (double v : part) acc += v;
+  *out = acc / ((double)p->nx * (double)p->ny);
   return CM_OK;
 }
 

@@ -159,6 +159,40 @@ int cm_apply(cm_plan* plan, int op, int precision, const void* in_dev, int in_ro
              void* stream);
 
 /*
+ * k-space operators (FFTElasticHalfSpace.py:613-805, 841-885).  Half spectra
+ * use the reference's layout: complex FP64 values (interleaved re, im) of
+ * shape (nxd / 2 + 1, nyd), halved along x, unnormalised (numpy's rfftn
+ * over axes (1, 0), the muGrid FFTEngine's forward transform).
+ *
+ * cm_fft_forward: the half spectrum of a real FP64 field that occupies rows
+ * [0,in_rows) x cols [0,in_cols) of the domain (leading dimension in_ld) and
+ * is zero elsewhere -- the fftengine.fft of evaluate_k_disp, evaluate_k_force
+ * and evaluate (:613-656, 862-866).
+ */
+int cm_fft_forward(cm_plan* plan, const double* in_dev, int in_rows, int in_cols, int in_ld,
+                   double* out_dev, void* stream);
+
+/*
+ * k_out = scale * T * k_in on half spectra of the reference layout, with T
+ * the Green's table G (op CM_OP_DISP) or the surface stiffness K = 1/G, 0
+ * where G = 0 (op CM_OP_FORCE).  evaluate_k_disp(f) = G fft(-f) / a_pt,
+ * evaluate_k_force(u) = -K fft(u) a_pt, evaluate_k_force_k(u_k) = -K u_k a_pt
+ * (:613-674).  k_in and k_out may be the same array.
+ */
+int cm_kspace_apply(cm_plan* plan, int op, double scale, const double* k_in_dev, double* k_out_dev,
+                    void* stream);
+
+/*
+ * Scalar product sum_ij a_ij b_ij of two real domain fields from their half
+ * spectra (the power theorem, :686-805): sum over the half spectrum of
+ * w_k Re(conj(a_k) b_k) / (nxd nyd), w = 1 on the rows without a mirror
+ * (row 0 and, for even nxd, row nxd / 2), 2 on the others.  *out_host
+ * receives the sum (FP64 partial sums per block added in a fixed order).
+ */
+int cm_kspace_dot(cm_plan* plan, const double* ka_dev, const double* kb_dev, double* out_host,
+                  void* stream);
+
+/*
  * Polonsky-Keer constrained conjugate gradients
  * (ConstrainedConjugateGradients.py:47-509) on one substrate.
  *   heights_dev      (nx, ny) FP64 topography heights

@@ -287,6 +287,33 @@ class PeriodicSubstrate:
             raise SubstrateError("displacements array has a different shape")
         return self._apply(self.surface_stiffness, disp, -self.area_per_pt)
 
+    # k-space (FFTElasticHalfSpace.py:613-805): half spectra halved along x
+    def evaluate_k_disp(self, forces):
+        return self.greens_function * fft_forward(-forces, self.workers) / self.area_per_pt
+
+    def evaluate_k_force(self, disp):
+        return -self.surface_stiffness * fft_forward(disp, self.workers) * self.area_per_pt
+
+    def evaluate_k_force_k(self, disp_k):
+        return -self.surface_stiffness * disp_k * self.area_per_pt
+
+    def evaluate_scalar_product_k_space(self, ka, kb):
+        """Power theorem on rfftn half spectra: rows without a mirror (0 and
+        the Nyquist row of an even length) count once, the others twice."""
+        nx = self.nb_domain_grid_pts[0]
+        w = np.full(ka.shape[0], 2.0)
+        w[0] = 1.0
+        if nx % 2 == 0:
+            w[-1] = 1.0
+        prod = (np.conj(ka) * kb).real
+        prod = prod.reshape(ka.shape[0], -1)
+        return float((w[:, None] * prod).sum() / np.prod(self.nb_domain_grid_pts))
+
+    def evaluate_energy_k(self, disp):
+        """``evaluate(disp, pot=True, forces=False)``: the k-space energy."""
+        dk = fft_forward(disp, self.workers)
+        return -0.5 * self.evaluate_scalar_product_k_space(dk, self.evaluate_k_force_k(dk))
+
 
 class FreeSubstrate(PeriodicSubstrate):
     """Oracle of ``FreeFFTElasticHalfSpace`` (FFTElasticHalfSpace.py:888)."""

@@ -2,12 +2,14 @@
 
 Run where a checkout of the reference is available (read-only is enough)::
 
-    python tests/golden/make_golden.py /path/to/reference [--semi-only]
+    python tests/golden/make_golden.py /path/to/reference [--only=main|semi|kspace]
     # or: CM_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 
 It imports ContactMechanics unmodified over the serial stand-ins of
-``refstubs.py`` and writes ``tests/golden/reference_vectors.npz`` and
-``tests/golden/semi_vectors.npz`` (``--semi-only``: the second only).  The fixtures are small
+``refstubs.py`` and writes ``tests/golden/reference_vectors.npz`` (operators,
+solves, sweeps), ``semi_vectors.npz`` (SemiPeriodicFFTElasticHalfSpace) and
+``kspace_vectors.npz`` (k-space operators and energies); ``--only=`` picks
+one of them.  The fixtures are small
 (grids of at most 64x64) so that the CPU test-suite stays fast.  The GPU box
 never runs this script; tests only read the committed ``.npz`` files.
 """
@@ -259,11 +261,51 @@ def main_semi(ref_root):
     print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")
 
 
+def main_kspace(ref_root):
+    """Golden vectors of the k-space operators and energies (kspace_vectors.npz)."""
+    refstubs.install(ref_root)
+    from ContactMechanics import FreeFFTElasticHalfSpace, PeriodicFFTElasticHalfSpace
+
+    rng = np.random.default_rng(20261205)
+    out = {}
+    cases = [("p16x12", PeriodicFFTElasticHalfSpace, (16, 12), (2.0, 1.5), dict(poisson=0.3)),
+             ("p9x7", PeriodicFFTElasticHalfSpace, (9, 7), (1.0, 1.0), {}),
+             ("p15", PeriodicFFTElasticHalfSpace, (15,), (2.0,), {}),
+             ("f8x6", FreeFFTElasticHalfSpace, (8, 6), (1.0, 2.0), {})]
+    for name, cls, nb, sizes, kw in cases:
+        s = cls(nb, 1.3, sizes, **kw)
+        dom = s.nb_domain_grid_pts
+        out[f"k_{name}_config"] = np.array(json.dumps(dict(
+            kind="free" if cls is FreeFFTElasticHalfSpace else "periodic",
+            nb_grid_pts=list(nb), physical_sizes=list(sizes), young=1.3, kwargs=kw)))
+        f = rng.standard_normal(dom)
+        u = rng.standard_normal(dom)
+        ka = s.evaluate_k_disp(f)
+        kb = s.evaluate_k_force(u)
+        out[f"k_{name}_f"] = f
+        out[f"k_{name}_u"] = u
+        out[f"k_{name}_kdisp"] = ka
+        out[f"k_{name}_kforce"] = kb
+        out[f"k_{name}_kforce_k"] = s.evaluate_k_force_k(ka)
+        out[f"k_{name}_dot"] = np.array(s.evaluate_scalar_product_k_space(ka, kb))
+        out[f"k_{name}_energy_k"] = np.array(s.evaluate(u, pot=True, forces=False)[0])
+        e, fk = s.evaluate_k(ka, pot=True, forces=True)
+        out[f"k_{name}_evaluate_k_energy"] = np.array(e)
+    path = os.path.join(HERE, "kspace_vectors.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref = args[0] if args else os.environ.get("CM_REFERENCE")
     if not ref:
-        sys.exit("usage: make_golden.py /path/to/reference [--semi-only] (or set CM_REFERENCE)")
-    if "--semi-only" not in sys.argv:
+        sys.exit("usage: make_golden.py /path/to/reference [--only=main|semi|kspace] "
+                 "(or set CM_REFERENCE)")
+    only = [a[7:] for a in sys.argv[1:] if a.startswith("--only=")]
+    if not only or "main" in only:
         main(ref)
-    main_semi(ref)
+    if not only or "semi" in only:
+        main_semi(ref)
+    if not only or "kspace" in only:
+        main_kspace(ref)
