@@ -33,14 +33,15 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long mbar;
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
+  C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
   if (threadIdx.x == 0) {
     mbar_init(&mbar, 1);
     mbar_init_fence();
   }
-  stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
+  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
+  const C* tw = Sh::ONEBUF ? a.op.twy : tws;
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
@@ -65,8 +66,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
   // otherwise they are loaded per element.
   R* stg = reinterpret_cast<R*>(bufA);
   const int nfield = 1 + (need_gap ? 2 : 0) + (MODE == MODE_T ? 1 : 0);
-  const int nst = nfield >= 3 && (size_t)nfield * ROWS * ty * sizeof(R) <= 2 * smem_padded(NP * N) * sizeof(C)
-                      ? nfield : 0;
+  const int nst = nfield >= 3 && (size_t)nfield * ROWS * ty * sizeof(R) <= Sh::STAGE ? nfield : 0;
   const int jt = need_gap ? 3 : 1;  // field index of t
   // reductions accumulate over the block's tiles; one partial per block
   double acc = 0.0;
@@ -182,7 +182,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
     C v[Sh::E];
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
-    fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
+    fft_p2x<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (xa < tx) {
       C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N + tt;
 #pragma unroll
@@ -207,8 +207,8 @@ k_ccg_row_fwd(CcgArgs<R> a) {
 // solves has its own elements per thread
 template <typename R, int MODE, int LOGN>
 using InvShape = OpShape<R, LOGN,
-                         (MODE == MODE_F && sizeof(R) == 4) ? CM_ROW_LR_INVF_F32
-                                                            : OpShape<R, LOGN>::LR>;
+                         (MODE == MODE_F && sizeof(R) == 4 && LOGN <= 12) ? CM_ROW_LR_INVF_F32
+                                                                          : OpShape<R, LOGN>::LR>;
 
 template <typename R, int MODE, int LOGN>
 __global__ void __launch_bounds__(InvShape<R, MODE, LOGN>::THREADS, InvShape<R, MODE, LOGN>::MINB)
@@ -219,10 +219,11 @@ k_ccg_row_inv(CcgArgs<R> a) {
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
+  C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
+  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
+  const C* tw = Sh::ONEBUF ? a.op.twy : tws;
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
@@ -258,7 +259,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) v[q] = have ? srow[q * P::TPS] : czero<C>();
     }
-    fft_p2r<C, true, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
+    fft_p2x<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (MODE == MODE_T) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) {

@@ -284,3 +284,77 @@ CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int
     Ns *= RAD;
   }
 }
+
+// The same transform for lengths whose ping-pong buffers and staged twiddle
+// tables do not fit a block's shared memory (FP64 at 2^13): one shared
+// buffer (every exchange writes, waits, reads and waits again before the
+// next write) and the twiddles read from the length-N table tw_n[m] = W^m in
+// global memory (L1/L2-cached; W^(q k N/(RAD Ns)) is entry q k step mod N,
+// the value the staged tables hold).  Same contract as fft_p2r otherwise.
+template <typename C, bool INV, int LOGN, int LR>
+CM_DEVINL void fft_p2r_1buf(C (&v)[1 << LR], C* buf, int base, int estride, int tt,
+                            const C* __restrict__ tw_n) {
+  typedef P2PlanR<LOGN, LR> P;
+  constexpr int RAD = P::RAD, N = P::N;
+  {
+    constexpr int R = P::FIRST;
+    constexpr int B = RAD / R;
+    C o[RAD];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+      C g[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) g[q] = v[i + B * q];
+      dft_rr<INV, R>(g);
+#pragma unroll
+      for (int q = 0; q < R; ++q) o[i * R + q] = g[q];
+    }
+    if (P::NST == 1) {
+#pragma unroll
+      for (int i = 0; i < RAD; ++i) v[i] = o[i];
+      return;
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+      const int j = tt + i * P::TPS;
+#pragma unroll
+      for (int q = 0; q < R; ++q) buf[spad(base + (j * R + q) * estride)] = o[i * R + q];
+    }
+  }
+  __syncthreads();
+  int Ns = P::FIRST;
+#pragma unroll
+  for (int s = 1; s < P::NST; ++s) {
+    const int k = tt & (Ns - 1);
+    const int step = N / (Ns * RAD);
+    C g[RAD];
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) g[q] = buf[spad(base + (tt + q * P::TPS) * estride)];
+#pragma unroll
+    for (int q = 1; q < RAD; ++q) {
+      const C w = __ldg(tw_n + ((q * k * step) & (N - 1)));
+      g[q] = INV ? cmulc(g[q], w) : cmul(g[q], w);
+    }
+    dft_rr<INV, RAD>(g);
+    if (s == P::NST - 1) {
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) v[q] = g[q];
+    } else {
+      __syncthreads();  // every read of this stage is done before the buffer is rewritten
+      const int ob = (tt - k) * RAD + k;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) buf[spad(base + (ob + q * Ns) * estride)] = g[q];
+      __syncthreads();
+    }
+    Ns *= RAD;
+  }
+}
+
+// fft_p2r, or fft_p2r_1buf when ONEBUF (bufB and the staged tables unused;
+// tw is then the global length-N table)
+template <typename C, bool INV, int LOGN, int LR, bool ONEBUF>
+CM_DEVINL void fft_p2x(C (&v)[1 << LR], C* bufA, C* bufB, int base, int estride, int tt,
+                       const C* tw) {
+  if constexpr (ONEBUF) fft_p2r_1buf<C, INV, LOGN, LR>(v, bufA, base, estride, tt, tw);
+  else fft_p2r<C, INV, LOGN, LR>(v, bufA, bufB, base, estride, tt, tw);
+}

@@ -13,6 +13,8 @@
 
 
 #define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+// the by-value operator and solver passes also cover 2^13
+#define CM_OP_P2_CASES(X) CM_P2_CASES(X) X(13)
 
 // Launch one power-of-two pass of the CCG iteration (MODE_T or MODE_F) for
 // sides 2^logn; false if logn has no specialisation.
@@ -43,6 +45,8 @@ struct OpArgs {
   int out_rows, out_cols, out_ld;
   int nx, nyh, lw;  // domain rows, half-spectrum columns, log2 of the table's column tiles
   int ny;           // domain columns (row length of the pair-major spectrum)
+  R* fwd_real;      // column pass: forward transform only, its real part to this
+                    // natural (nx, ny/2 + 1) array (nullptr: the operator)
   int ntile_cols;
   C* spec;
   const R* tab;     // the selected Green's table, tiled like the spectrum
@@ -102,6 +106,10 @@ template <typename R>
 int op_p2_supported(int logx, int logy, int lw);
 template <typename R>
 int op_p2_apply(const OpArgs<R>& a, int logx, int logy, cudaStream_t s);
+// The row pass and a forward-only column pass writing the real part of the
+// 2D transform to a.fwd_real (same return codes).
+template <typename R>
+int op_p2_fwd_real(const OpArgs<R>& a, int logx, int logy, cudaStream_t s);
 // The passes of one CCG iteration of a single solve on a power-of-two domain
 // (MODE_T: r = G t, MODE_F: u = G f), same return codes.
 template <typename R, int MODE>

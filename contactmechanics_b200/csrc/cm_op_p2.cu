@@ -125,7 +125,7 @@ template <typename R>
 int dispatch_row_fwd(int logn, const OpArgs<R>& a, cudaStream_t s) {
   switch (logn) {
 #define CM_CASE(L) case L: return row_fwd<R, L>(a, s);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -134,7 +134,7 @@ template <typename R>
 int dispatch_col(int logn, const OpArgs<R>& a, cudaStream_t s) {
   switch (logn) {
 #define CM_CASE(L) case L: return col<R, L>(a, s);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -143,7 +143,7 @@ template <typename R>
 int dispatch_row_inv(int logn, const OpArgs<R>& a, cudaStream_t s) {
   switch (logn) {
 #define CM_CASE(L) case L: return row_inv<R, L>(a, s);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -189,7 +189,7 @@ template <typename R, int MODE>
 int ccg_p2_row_fwd(const CcgArgs<R>& a, int logy, cudaStream_t s) {
   switch (logy) {
 #define CM_CASE(L) case L: return ccg_row_fwd<R, MODE, L>(a, s);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -204,7 +204,7 @@ template <typename R, int MODE>
 int ccg_p2_row_inv(const CcgArgs<R>& a, int logy, cudaStream_t s) {
   switch (logy) {
 #define CM_CASE(L) case L: return ccg_row_inv<R, MODE, L>(a, s);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -221,14 +221,14 @@ int ccg_p2_prepare(const CcgArgs<R>& a, int logx, int logy) {
     if (!rc) rc = ccg_row_inv<R, MODE_T, L>(a, nullptr, false);          \
     if (!rc) rc = ccg_row_inv<R, MODE_F, L>(a, nullptr, false);          \
     break;
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
   if (rc) return rc;
   switch (logx) {
 #define CM_CASE(L) case L: return col<R, L>(a.op, nullptr, false);
-    CM_P2_CASES(CM_CASE)
+    CM_OP_P2_CASES(CM_CASE)
 #undef CM_CASE
     default: return -1;
   }
@@ -265,7 +265,7 @@ int ccg_p2_ew_blocks_per_sm() {
 template <typename R>
 int op_p2_supported(int logx, int logy, int lw) {
   (void)lw;  // the column pass reads the tables in any column tiling
-  return logx >= 6 && logx <= 12 && logy >= 6 && logy <= 12;
+  return logx >= 6 && logx <= 13 && logy >= 6 && logy <= 13;
 }
 
 template <typename R>
@@ -278,6 +278,16 @@ int op_p2_apply(const OpArgs<R>& a, int logx, int logy, cudaStream_t s) {
   return rc;
 }
 
+template <typename R>
+int op_p2_fwd_real(const OpArgs<R>& a, int logx, int logy, cudaStream_t s) {
+  if (!op_p2_supported<R>(logx, logy, a.lw) || !a.fwd_real) return -1;
+  int rc = dispatch_row_fwd<R>(logy, a, s);
+  if (!rc) rc = dispatch_col<R>(logx, a, s);
+  if (!rc && cudaGetLastError() != cudaSuccess) rc = 1;
+  return rc;
+}
+
+template int op_p2_fwd_real<double>(const OpArgs<double>&, int, int, cudaStream_t);
 template int op_p2_supported<float>(int, int, int);
 template int op_p2_supported<double>(int, int, int);
 template int op_p2_apply<float>(const OpArgs<float>&, int, int, cudaStream_t);

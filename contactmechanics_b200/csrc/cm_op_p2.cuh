@@ -1,5 +1,5 @@
 // The elastic operator u = IFFT(T . FFT(f)) (FFTElasticHalfSpace.py:573-611,
-// free :1141-1197) for power-of-two domains (sides 64..4096), as three
+// free :1141-1197) for power-of-two domains (sides 64..8192), as three
 // passes over caller buffers:
 //
 //   k_op_row_fwd  row pairs (2p, 2p+1) with rows < in_rows: one complex
@@ -90,10 +90,20 @@
 #define CM_ROW_LR_F64 3
 #endif
 
+// default log2 elements per thread of the row passes: FP64 transforms of
+// length 2^13 take 16 elements per thread (512 threads a sequence)
+template <typename R>
+constexpr int row_lr(int logn) {
+  return sizeof(R) == 8 ? (logn >= 13 ? 4 : CM_ROW_LR_F64) : CM_ROW_LR_F32;
+}
+
 // threads of one block of the row passes for transform length 2^LOGN with
-// 2^LRV elements per thread
-template <typename R, int LOGN, int LRV = (sizeof(R) == 8 ? CM_ROW_LR_F64 : CM_ROW_LR_F32)>
+// 2^LRV elements per thread.  ONEBUF: the ping-pong buffers and the staged
+// twiddles do not fit a block's shared memory (FP64 at 2^13), so the
+// transform runs on one buffer with the twiddles read from global memory.
+template <typename R, int LOGN, int LRV = row_lr<R>(LOGN)>
 struct OpShape {
+  typedef typename CT<R>::C C;
   static constexpr int N = 1 << LOGN;
   static constexpr int LR = LRV;
   static constexpr int E = 1 << LR;  // elements per thread
@@ -101,10 +111,15 @@ struct OpShape {
   static constexpr int BASE = (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // row pairs per block
-  static constexpr int MINB = sizeof(R) == 8 ? CM_FP64_ROW_MINB : CM_ROW_F32_MINB;
-  static size_t smem() {
-    return (size_t)(N + 2 * smem_padded(NP * N)) * sizeof(typename CT<R>::C);
-  }
+  static constexpr size_t BUF = (size_t)(NP * N + ((NP * N) >> 3) + 1) * sizeof(C);
+  static constexpr bool ONEBUF = (N * sizeof(C) + 2 * BUF) > CM_SMEM_DYN_MAX;
+  static constexpr size_t SMEM = ONEBUF ? BUF : N * sizeof(C) + 2 * BUF;
+  static constexpr size_t STAGE = ONEBUF ? BUF : 2 * BUF;  // bytes for staging input rows
+  // resident blocks per SM the kernels are compiled for; one when a block
+  // holds more than half of the shared memory
+  static constexpr int MINB = SMEM > CM_SMEM_DYN_MAX / 2 ? 1
+                              : sizeof(R) == 8 ? CM_FP64_ROW_MINB : CM_ROW_F32_MINB;
+  static size_t smem() { return SMEM; }
 };
 
 // Column pass for columns of length 2^LOGX: 16 elements per thread, groups of
@@ -128,7 +143,12 @@ struct ColShape {
   static constexpr int GROUP = W * TPS;
   static constexpr int THREADS = GROUP > CM_COL_BASE ? GROUP : CM_COL_BASE;
   static constexpr int NG = THREADS / GROUP;  // column groups per block
-  static size_t smem() { return (size_t)(NX + 2 * smem_padded(NG * NX * W)) * sizeof(C); }
+  static constexpr size_t BUF = (size_t)(NG * NX * W + ((NG * NX * W) >> 3) + 1) * sizeof(C);
+  // one buffer and global twiddles when even one column's ping-pong buffers
+  // do not fit (FP64 at 2^13)
+  static constexpr bool ONEBUF = NX * sizeof(C) + 2 * BUF > CM_SMEM_DYN_MAX;
+  static constexpr size_t SMEM = ONEBUF ? BUF : NX * sizeof(C) + 2 * BUF;
+  static size_t smem() { return SMEM; }
 };
 
 template <typename R, int LOGN>
@@ -140,10 +160,11 @@ k_op_row_fwd(OpArgs<R> a) {
   constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
+  C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
+  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
+  const C* tw = Sh::ONEBUF ? a.twy : tws;
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
@@ -161,7 +182,7 @@ k_op_row_fwd(OpArgs<R> a) {
       }
       v[q] = cmake<C>(ra, rb);
     }
-    fft_p2r<C, false, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
+    fft_p2x<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (p < npairs) {
       C* __restrict__ row = a.spec + (size_t)p * N + tt;
 #pragma unroll
@@ -240,10 +261,11 @@ k_op_col(OpArgs<R> a) {
   constexpr int NX = P::N, W = Sh::W, LW = Sh::LW, E = Sh::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + NX;
+  C* bufA = Sh::ONEBUF ? tws : tws + NX;
   C* bufB = bufA + smem_padded(Sh::NG * NX * W);
   pdl_trigger();
-  stage_tw_p2r<LOGX, Sh::LR>(tws, a.twx);
+  if (!Sh::ONEBUF) stage_tw_p2r<LOGX, Sh::LR>(tws, a.twx);
+  const C* tw = Sh::ONEBUF ? a.twx : tws;
   pdl_wait();
   if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   __syncthreads();
@@ -261,14 +283,24 @@ k_op_col(OpArgs<R> a) {
     const int km = (ny - k) & (ny - 1);
     C v[E];
     col_split_load<C, P::TPS, E>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
-    fft_p2r<C, false, LOGX, Sh::LR>(v, bufA, bufB, base, W, tt, tws);
+    fft_p2x<C, false, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
+    if (a.fwd_real) {
+      // forward transform only: the real part of the 2D transform, in the
+      // natural (nx, ny/2 + 1) layout (a real, even kernel's Green's table)
+      if (ok) {
+#pragma unroll
+        for (int q = 0; q < E; ++q) a.fwd_real[(size_t)(tt + q * P::TPS) * units + k] = v[q].x;
+      }
+      __syncthreads();
+      continue;
+    }
     const R* __restrict__ tb =
         a.tab + ((size_t)(k >> tlw) * NX << tlw) + (k & (tW - 1)) + ((size_t)tt << tlw);
 #pragma unroll
     for (int q = 0; q < E; ++q)
       v[q] = cscale(v[q], ok ? __ldg(tb + ((size_t)(q * P::TPS) << tlw)) : (R)0);
     __syncthreads();
-    fft_p2r<C, true, LOGX, Sh::LR>(v, bufA, bufB, base, W, tt, tws);
+    fft_p2x<C, true, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
     col_pack_store<C, P::TPS, W, E>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
     __syncthreads();  // buffers free for the next group
   }
@@ -283,10 +315,11 @@ k_op_row_inv(OpArgs<R> a) {
   constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* bufA = tws + N;
+  C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
+  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
+  const C* tw = Sh::ONEBUF ? a.twy : tws;
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
@@ -297,7 +330,7 @@ k_op_row_inv(OpArgs<R> a) {
     const C* __restrict__ row = a.spec + (size_t)p * N + tt;
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = p < npairs ? row[q * P::TPS] : czero<C>();
-    fft_p2r<C, true, LOGN, Sh::LR>(v, bufA, bufB, s * N, 1, tt, tws);
+    fft_p2x<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;

@@ -103,6 +103,7 @@ static std::vector<C> make_twiddles(int n) {
 }
 
 struct Tiles {
+  bool generic_ok;                  // the per-pass kernels fit (else only the by-value passes)
   int row_tile, col_tile, lw, comp_rows;
   int threads_row, threads_col;
   bool p2;                          // both sides 2^6..2^12: specialised transforms
@@ -120,7 +121,9 @@ static int pow2_threads(size_t work) {
 
 // Tile shapes: a row tile holds `row_tile` real rows (packed in pairs), a
 // column tile `col_tile` = 2^lw half-spectrum columns.  Shared memory holds
-// the twiddles of the transform plus two ping-pong buffers.
+// the twiddles of the transform plus two ping-pong buffers; when a sequence
+// and its buffers do not fit (FP64 sides of 8192), generic_ok is false and
+// only the power-of-two by-value passes can serve the plan.
 static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, Tiles* t) {
   // 2048 transform elements per tile: 256 threads for the register-resident
   // transforms, so two blocks share an SM and overlap memory with compute
@@ -128,14 +131,14 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   int np = (int)std::max<size_t>(1, elems / (size_t)ny);
   np = std::min(np, (nx + 1) / 2);
   const size_t srow = (2 * (size_t)np * ny + ny) * csize;
-  if (srow > CM_SMEM_DYN_MAX) return CM_ERR_SIZE;
+  t->generic_ok = srow <= CM_SMEM_DYN_MAX;
   t->row_tile = 2 * np;
   t->smem_row = srow;
   t->threads_row = pow2_threads((size_t)np * ny);
   int lw = 0;
   while ((2ul << lw) * (size_t)nx <= elems && (1 << (lw + 1)) <= nyh) ++lw;
   const size_t scol = (2 * ((size_t)1 << lw) * nx + nx) * csize;
-  if (scol > CM_SMEM_DYN_MAX) return CM_ERR_SIZE;
+  t->generic_ok = t->generic_ok && scol <= CM_SMEM_DYN_MAX;
   t->lw = lw;
   t->col_tile = 1 << lw;
   t->smem_col = scol;
@@ -715,6 +718,7 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
       if (rc > 0) return CM_ERR_CUDA;
       w.by_value = rc == 0;
     }
+    if (!w.by_value && !w.tiles.generic_ok) return CM_ERR_SIZE;
     if (w.by_value) {
       // the element-wise passes walk the solve's tiles with at most one
       // resident wave of blocks (one reduction partial per block)
@@ -788,6 +792,7 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
       a.twy = hs.twy;
       a.st = nullptr;
       a.cg_only = 0;
+      a.fwd_real = nullptr;
       const int rc = op_p2_apply<R>(a, lx, ly, s);
       if (rc == 0) {
         g_launches += 3;
@@ -796,6 +801,7 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
       if (rc > 0) return CM_ERR_CUDA;
     }
   }
+  if (!w.tiles.generic_ok) return CM_ERR_SIZE;  // only the by-value passes fit this domain
   CK(cudaMemcpyAsync(w.d_plain, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
   const int nt_in = (in_rows + hs.row_tile - 1) / hs.row_tile;
   const int nt_out = (out_rows + hs.row_tile - 1) / hs.row_tile;
@@ -810,6 +816,37 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
   }
   CK(cudaGetLastError());
   return CM_OK;
+}
+
+// G = Re FFT2(in) of a real FP64 domain field in the natural (nx, nyh) layout,
+// by the power-of-two row pass and a forward-only column pass; -1 when the
+// domain has no power-of-two passes
+static int forward_real_p2(cm_plan* p, const double* in, double* out, cudaStream_t s) {
+  const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+  if (!(lx > 0 && ly > 0 && op_p2_supported<double>(lx, ly, p->w64.tiles.lw))) return -1;
+  set_smem_attrs<double>();
+  OpArgs<double> a;
+  memset(&a, 0, sizeof(a));
+  a.in = in;
+  a.in_rows = p->nx;
+  a.in_cols = p->ny;
+  a.in_ld = p->ny;
+  a.out_rows = p->nx;
+  a.out_cols = p->ny;
+  a.out_ld = p->ny;
+  a.nx = p->nx;
+  a.nyh = p->nyh;
+  a.lw = p->w64.tiles.lw;
+  a.ny = p->ny;
+  a.ntile_cols = p->w64.tiles.ntile_cols;
+  a.spec = p->w64.spec;
+  a.tab = p->w64.tab[0];
+  a.twx = p->w64.twx;
+  a.twy = p->w64.twy;
+  a.fwd_real = out;
+  const int rc = op_p2_fwd_real<double>(a, lx, ly, s);
+  if (rc == 0) g_launches += 2;
+  return rc > 0 ? CM_ERR_CUDA : rc;
 }
 
 static int apply_dispatch(cm_plan* p, int op, int precision, const void* in, int in_rows, int in_cols,
@@ -1171,6 +1208,8 @@ template <typename R>
 static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_t s) {
   std::vector<Slot<R>> hs(n);
   std::vector<int2> it[4];
+  for (int i = 0; i < n; ++i)
+    if (!work_of<R>(plans[i]).tiles.generic_ok) return CM_ERR_SIZE;  // single-solve passes only
   for (int i = 0; i < n; ++i) {
     Work<R>& w = work_of<R>(plans[i]);
     hs[i] = base_slot(plans[i], w);
@@ -1633,10 +1672,17 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
         cudaSuccess)
       return fail(CM_ERR_CUDA);
     k_love_expand<<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(love, quad, key.qy, p->nx, p->ny);
-    rc = launch_plain<double>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
-                                         0, 0, s);
-    if (rc != CM_OK) return fail(rc);
-    k_real_part<<<grid_for(nh), 256, 0, s>>>(p->w64.spec, p->G, p->nx, p->nyh, p->w64.tiles.lw);
+    // its transform: the power-of-two passes where the domain has them, else
+    // the per-pass kernels
+    rc = forward_real_p2(p, love, p->G, s);
+    if (rc < 0) {
+      rc = launch_plain<double>(p, p->w64, MODE_FWD, 0, love, p->nx, p->ny, p->ny, nullptr, 0,
+                                0, 0, s);
+      if (rc != CM_OK) return fail(rc);
+      k_real_part<<<grid_for(nh), 256, 0, s>>>(p->w64.spec, p->G, p->nx, p->nyh, p->w64.tiles.lw);
+    } else if (rc != CM_OK) {
+      return fail(rc);
+    }
   }
   const double area = (desc->sx / p->tx) * (desc->sy / p->ty);
   const double N = (double)p->nx * (double)p->ny;
@@ -1888,6 +1934,9 @@ int cm_ccg_begin(cm_stepper* stp, cm_plan* p, const cm_ccg_params* prm, const do
   if (prm->precision != CM_FP64 && prm->precision != CM_FP32 && prm->precision != CM_MIXED) return CM_ERR_ARG;
   if (prm->has_hardness && !(prm->hardness > 0)) return CM_ERR_ARG;
   if (p->phase != 0) return CM_ERR_ARG;  // the plan already holds a solve
+  // steps run the per-pass kernels, which must fit the domain
+  if (!p->w64.tiles.generic_ok || (prm->precision != CM_FP64 && !p->w32.tiles.generic_ok))
+    return CM_ERR_SIZE;
   p->params = *prm;
   p->phase_prec = prm->precision;
   p->nit32 = p->nfev32 = 0;
