@@ -392,30 +392,54 @@ def c3_problems(n=C3_N):
 
 
 def run_batched(fp64_subset=48):
-    """Mixed-precision batched solves/s of the 512-solve configuration, the
-    plain FP64 single-solve path on a subset of the same solves, and the
-    largest relative displacement difference between the two on that subset."""
+    """Mixed-precision batched solves/s of the 512-solve configuration, under
+    the library's default launch shapes and under the autotuner's table
+    (Autotune: tile sizes per side, block threads), the plain FP64
+    single-solve path on a subset of the same solves, and the largest
+    relative displacement difference between the two on that subset."""
     import torch
     import contactmechanics_b200 as cm
+    from contactmechanics_b200 import Autotune
     probs = c3_problems()
-    subs = [cm.PeriodicFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0)) for nb, _, _ in probs]
     hs = [torch.from_numpy(h).cuda() for _, h, _ in probs]
     F = [p for _, _, p in probs]
     PT = [1e-9 * float(h.max() - h.min()) for _, h, _ in probs]
     FT = [1e-12 * p for p in F]
 
-    def batch():
-        return cm.constrained_conjugate_gradients_batch(subs, hs, external_force=F, pentol=PT,
-                                                        forcetol=FT, precision="mixed")
-    batch()  # warm-up: allocations, graphs
-    torch.cuda.synchronize()
+    def make_subs():
+        # plans are created under the tuning in force
+        return [cm.PeriodicFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0)) for nb, _, _ in probs]
+
+    def timed_batch(subs):
+        def batch():
+            return cm.constrained_conjugate_gradients_batch(subs, hs, external_force=F, pentol=PT,
+                                                            forcetol=FT, precision="mixed")
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = batch()
+        e1.record()
+        e1.synchronize()
+        assert all(r.success for r in res)
+        return res, e0.elapsed_time(e1)
+
+    Autotune.clear()
+    subs_default = make_subs()
+    tuned = Autotune.load() if os.path.exists(Autotune.DEFAULT_TABLE) else None
+    if tuned is not None:
+        Autotune.apply(tuned)
+    subs = make_subs()
+    # one warm-up (allocations, graphs) of each, then alternating timed
+    # batches, best of two each
+    timed_batch(subs_default)
+    timed_batch(subs)
+    ms_default, ms_batch, res = float("inf"), float("inf"), None
+    for _ in range(2):
+        ms_default = min(ms_default, timed_batch(subs_default)[1])
+        r, ms = timed_batch(subs)
+        if ms < ms_batch:
+            res, ms_batch = r, ms
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    res = batch()
-    e1.record()
-    e1.synchronize()
-    ms_batch = e0.elapsed_time(e1)
-    assert all(r.success for r in res)
     idx = list(range(0, C3_N, C3_N // fp64_subset))[:fp64_subset]
     for i in idx[:4]:  # warm-up of the single-solve path
         cm.constrained_conjugate_gradients(subs[i], hs[i], external_force=F[i], pentol=PT[i],
@@ -436,6 +460,8 @@ def run_batched(fp64_subset=48):
     single_rate = len(idx) / (ms_single / 1e3)
     return {"workload": C3_WORKLOAD, "solves": C3_N,
             "mixed_batched_solves_per_s": batched, "ms_batch": ms_batch,
+            "default_shapes_solves_per_s": C3_N / (ms_default / 1e3),
+            "tuned_shapes": {k: tuned[k] for k in ("tiles", "threads")} if tuned else None,
             "fp64_single_solve_solves_per_s": single_rate,
             "fp64_single_solve_sample": f"{len(idx)} of the 512 solves (every {C3_N // fp64_subset}th)",
             "speedup_vs_fp64_single": batched / single_rate, "rel_err_vs_fp64_max": max(errs),

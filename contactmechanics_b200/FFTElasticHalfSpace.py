@@ -35,6 +35,9 @@ class _Plan:
     def __init__(self, desc):
         L = _lib.lib()
         self._L = L
+        # the launch shapes the package's autotuner measured for this GPU
+        from .Autotune import apply_default
+        apply_default()
         ptr = ctypes.c_void_p()
         _lib.check(L.cm_plan_create(ctypes.byref(desc), None, ctypes.byref(ptr)))
         self.ptr = ptr

@@ -119,6 +119,24 @@ static int pow2_threads(size_t work) {
   return (int)t;
 }
 
+// ---------------------------------------------------------------------------
+// tuning of the per-pass kernels (batched solves, stepping interface, sizes
+// without power-of-two passes): transform elements per row or column tile
+// by sequence length and precision, and the threads of a batched transform
+// launch; set through cm_tuning_* (the package's autotuner measures them)
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::vector<std::pair<int, int>> g_tune_elems[2];  // [FP64, FP32]: (length, elements)
+static int g_batch_threads[2] = {CM_THREADS, CM_THREADS};
+
+static int tuned_elems(size_t csize, int length, int dflt) {
+  const int pi = csize == 16 ? 0 : 1;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (const auto& e : g_tune_elems[pi])
+    if (e.first == length) return e.second;
+  return dflt;
+}
+
 // Tile shapes: a row tile holds `row_tile` real rows (packed in pairs), a
 // column tile `col_tile` = 2^lw half-spectrum columns.  Shared memory holds
 // the twiddles of the transform plus two ping-pong buffers; when a sequence
@@ -127,8 +145,11 @@ static int pow2_threads(size_t work) {
 static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, Tiles* t) {
   // 2048 transform elements per tile: 256 threads for the register-resident
   // transforms, so two blocks share an SM and overlap memory with compute
-  const size_t elems = std::min<size_t>(CM_SMEM_ROW / (2 * csize), 2048);
-  int np = (int)std::max<size_t>(1, elems / (size_t)ny);
+  const size_t elems_max = CM_SMEM_ROW / (2 * csize);
+  const size_t elems = std::min<size_t>(elems_max, 2048);
+  const size_t relems = std::min<size_t>(std::max(tuned_elems(csize, ny, (int)elems), 1), elems_max);
+  const size_t celems = std::min<size_t>(std::max(tuned_elems(csize, nx, (int)elems), 1), elems_max);
+  int np = (int)std::max<size_t>(1, relems / (size_t)ny);
   np = std::min(np, (nx + 1) / 2);
   const size_t srow = (2 * (size_t)np * ny + ny) * csize;
   t->generic_ok = srow <= CM_SMEM_DYN_MAX;
@@ -136,7 +157,7 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   t->smem_row = srow;
   t->threads_row = pow2_threads((size_t)np * ny);
   int lw = 0;
-  while ((2ul << lw) * (size_t)nx <= elems && (1 << (lw + 1)) <= nyh) ++lw;
+  while ((2ul << lw) * (size_t)nx <= celems && (1 << (lw + 1)) <= nyh) ++lw;
   const size_t scol = (2 * ((size_t)1 << lw) * nx + nx) * csize;
   t->generic_ok = t->generic_ok && scol <= CM_SMEM_DYN_MAX;
   t->lw = lw;
@@ -1242,18 +1263,19 @@ static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_
 template <typename R>
 static void launch_iteration_batch(const BatchDev<R>& b, bool bisect, cudaStream_t s) {
   const Slot<R>* S = b.slots;
+  const int TT = g_batch_threads[sizeof(R) == 8 ? 0 : 1];  // threads of the transform launches
   k_ccg_begin<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
   if (bisect)
     for (int i = 0; i < CM_BISECT_PASSES; ++i)
       k_ccg_bisect<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
   k_ccg_gsum<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
-  k_row_fwd<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
-  k_col<R, MODE_T><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
-  k_row_inv<R, MODE_T><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
+  k_row_fwd<R, MODE_T><<<b.n_items[1], TT, b.smem_row, s>>>(S, b.items[1]);
+  k_col<R, MODE_T><<<b.n_items[3], TT, b.smem_col, s>>>(S, b.items[3]);
+  k_row_inv<R, MODE_T><<<b.n_items[1], TT, b.smem_row, s>>>(S, b.items[1]);
   k_ccg_update<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], 0);
-  k_row_fwd<R, MODE_F><<<b.n_items[1], CM_THREADS, b.smem_row, s>>>(S, b.items[1]);
-  k_col<R, MODE_F><<<b.n_items[3], CM_THREADS, b.smem_col, s>>>(S, b.items[3]);
-  k_row_inv<R, MODE_F><<<b.n_items[2], CM_THREADS, b.smem_row, s>>>(S, b.items[2]);
+  k_row_fwd<R, MODE_F><<<b.n_items[1], TT, b.smem_row, s>>>(S, b.items[1]);
+  k_col<R, MODE_F><<<b.n_items[3], TT, b.smem_col, s>>>(S, b.items[3]);
+  k_row_inv<R, MODE_F><<<b.n_items[2], TT, b.smem_row, s>>>(S, b.items[2]);
 }
 
 // Run the CCG loop of every solve of the batch to completion.
@@ -2129,6 +2151,40 @@ int cm_kspace_dot(cm_plan* p, const double* ka, const double* kb, double* out, v
   double acc = 0.0;
   for (double v : part) acc += v;
   *out = acc / ((double)p->nx * (double)p->ny);
+  return CM_OK;
+}
+
+int cm_tuning_set_tiles(int precision, int length, int tile_elems) {
+  if ((precision != CM_FP64 && precision != CM_FP32) || length < 1 || tile_elems < 0) return CM_ERR_ARG;
+  const int pi = precision == CM_FP64 ? 0 : 1;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto& v = g_tune_elems[pi];
+  for (size_t i = 0; i < v.size(); ++i)
+    if (v[i].first == length) {
+      v.erase(v.begin() + i);
+      break;
+    }
+  if (tile_elems > 0) v.emplace_back(length, tile_elems);
+  return CM_OK;
+}
+
+int cm_tuning_set_batch_threads(int precision, int threads) {
+  if ((precision != CM_FP64 && precision != CM_FP32)) return CM_ERR_ARG;
+  if (threads < 32 || threads > CM_FFT_THREADS || (threads & 31)) return CM_ERR_ARG;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_batch_threads[precision == CM_FP64 ? 0 : 1] = threads;
+  return CM_OK;
+}
+
+int cm_tuning_get(int precision, int length, int* tile_elems, int* batch_threads) {
+  if ((precision != CM_FP64 && precision != CM_FP32) || length < 1) return CM_ERR_ARG;
+  const size_t csize = precision == CM_FP64 ? 16 : 8;
+  const int dflt = (int)std::min<size_t>(CM_SMEM_ROW / (2 * csize), 2048);
+  if (tile_elems) *tile_elems = tuned_elems(csize, length, dflt);
+  if (batch_threads) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    *batch_threads = g_batch_threads[precision == CM_FP64 ? 0 : 1];
+  }
   return CM_OK;
 }
 

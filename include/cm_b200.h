@@ -303,6 +303,23 @@ int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young
 int cm_selftest_grid_barrier(int blocks, int phantom, double limit_us, int* gave_up);
 
 /*
+ * Tuning of the per-pass kernels that batched solves (cm_ccg_solve_batch),
+ * the stepping interface and sizes without power-of-two passes run.
+ * cm_tuning_set_tiles: transform elements per row or column tile for
+ * sequences of `length` points (a row tile of a domain with ny columns holds
+ * tile_elems / ny rows, a column tile up to tile_elems / nx columns), for
+ * plans created afterwards; 0 restores the default (2048).
+ * cm_tuning_set_batch_threads: threads per block of the batched transform
+ * launches (a multiple of 32, at most 512; default 256).  cm_tuning_get
+ * reports the values in force.  The package's autotuner measures them and
+ * stores them as JSON.  No reference counterpart (the reference's transforms
+ * are muGrid's).
+ */
+int cm_tuning_set_tiles(int precision, int length, int tile_elems);
+int cm_tuning_set_batch_threads(int precision, int threads);
+int cm_tuning_get(int precision, int length, int* tile_elems, int* batch_threads);
+
+/*
  * Number of kernels this library has launched in the process (graph nodes
  * count once per replay).  Instrumentation; no reference counterpart.
  */

@@ -99,3 +99,22 @@ def test_batch_mixed_vs_oracle(cm):
         assert rel < 1e-6, rel
         a, ar = np.count_nonzero(rb.jac > 0), np.count_nonzero(ref["jac"] > 0)
         assert abs(a - ar) <= max(1, 1e-3 * ar)
+
+
+def test_batch_under_other_launch_shapes(cm):
+    """Batched results do not depend on the tuned tile sizes and block
+    threads beyond rounding: extreme choices still match the oracle."""
+    from contactmechanics_b200 import Autotune
+    try:
+        Autotune.apply({"tiles": {"fp64": {"64": 512, "96": 512, "128": 512}},
+                        "threads": {"fp64": 128}})
+        probs = [_problem(cm, c, 40 + i) for i, c in enumerate(CASES[:3])]  # plans under the shapes
+        res = _batch(cm, probs, "fp64")
+    finally:
+        Autotune.clear()
+        Autotune._applied = False
+        Autotune.apply_default()
+    for (sub, o, h, kw), r in zip(probs, res):
+        ref = oc.constrained_conjugate_gradients(o, h, **kw)
+        assert r.success and ref["success"]
+        np.testing.assert_allclose(r.x, ref["x"], rtol=0, atol=1e-10 * abs(ref["x"]).max())
