@@ -439,6 +439,15 @@ def run_batched(fp64_subset=48):
         r, ms = timed_batch(subs)
         if ms < ms_batch:
             res, ms_batch = r, ms
+    # the same batch in one launch of the persistent cluster kernel (opt-in)
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
+    try:
+        _lib.check(L.cm_tuning_set_batch_persistent(1))
+        timed_batch(subs)
+        ms_persistent = min(timed_batch(subs)[1] for _ in range(2))
+    finally:
+        L.cm_tuning_set_batch_persistent(0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     idx = list(range(0, C3_N, C3_N // fp64_subset))[:fp64_subset]
     for i in idx[:4]:  # warm-up of the single-solve path
@@ -461,6 +470,7 @@ def run_batched(fp64_subset=48):
     return {"workload": C3_WORKLOAD, "solves": C3_N,
             "mixed_batched_solves_per_s": batched, "ms_batch": ms_batch,
             "default_shapes_solves_per_s": C3_N / (ms_default / 1e3),
+            "persistent_kernel_solves_per_s": C3_N / (ms_persistent / 1e3),
             "tuned_shapes": {k: tuned[k] for k in ("tiles", "threads")} if tuned else None,
             "fp64_single_solve_solves_per_s": single_rate,
             "fp64_single_solve_sample": f"{len(idx)} of the 512 solves (every {C3_N // fp64_subset}th)",

@@ -33,8 +33,12 @@ _applied = False
 
 def apply(table):
     """Install a tuning table {"tiles": {prec: {length: elems}}, "threads":
-    {prec: threads}} for plans created afterwards."""
+    {prec: threads}, "batch_persistent": bool} for plans created afterwards
+    ("batch_persistent" selects the persistent cluster kernel for elastic
+    batches instead of the lockstep graph)."""
     L = _lib.load_library()
+    if "batch_persistent" in table:
+        _lib.check(L.cm_tuning_set_batch_persistent(int(bool(table["batch_persistent"]))))
     for prec, tiles in table.get("tiles", {}).items():
         for length, elems in tiles.items():
             _lib.check(L.cm_tuning_set_tiles(_lib.PRECISIONS[prec], int(length), int(elems)))
@@ -45,6 +49,7 @@ def apply(table):
 def clear(lengths=SIDES):
     """Back to the library's defaults."""
     L = _lib.load_library()
+    _lib.check(L.cm_tuning_set_batch_persistent(0))
     for prec in ("fp32", "fp64"):
         for n in lengths:
             _lib.check(L.cm_tuning_set_tiles(_lib.PRECISIONS[prec], int(n), 0))

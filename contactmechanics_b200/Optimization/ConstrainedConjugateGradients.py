@@ -347,17 +347,21 @@ def constrained_conjugate_gradients_batch(substrates, topographies, hardness=Non
         result.timing = {"ms_fp32": r.ms_fp32, "ms_fp64": r.ms_fp64, "ms_total": r.ms_total,
                          "polls": r.polls}
         sub = substrates[i]
-        act_dom = torch.zeros(tuple(sub.nb_domain_grid_pts), dtype=torch.bool, device="cuda")
-        nb = sub.nb_grid_pts
-        act_dom[:nb[0], :nb[1]] = acts[i].bool()
+        nb, dom = tuple(sub.nb_grid_pts), tuple(sub.nb_domain_grid_pts)
+        act = acts[i].view(torch.bool)  # the library writes 0/1 bytes
+        if dom == nb:
+            act_dom = act
+        else:
+            act_dom = torch.zeros(dom, dtype=torch.bool, device="cuda")
+            act_dom[:nb[0], :nb[1]] = act
         if as_torch[i]:
             result.x, result.jac, result.active_set = xs[i], jacs[i], act_dom
             if pls[i] is not None and result.success:
-                result.plastic = pls[i].bool()
+                result.plastic = pls[i].view(torch.bool)
         else:
             result.x, result.jac = xs[i].cpu().numpy(), jacs[i].cpu().numpy()
             result.active_set = act_dom.cpu().numpy()
             if pls[i] is not None and result.success:
-                result.plastic = pls[i].bool().cpu().numpy()
+                result.plastic = pls[i].view(torch.bool).cpu().numpy()
         out.append(result)
     return out

@@ -105,6 +105,7 @@ SIGNATURES = {
     "cm_tuning_set_tiles": (_i, [_i, _i, _i]),
     "cm_tuning_set_batch_threads": (_i, [_i, _i]),
     "cm_tuning_get": (_i, [_i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "cm_tuning_set_batch_persistent": (_i, [_i]),
     "cm_fft_forward": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp]),
     "cm_kspace_apply": (_i, [_vp, _i, ctypes.c_double, _vp, _vp, _vp]),
     "cm_kspace_dot": (_i, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]),

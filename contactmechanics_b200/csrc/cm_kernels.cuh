@@ -322,33 +322,30 @@ CM_DEVINL void fin_force(CcgState& s, double (&a)[2]) {
 // ---------------------------------------------------------------------------
 // operator passes
 // ---------------------------------------------------------------------------
+// Loads of fields that other blocks of the same launch may have written
+// (the persistent batch kernel runs every pass of a solve in one launch)
+// bypass L1; tables and twiddles are constant and read through it.
+template <typename T> CM_DEVINL T ldf(const T* p) { return __ldcg(p); }
+
+// Row tile `tile` of the forward pass: the tile's rows of the field (the
+// caller's buffer, or the CCG prologue's search direction / final force),
+// packed-pair FFTs along y, half spectrum to the column-tile layout.  fd /
+// tws hold the staged descriptor and twiddles of length ny; buf and scratch
+// row_tile/2 * ny elements each.  acc / amax collect this thread's share of
+// the tile's sums (MODE_T: sum g t over the CG set; MODE_F: sum f, max |f|).
 template <typename R, int MODE>
-__global__ void __launch_bounds__(CM_FFT_THREADS)
-k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+CM_DEVINL void row_fwd_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, int tile,
+                            const FftDesc& fd, const typename CT<R>::C* tws,
+                            typename CT<R>::C* buf, typename CT<R>::C* scratch, double& acc,
+                            double& amax) {
   typedef typename CT<R>::C C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc fd;
-  const int2 item = items[blockIdx.x];
-  const Slot<R>* __restrict__ Sp = slots + item.x;
-  CcgState* st = Sp->st;
-  CcgView cv{};
-  if (MODE == MODE_T || MODE == MODE_F) {
-    if (st->done) return;
-    if (MODE == MODE_T && st->branch != 0) return;
-    load_view(st, cv);
-  }
   const int nx = Sp->nx, ny = Sp->ny, nyh = Sp->nyh, ty = Sp->ty, lw = Sp->lw;
   const int rows_total = (MODE == MODE_PLAIN || MODE == MODE_FWD) ? Sp->in_rows : Sp->tx;
   const int row_tile = Sp->row_tile;
-  const int x0 = item.y * row_tile;
+  const int x0 = tile * row_tile;
   const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* buf = tws + ny;
-  C* scratch = buf + (row_tile >> 1) * ny;
-  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
   C* __restrict__ spec = Sp->spec;
-  double acc = 0.0, amax = 0.0;
 
   if (MODE == MODE_PLAIN || MODE == MODE_FWD) {
     const R* __restrict__ in = Sp->in;
@@ -358,8 +355,8 @@ k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
       const int xa = x0 + 2 * p;
       R va = 0, vb = 0;
       if (y < in_cols) {
-        va = in[(size_t)xa * in_ld + y];
-        if (xa + 1 < x0 + nrows) vb = in[(size_t)(xa + 1) * in_ld + y];
+        va = ldf(in + (size_t)xa * in_ld + y);
+        if (xa + 1 < x0 + nrows) vb = ldf(in + (size_t)(xa + 1) * in_ld + y);
       }
       return cmake<C>(va, vb);
     }, [&](int e, C v) { buf[e] = v; });
@@ -379,12 +376,12 @@ k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
         v.f[w] = 0; v.u[w] = 0; v.h[w] = 0; v.t[w] = 0;
         if (x < x0 + nrows && y < ty) {
           const size_t ic = (size_t)x * ty + y;
-          v.f[w] = fio[ic];
+          v.f[w] = ldf(fio + ic);
           if (MODE == MODE_T || cv.apply_nc) {
-            v.u[w] = u[(size_t)x * ny + y];
-            v.h[w] = h[ic];
+            v.u[w] = ldf(u + (size_t)x * ny + y);
+            v.h[w] = ldf(h + ic);
           }
-          if (MODE == MODE_T) v.t[w] = t[ic];
+          if (MODE == MODE_T) v.t[w] = ldf(t + ic);
         }
       }
       return v;
@@ -439,6 +436,30 @@ k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
     if (xa + 1 < x0 + nrows)
       spec[spec_at(xa + 1, k, nx, lw)] = cmake<C>((z.y + zm.y) * (R)0.5, (zm.x - z.x) * (R)0.5);
   }
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
+k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  typedef typename CT<R>::C C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
+  const int2 item = items[blockIdx.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  CcgView cv{};
+  if (MODE == MODE_T || MODE == MODE_F) {
+    if (st->done) return;
+    if (MODE == MODE_T && st->branch != 0) return;
+    load_view(st, cv);
+  }
+  const int ny = Sp->ny;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + ny;
+  C* scratch = buf + (Sp->row_tile >> 1) * ny;
+  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
+  double acc = 0.0, amax = 0.0;
+  row_fwd_tile<R, MODE>(Sp, cv, item.y, fd, tws, buf, scratch, acc, amax);
   if (MODE == MODE_T) {
     double v[1] = {acc};
     const int kinds[1] = {RED_SUM};
@@ -452,22 +473,17 @@ k_row_fwd(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   }
 }
 
+// Column tile `tile` (spectrum columns tile*W .. tile*W + W): FFT along x,
+// multiply by the Green's table, inverse FFT along x.  fd / tws: staged
+// descriptor and twiddles of length nx; buf and scratch nx * W elements each.
 template <typename R, int MODE>
-__global__ void __launch_bounds__(CM_FFT_THREADS)
-k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+CM_DEVINL void col_tile(const Slot<R>* __restrict__ Sp, int tile, const FftDesc& fd,
+                        const typename CT<R>::C* tws, typename CT<R>::C* buf,
+                        typename CT<R>::C* scratch) {
   typedef typename CT<R>::C C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc fd;
-  const int2 item = items[blockIdx.x];
-  const Slot<R>* __restrict__ Sp = slots + item.x;
-  if (MODE == MODE_T || MODE == MODE_F) {
-    const CcgState* st = Sp->st;
-    if (st->done) return;
-    if (MODE == MODE_T && st->branch != 0) return;
-  }
   const int nx = Sp->nx, nyh = Sp->nyh, lw = Sp->lw;
   const int W = 1 << lw;
-  const int k0 = item.y * W;
+  const int k0 = tile * W;
   const int wc = min(W, nyh - k0);
   int nx_in, nx_out;
   const R* __restrict__ tab;
@@ -480,21 +496,17 @@ k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
     nx_out = (MODE == MODE_T) ? Sp->tx : nx;
     tab = Sp->tab[0];
   }
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* buf = tws + nx;
-  C* scratch = buf + nx * W;
-  stage_fft(fd, Sp->fx, tws, Sp->twx, nx);
   // the tile is one contiguous block of nx * W elements in HBM
-  C* __restrict__ blk = Sp->spec + (size_t)item.y * nx * W;
-  const R* __restrict__ tblk = tab + (size_t)item.y * nx * W;
+  C* __restrict__ blk = Sp->spec + (size_t)tile * nx * W;
+  const R* __restrict__ tblk = tab + (size_t)tile * nx * W;
   const int total = nx * wc;
   if (wc == W) {
-    batched_loop<8>(nx_in * W, [&](int e) { return blk[e]; }, [&](int e, C v) { buf[e] = v; });
+    batched_loop<8>(nx_in * W, [&](int e) { return ldf(blk + e); }, [&](int e, C v) { buf[e] = v; });
     for (int e = nx_in * W + threadIdx.x; e < total; e += blockDim.x) buf[e] = czero<C>();
   } else {
     batched_loop<8>(total, [&](int e) {
       const int x = e / wc, c = e - x * wc;
-      return (x < nx_in) ? blk[x * W + c] : czero<C>();
+      return (x < nx_in) ? ldf(blk + x * W + c) : czero<C>();
     }, [&](int e, C v) { buf[e] = v; });
   }
   __syncthreads();
@@ -515,6 +527,27 @@ k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
       blk[x * W + c] = res[e];
     }
   }
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
+k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  typedef typename CT<R>::C C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
+  const int2 item = items[blockIdx.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  if (MODE == MODE_T || MODE == MODE_F) {
+    const CcgState* st = Sp->st;
+    if (st->done) return;
+    if (MODE == MODE_T && st->branch != 0) return;
+  }
+  const int nx = Sp->nx;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + nx;
+  C* scratch = buf + nx * (1 << Sp->lw);
+  stage_fft(fd, Sp->fx, tws, Sp->twx, nx);
+  col_tile<R, MODE>(Sp, item.y, fd, tws, buf, scratch);
 }
 
 // Convergence test at the end of an iteration (ConstrainedConjugateGradients.py
@@ -558,39 +591,30 @@ CM_DEVINL void ccg_converge(CcgState& s, double maxdu_in, double maxpen_in) {
   }
 }
 
+// Row tile `tile` of the inverse pass: half spectrum -> real rows, then the
+// caller's buffer, or the CCG epilogue.  fd / tws / buf / scratch as for
+// row_fwd_tile.  a0 / a1 collect this thread's share of the tile's sums
+// (MODE_T: sum r t; MODE_F: max |du|, max penetration over the CG set).
 template <typename R, int MODE>
-__global__ void __launch_bounds__(CM_FFT_THREADS)
-k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, int tile,
+                            const FftDesc& fd, const typename CT<R>::C* tws,
+                            typename CT<R>::C* buf, typename CT<R>::C* scratch, double& a0,
+                            double& a1) {
   typedef typename CT<R>::C C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc fd;
-  const int2 item = items[blockIdx.x];
-  const Slot<R>* __restrict__ Sp = slots + item.x;
-  CcgState* st = Sp->st;
-  CcgView cv{};
-  if (MODE == MODE_T || MODE == MODE_F) {
-    if (st->done) return;
-    if (MODE == MODE_T && st->branch != 0) return;
-    load_view(st, cv);
-  }
   const int nx = Sp->nx, ny = Sp->ny, nyh = Sp->nyh, ty = Sp->ty, tx = Sp->tx, lw = Sp->lw;
   const int rows_total = (MODE == MODE_PLAIN) ? Sp->out_rows : (MODE == MODE_T ? tx : nx);
   const int row_tile = Sp->row_tile;
-  const int x0 = item.y * row_tile;
+  const int x0 = tile * row_tile;
   const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* buf = tws + ny;
-  C* scratch = buf + (row_tile >> 1) * ny;
-  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
   const C* __restrict__ spec = Sp->spec;
   struct XY { C X, Y; };
   batched_loop<4>(npairs * nyh, [&](int e) {
     const int p = e / nyh, k = e - p * nyh;
     const int xa = x0 + 2 * p;
     XY v;
-    v.X = spec[spec_at(xa, k, nx, lw)];
-    v.Y = (xa + 1 < x0 + nrows) ? spec[spec_at(xa + 1, k, nx, lw)] : czero<C>();
+    v.X = ldf(spec + spec_at(xa, k, nx, lw));
+    v.Y = (xa + 1 < x0 + nrows) ? ldf(spec + spec_at(xa + 1, k, nx, lw)) : czero<C>();
     return v;
   }, [&](int e, XY v) {
     const int p = e / nyh, k = e - p * nyh;
@@ -602,7 +626,6 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
   });
   __syncthreads();
   const C* res = fft_smem<C, true>(buf, scratch, fd, npairs, ny, 1, false, tws);
-  double a0 = 0.0, a1 = -INFINITY;  // MODE_T: sum r t ; MODE_F: max|du|, max penetration
   if (MODE == MODE_PLAIN) {
     R* __restrict__ out = Sp->out;
     const int out_cols = Sp->out_cols, out_ld = Sp->out_ld;
@@ -622,8 +645,8 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
       const int xa = x0 + 2 * p;
       T2 v{0, 0};
       if (y < ty) {
-        v.a = t[(size_t)xa * ty + y];
-        if (xa + 1 < x0 + nrows) v.b = t[(size_t)(xa + 1) * ty + y];
+        v.a = ldf(t + (size_t)xa * ty + y);
+        if (xa + 1 < x0 + nrows) v.b = ldf(t + (size_t)(xa + 1) * ty + y);
       }
       return v;
     }, [&](int e, T2 v) {
@@ -645,12 +668,12 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
         const int x = x0 + 2 * p + w;
         v.uo[w] = 0; v.fa[w] = 0; v.h[w] = 0; v.gn[w] = 0;
         if (x >= x0 + nrows) continue;
-        v.uo[w] = u[(size_t)x * ny + y];
+        v.uo[w] = ldf(u + (size_t)x * ny + y);
         if (x < tx && y < ty) {
           const size_t ic = (size_t)x * ty + y;
-          v.h[w] = h[ic];
-          if (cv.branch == 0) v.fa[w] = fa_buf[ic];
-          else v.gn[w] = gneg[ic];
+          v.h[w] = ldf(h + ic);
+          if (cv.branch == 0) v.fa[w] = ldf(fa_buf + ic);
+          else v.gn[w] = ldf(gneg + ic);
         }
       }
       return v;
@@ -674,6 +697,30 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
       }
     });
   }
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(CM_FFT_THREADS)
+k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  typedef typename CT<R>::C C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc fd;
+  const int2 item = items[blockIdx.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  CcgView cv{};
+  if (MODE == MODE_T || MODE == MODE_F) {
+    if (st->done) return;
+    if (MODE == MODE_T && st->branch != 0) return;
+    load_view(st, cv);
+  }
+  const int ny = Sp->ny;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* buf = tws + ny;
+  C* scratch = buf + (Sp->row_tile >> 1) * ny;
+  stage_fft(fd, Sp->fy, tws, Sp->twy, ny);
+  double a0 = 0.0, a1 = -INFINITY;  // MODE_T: sum r t ; MODE_F: max|du|, max penetration
+  row_inv_tile<R, MODE>(Sp, cv, item.y, fd, tws, buf, scratch, a0, a1);
   if (MODE == MODE_T) {
     double v[1] = {a0};
     const int kinds[1] = {RED_SUM};
@@ -732,6 +779,29 @@ struct EwTiles {
   }
 };
 
+// Start of an iteration over one comp tile: contact areas and raw-gap sums
+// (counts in int and extrema in R are exact; only the sum is FP64).
+template <typename R>
+CM_DEVINL void begin_tile(const Slot<R>* __restrict__ Sp, int tile, const R* __restrict__ f,
+                          int has_h, R hdn, int& a_c, int& a_cg, double& s_cg, R& gmax, R& gmin) {
+  struct V3 { R f, u, h; };
+  const CompTile<R> T(Sp, tile);
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V3{ldf(f + ic), ldf(T.u + iu), ldf(T.h + ic)};
+  }, [&](int, V3 v) {
+    const bool c0 = v.f < 0;
+    const bool c = c0 && (!has_h || v.f > hdn);
+    const R g = v.u - v.h;
+    a_c += c0;
+    a_cg += c;
+    if (c) s_cg += (double)g;
+    gmax = fmax(gmax, g);
+    gmin = fmin(gmin, g);
+  });
+}
+
 // Start of an iteration: contact areas, raw-gap sums, step kind and offset
 // (ConstrainedConjugateGradients.py:239-270, 300-318).
 template <typename R>
@@ -751,32 +821,35 @@ k_ccg_begin(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, i
   const int has_h = st->p.has_h;
   const R hdn = neg_down<R>(st->p.H);
   const R* __restrict__ f = (st->parity & 1) ? f1 : f0;
-  // counts in int and extrema in R are exact; only the sum is accumulated in FP64
   int a_c = 0, a_cg = 0;
   double s_cg = 0;
   R gmax = -INFINITY, gmin = INFINITY;
-  struct V3 { R f, u, h; };
-  for (int tile = W.first; tile < W.end; tile += W.step) {
-    const CompTile<R> T(Sp, tile);
-    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-      size_t ic, iu;
-      T.at(e, ic, iu);
-      return V3{f[ic], T.u[iu], T.h[ic]};
-    }, [&](int, V3 v) {
-      const bool c0 = v.f < 0;
-      const bool c = c0 && (!has_h || v.f > hdn);
-      const R g = v.u - v.h;
-      a_c += c0;
-      a_cg += c;
-      if (c) s_cg += (double)g;
-      gmax = fmax(gmax, g);
-      gmin = fmin(gmin, g);
-    });
-  }
+  for (int tile = W.first; tile < W.end; tile += W.step)
+    begin_tile<R>(Sp, tile, f, has_h, hdn, a_c, a_cg, s_cg, gmax, gmin);
   double v[5] = {(double)a_c, (double)a_cg, s_cg, (double)gmax, (double)gmin};
   const int kinds[5] = {RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
   tile_finish<5>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
                  [&](double (&a)[5]) { fin_begin(*st, a); });
+}
+
+// G over one comp tile: sum over the CG area of g^2.
+template <typename R>
+CM_DEVINL void gsum_tile(const Slot<R>* __restrict__ Sp, int tile, const R* __restrict__ f,
+                         int has_h, R hdn, R off, double& G) {
+  struct V3 { R f, u, h; };
+  const CompTile<R> T(Sp, tile);
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V3{ldf(f + ic), ldf(T.u + iu), ldf(T.h + ic)};
+  }, [&](int, V3 v) {
+    const bool c = (v.f < 0) && (!has_h || v.f > hdn);
+    const R g = (v.u - v.h) - off;
+    // the reference sums c * g^2 over the whole topography, so a NaN gap
+    // outside the contact set makes G NaN as well (0 * NaN)
+    if (c) G += (double)g * (double)g;
+    else if (isnan(g)) G += (double)g;
+  });
 }
 
 // G = sum over the CG area of g^2 and the conjugation factor (:273-279).
@@ -797,22 +870,7 @@ k_ccg_gsum(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, in
   const R off = (R)st->offset;
   const R* __restrict__ f = (st->parity & 1) ? f1 : f0;
   double G = 0;
-  struct V3 { R f, u, h; };
-  for (int tile = W.first; tile < W.end; tile += W.step) {
-    const CompTile<R> T(Sp, tile);
-    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-      size_t ic, iu;
-      T.at(e, ic, iu);
-      return V3{f[ic], T.u[iu], T.h[ic]};
-    }, [&](int, V3 v) {
-      const bool c = (v.f < 0) && (!has_h || v.f > hdn);
-      const R g = (v.u - v.h) - off;
-      // the reference sums c * g^2 over the whole topography, so a NaN gap
-      // outside the contact set makes G NaN as well (0 * NaN)
-      if (c) G += (double)g * (double)g;
-      else if (isnan(g)) G += (double)g;
-    });
-  }
+  for (int tile = W.first; tile < W.end; tile += W.step) gsum_tile<R>(Sp, tile, f, has_h, hdn, off, G);
   double v[1] = {G};
   const int kinds[1] = {RED_SUM};
   tile_finish<1>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
@@ -966,6 +1024,54 @@ k_ccg_bisect_passes(const Slot<R>* __restrict__ slots, const int2* __restrict__ 
   }
 }
 
+// Reduction values of the force update (counts in int and extrema in R are
+// exact: x -> (double)x + H is monotonic, so the minimum of fn + H is the
+// minimum fn plus H; only the sum is FP64).
+template <typename R>
+struct UpdateAcc {
+  int a_fl = 0, n_nc = 0;
+  R min_fn = INFINITY, max_t = 0;
+  double s_fp = 0;
+};
+
+// Force update and projection over one comp tile: f (start of the
+// iteration) -> fo.
+template <typename R>
+CM_DEVINL void update_tile(const Slot<R>* __restrict__ Sp, int tile, const R* __restrict__ f,
+                           R* __restrict__ fo, int has_h, int branch, double H, R hdn, R off,
+                           R tau, double mix, UpdateAcc<R>& A) {
+  const R* __restrict__ t = Sp->t;
+  unsigned char* __restrict__ gneg = Sp->gneg;
+  struct V4 { R f, u, h, t; };
+  const CompTile<R> T(Sp, tile);
+  batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    return V4{ldf(f + ic), ldf(T.u + iu), ldf(T.h + ic), branch == 0 ? ldf(t + ic) : (R)0};
+  }, [&](int e, V4 v) {
+    const size_t ic = (size_t)T.cx0 * T.ty + e;
+    const R fa = v.f;
+    const R g = (v.u - v.h) - off;
+    R fn;
+    if (branch == 0) {
+      const bool c = (fa < 0) && (!has_h || fa > hdn);
+      fn = c ? (R)(fa + tau * v.t) : fa;
+    } else {
+      fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
+    }
+    const bool tensile = fn >= 0;
+    const bool flowing = has_h && fn <= hdn;
+    const bool nc = (tensile && g < 0) || (flowing && g > 0);
+    if (tensile) A.max_t = fmax(A.max_t, fn);
+    if (flowing) { A.a_fl += 1; A.min_fn = fmin(A.min_fn, fn); }
+    const R fp = tensile ? (R)0 : fn;
+    A.s_fp += (double)fp;
+    A.n_nc += nc;
+    fo[ic] = fp;
+    if (has_h) gneg[ic] = g < 0;
+  });
+}
+
 // Force update, projection onto [0, H], constraint bookkeeping
 // (ConstrainedConjugateGradients.py:296, 320-389).
 template <typename R>
@@ -977,8 +1083,6 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, 
   const EwTiles W(item, strided, Sp->nt_comp);
   R* const f0 = Sp->f[0];
   R* const f1 = Sp->f[1];
-  const R* __restrict__ t = Sp->t;
-  unsigned char* __restrict__ gneg = Sp->gneg;
   pdl_trigger();
   pdl_wait();
   if (st->done) return;
@@ -990,43 +1094,120 @@ k_ccg_update(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, 
   const R* __restrict__ f = par ? f1 : f0;
   R* __restrict__ fo = par ? f0 : f1;
   const R hdn = neg_down<R>(H);
-  // counts in int and extrema in R are exact (x -> (double)x + H is monotonic,
-  // so the minimum of fn + H is the minimum fn plus H); only the sum is FP64
-  int a_fl = 0, n_nc = 0;
-  R min_fn = INFINITY, max_t = 0;
-  double s_fp = 0;
-  struct V4 { R f, u, h, t; };
-  for (int tile = W.first; tile < W.end; tile += W.step) {
-    const CompTile<R> T(Sp, tile);
-    batched_loop<sizeof(R) == 8 ? 4 : 8>(T.cn, [&](int e) {
-      size_t ic, iu;
-      T.at(e, ic, iu);
-      return V4{f[ic], T.u[iu], T.h[ic], branch == 0 ? t[ic] : (R)0};
-    }, [&](int e, V4 v) {
-      const size_t ic = (size_t)T.cx0 * T.ty + e;
-      const R fa = v.f;
-      const R g = (v.u - v.h) - off;
-      R fn;
-      if (branch == 0) {
-        const bool c = (fa < 0) && (!has_h || fa > hdn);
-        fn = c ? (R)(fa + tau * v.t) : fa;
-      } else {
-        fn = (R)((R)(1 - mix) * fa - (g < 0 ? (R)(mix * H) : (R)0));
-      }
-      const bool tensile = fn >= 0;
-      const bool flowing = has_h && fn <= hdn;
-      const bool nc = (tensile && g < 0) || (flowing && g > 0);
-      if (tensile) max_t = fmax(max_t, fn);
-      if (flowing) { a_fl += 1; min_fn = fmin(min_fn, fn); }
-      const R fp = tensile ? (R)0 : fn;
-      s_fp += (double)fp;
-      n_nc += nc;
-      fo[ic] = fp;
-      if (has_h) gneg[ic] = g < 0;
-    });
-  }
-  double v[5] = {(double)a_fl, (double)min_fn + H, (double)max_t, s_fp, (double)n_nc};
+  UpdateAcc<R> A;
+  for (int tile = W.first; tile < W.end; tile += W.step)
+    update_tile<R>(Sp, tile, f, fo, has_h, branch, H, hdn, off, tau, mix, A);
+  double v[5] = {(double)A.a_fl, (double)A.min_fn + H, (double)A.max_t, A.s_fp, (double)A.n_nc};
   const int kinds[5] = {RED_SUM, RED_MIN, RED_MAX, RED_SUM, RED_SUM};
   tile_finish<5>(Sp->partials, Sp->counter, W.part, W.nparts, v, kinds,
                  [&](double (&a)[5]) { fin_update(*st, a); });
+}
+
+// ---------------------------------------------------------------------------
+// solve preparation and results (per comp tile)
+// ---------------------------------------------------------------------------
+// heights -> working precision over one comp tile; max, min and sum of the
+// FP64 heights.
+template <typename R>
+CM_DEVINL void h_prep_tile(const Slot<R>* __restrict__ Sp, int tile, const double* __restrict__ h64,
+                           double& mx, double& mn, double& sm) {
+  const CompTile<R> T(Sp, tile);
+  R* __restrict__ h = const_cast<R*>(Sp->h);
+  const size_t base = (size_t)T.cx0 * T.ty;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    const double hv = h64[base + e];
+    h[base + e] = (R)hv;
+    mx = fmax(mx, hv);
+    mn = fmin(mn, hv);
+    sm += hv;
+  }
+}
+
+CM_DEVINL void fin_h_prep(CcgState& s, double (&a)[3]) {
+  s.p.max_surface = a[0];
+  s.gmin = a[1];  // scratch until the loop starts
+  s.sum_cg = a[2];
+}
+
+// sum of squared deviations from the mean height over one comp tile
+template <typename R>
+CM_DEVINL void h_var_tile(const Slot<R>* __restrict__ Sp, int tile, const double* __restrict__ h64,
+                          double mean, double& v2) {
+  const CompTile<R> T(Sp, tile);
+  const size_t base = (size_t)T.cx0 * T.ty;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    const double d = h64[base + e] - mean;
+    v2 += d * d;
+  }
+}
+
+// rms height and the reference's default penetration tolerance
+// (ConstrainedConjugateGradients.py:150-162); FP32 phases widen pentol.
+CM_DEVINL void fin_h_var(CcgState& s, double (&a)[1], int pentol_auto, double rel_pentol, int tx,
+                         int ty) {
+  if (pentol_auto) {
+    const double rms = sqrt(a[0] / s.p.n_surface);
+    double pt = rms / (10.0 * (0.5 * ((double)tx + (double)ty)));
+    if (pt == 0) pt = (s.p.offset0 + s.sum_cg / s.p.n_surface) / 1000;
+    if (pt == 0) pt = 1e-3;
+    s.p.pentol = pt;
+  }
+  if (rel_pentol > 0) s.p.pentol = fmax(s.p.pentol, rel_pentol * (s.p.max_surface - s.gmin));
+  s.gmin = 0;
+  s.sum_cg = 0;
+}
+
+// initial displacement at domain index i: given or zero, lifted onto the
+// surface on the topography region (ConstrainedConjugateGradients.py:168-201)
+template <typename R>
+CM_DEVINL void init_u_at(const Slot<R>& S, const double* __restrict__ u0, double offset, long i) {
+  const int x = (int)(i / S.ny), y = (int)(i % S.ny);
+  double u = u0 ? u0[i] : 0.0;
+  if (x < S.tx && y < S.ty) {
+    const double lo = (double)ldf(S.h + (size_t)x * S.ty + y) + offset;
+    u = (u < lo) ? lo : u;
+  }
+  S.u[i] = (R)u;
+}
+
+// result.jac, active_set, plastic over one comp tile, with the sums of the
+// elastic energy and the contact areas (ConstrainedConjugateGradients.py
+// :454-475, 494-509)
+template <typename R>
+CM_DEVINL void result_tile(const Slot<R>* __restrict__ Sp, int tile, int par, int has_h,
+                           int mixing, double H, double* jac, unsigned char* active,
+                           unsigned char* plastic, double (&v)[4]) {
+  const R* __restrict__ ff = Sp->f[par];       // final force
+  const R* __restrict__ fa = Sp->f[par ^ 1];   // force at the start of the last iteration
+  const unsigned char* __restrict__ gneg = Sp->gneg;
+  const CompTile<R> T(Sp, tile);
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
+    size_t ic, iu;
+    T.at(e, ic, iu);
+    const R f = ldf(ff + ic);
+    const R u = ldf(T.u + iu);
+    v[0] += (double)f * (double)u;
+    if (jac) jac[ic] = -(double)f;
+    v[1] += (f < 0);
+    bool act;
+    if (mixing) act = ldf(gneg + ic) != 0;
+    else {
+      const R a = ldf(fa + ic);
+      act = (a < 0) && (!has_h || (double)a > -H);
+    }
+    v[2] += act;
+    if (active) active[ic] = act;
+    if (has_h) {
+      const bool p = ldf(gneg + ic) != 0;
+      v[3] += p;
+      if (plastic) plastic[ic] = p;
+    }
+  }
+}
+
+CM_DEVINL void fin_result(CcgState& s, double (&a)[4]) {
+  s.sum_cgt = -a[0] / 2;  // result.fun
+  s.A_contact = (long long)a[1];
+  s.A_cg = (long long)a[2];
+  s.A_fl = (long long)a[3];
 }

@@ -132,3 +132,10 @@ int ccg_p2_update(const CcgArgs<R>& a, cudaStream_t s, bool chained);
 template <typename R>
 int ccg_p2_ew_blocks_per_sm();
 
+// The persistent batch kernel (cm_batch.cu): one launch over n jobs taken in
+// queue order `order` (next: a zeroed device counter), smem bytes of dynamic
+// shared memory per block; *clusters receives the clusters launched.
+// Returns 0 when launched.
+int batch_solve_launch(const BatchJob* jobs, const int* order, int n, int* next, size_t smem,
+                       cudaStream_t s, int* clusters);
+

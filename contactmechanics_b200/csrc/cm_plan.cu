@@ -128,6 +128,9 @@ static int pow2_threads(size_t work) {
 static std::mutex g_tune_mu;
 static std::vector<std::pair<int, int>> g_tune_elems[2];  // [FP64, FP32]: (length, elements)
 static int g_batch_threads[2] = {CM_THREADS, CM_THREADS};
+// batches of elastic solves run in the persistent cluster kernel (cm_batch.cu)
+// when set; by default they take the lockstep per-pass graph, measured faster
+static std::atomic<int> g_batch_persistent{0};
 
 static int tuned_elems(size_t csize, int length, int dflt) {
   const int pi = csize == 16 ? 0 : 1;
@@ -352,29 +355,15 @@ __global__ void __launch_bounds__(CM_THREADS)
 k_h_prep(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64) {
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
-  const CompTile<R> T(Sp, item.y);
-  R* __restrict__ h = const_cast<R*>(Sp->h);
-  const size_t base = (size_t)T.cx0 * T.ty;
-  double mx = -INFINITY, mn = INFINITY, sm = 0;
-  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
-    const double hv = h64[base + e];
-    h[base + e] = (R)hv;
-    mx = fmax(mx, hv);
-    mn = fmin(mn, hv);
-    sm += hv;
-  }
-  double v[3] = {mx, mn, sm};
+  double v[3] = {-INFINITY, INFINITY, 0.0};
+  h_prep_tile<R>(Sp, item.y, h64, v[0], v[1], v[2]);
   const int kinds[3] = {RED_MAX, RED_MIN, RED_SUM};
   CcgState* st = Sp->st;
-  tile_finish<3>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[3]) {
-    st->p.max_surface = a[0];
-    st->gmin = a[1];  // scratch until the loop starts
-    st->sum_cg = a[2];
-  });
+  tile_finish<3>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[3]) { fin_h_prep(*st, a); });
 }
 
-// rms height and the reference's default penetration tolerance
-// (ConstrainedConjugateGradients.py:150-162); FP32 phases widen pentol.
+// rms height and the default penetration tolerance
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64,
@@ -382,46 +371,20 @@ k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
-  const CompTile<R> T(Sp, item.y);
-  const size_t base = (size_t)T.cx0 * T.ty;
-  const double mean = st->sum_cg / st->p.n_surface;
-  double v2 = 0;
-  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
-    const double d = h64[base + e] - mean;
-    v2 += d * d;
-  }
-  double v[1] = {v2};
+  double v[1] = {0.0};
+  h_var_tile<R>(Sp, item.y, h64, st->sum_cg / st->p.n_surface, v[0]);
   const int kinds[1] = {RED_SUM};
   const int tx = Sp->tx, ty = Sp->ty;
   tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[1]) {
-    CcgState& s = *st;
-    if (pentol_auto) {
-      const double rms = sqrt(a[0] / s.p.n_surface);
-      double pt = rms / (10.0 * (0.5 * ((double)tx + (double)ty)));
-      if (pt == 0) pt = (s.p.offset0 + s.sum_cg / s.p.n_surface) / 1000;
-      if (pt == 0) pt = 1e-3;
-      s.p.pentol = pt;
-    }
-    if (rel_pentol > 0) s.p.pentol = fmax(s.p.pentol, rel_pentol * (s.p.max_surface - s.gmin));
-    s.gmin = 0;
-    s.sum_cg = 0;
+    fin_h_var(*st, a, pentol_auto, rel_pentol, tx, ty);
   });
 }
 
-// initial displacement: given or zero, lifted onto the surface on the
-// topography region (ConstrainedConjugateGradients.py:168-201)
 template <typename R>
 __global__ void k_init_u(Slot<R> S, const double* u0, double offset) {
   const long n = (long)S.nx * S.ny;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const int x = (int)(i / S.ny), y = (int)(i % S.ny);
-    double u = u0 ? u0[i] : 0.0;
-    if (x < S.tx && y < S.ty) {
-      const double lo = (double)S.h[(size_t)x * S.ty + y] + offset;
-      u = (u < lo) ? lo : u;
-    }
-    S.u[i] = (R)u;
-  }
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    init_u_at<R>(S, u0, offset, i);
 }
 
 // copy the topography part of a domain-sized FP64 force field
@@ -434,8 +397,7 @@ __global__ void k_init_f(Slot<R> S, const double* f0, int ld) {
   }
 }
 
-// result.x, result.jac, active_set, plastic and the elastic energy
-// (ConstrainedConjugateGradients.py:454-475, 494-509)
+// result.jac, active_set, plastic and the elastic energy
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_ccg_result(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, double* jac,
@@ -443,44 +405,12 @@ k_ccg_result(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, 
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
-  const int par = st->parity, has_h = st->p.has_h, mixing = (st->branch == 1);
-  const double H = st->p.H;
-  const R* __restrict__ ff = Sp->f[par];       // final force
-  const R* __restrict__ fa = Sp->f[par ^ 1];   // force at the start of the last iteration
-  const unsigned char* __restrict__ gneg = Sp->gneg;
-  const CompTile<R> T(Sp, item.y);
-  double e_sum = 0, area = 0, cg_area = 0, pl = 0;
-  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) {
-    size_t ic, iu;
-    T.at(e, ic, iu);
-    const R f = ff[ic];
-    const R u = T.u[iu];
-    e_sum += (double)f * (double)u;
-    if (jac) jac[ic] = -(double)f;
-    area += (f < 0);
-    bool act;
-    if (mixing) act = gneg[ic] != 0;
-    else {
-      const R a = fa[ic];
-      act = (a < 0) && (!has_h || (double)a > -H);
-    }
-    cg_area += act;
-    if (active) active[ic] = act;
-    if (has_h) {
-      const bool p = gneg[ic] != 0;
-      pl += p;
-      if (plastic) plastic[ic] = p;
-    }
-  }
-  double v[4] = {e_sum, area, cg_area, pl};
+  double v[4] = {0, 0, 0, 0};
+  result_tile<R>(Sp, item.y, st->parity, st->p.has_h, st->branch == 1, st->p.H, jac, active,
+                 plastic, v);
   const int kinds[4] = {RED_SUM, RED_SUM, RED_SUM, RED_SUM};
-  tile_finish<4>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[4]) {
-    CcgState& s = *st;
-    s.sum_cgt = -a[0] / 2;  // result.fun
-    s.A_contact = (long long)a[1];
-    s.A_cg = (long long)a[2];
-    s.A_fl = (long long)a[3];
-  });
+  tile_finish<4>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[4]) { fin_result(*st, a); });
 }
 
 template <typename R>
@@ -491,7 +421,9 @@ __global__ void k_to_f64(const R* src, double* dst, long n) {
 
 // force field of one precision -> FP64 domain-sized field (zero padding)
 template <typename R>
-__global__ void k_force_to_domain(const R* f, int tx, int ty, double* out, int nx, int ny) {
+__global__ void k_force_to_domain(const CcgState* st, const R* f0, const R* f1, int tx, int ty,
+                                  double* out, int nx, int ny) {
+  const R* f = st->parity ? f1 : f0;  // the buffer holding the solver's current forces
   const long n = (long)nx * ny;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const int x = (int)(i / ny), y = (int)(i % ny);
@@ -546,7 +478,9 @@ struct cm_plan {
   int max_items = 0;
   Work<float> w32;
   Work<double> w64;
-  CcgState* h_state = nullptr;  // pinned readback
+  // pinned host states: [0] readback, [1] and [2] staging of the FP32 and FP64
+  // initial states (a pageable source would make each copy wait for the stream)
+  CcgState* h_state = nullptr;
   std::vector<void*> allocs;
   // stepping interface: phase of the solve this plan holds
   int phase = 0;          // 0 none, 1 FP32, 2 FP64
@@ -1043,12 +977,9 @@ struct SolveInput {
 
 // State, heights and initial fields of one solve (ConstrainedConjugateGradients.py
 // :132-219), enqueued on stream s.
-template <typename R>
-static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
-                    double rel_pentol, double rel_forcetol, int maxiter, cudaStream_t s) {
-  set_smem_attrs<R>();
-  CKS(ensure_ccg(p, w));
-  CcgState st;
+// The solver state at the start of a solve phase (ConstrainedConjugateGradients.py:132-215).
+static void initial_state(const cm_plan* p, const cm_ccg_params* prm, double rel_forcetol,
+                          int maxiter, CcgState& st) {
   memset(&st, 0, sizeof(st));
   CcgParams& P = st.p;
   P.F = prm->external_force;
@@ -1072,7 +1003,21 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
   st.cur_mixfac = P.mixfac;
   st.nfev = 1;
   st.scale = 1.0;
-  CK(cudaMemcpyAsync(w.st, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+}
+
+template <typename R>
+static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
+                    double rel_pentol, double rel_forcetol, int maxiter, cudaStream_t s) {
+  set_smem_attrs<R>();
+  CKS(ensure_ccg(p, w));
+  CcgState st;
+  initial_state(p, prm, rel_forcetol, maxiter, st);
+  // Staged through pinned memory so that the copy does not wait for the
+  // stream.  Every path reads a solve's results (a synchronisation) before
+  // it initialises the same Work again, so the staging slot is free here.
+  CcgState* stage = p->h_state + (sizeof(R) == 8 ? 2 : 1);
+  *stage = st;
+  CK(cudaMemcpyAsync(w.st, stage, sizeof(st), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), s));  // a solve that gave up may leave it set
   if (w.bar) CK(cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), s));
   g_launches += 3;  // heights statistics (2) and the initial field
@@ -1085,7 +1030,7 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
     CKS(launch_plain<R>(p, w, MODE_PLAIN, CM_OP_DISP, w.f[0], p->tx, p->ty, p->ty, w.u, p->nx,
                               p->ny, p->ny, s));
   } else {
-    k_init_u<R><<<gd, 256, 0, s>>>(hs, in.u0, P.offset0);
+    k_init_u<R><<<gd, 256, 0, s>>>(hs, in.u0, st.p.offset0);
     CKS(launch_plain<R>(p, w, MODE_PLAIN, CM_OP_FORCE, w.u, p->nx, p->ny, p->ny, w.f[0], p->tx,
                               p->ty, p->ty, s));
   }
@@ -1155,10 +1100,10 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   return CM_OK;
 }
 
+// Result fields of a finished solve (launches only).
 template <typename R>
-static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned char* active,
-                      unsigned char* plastic, CcgState* fin, cudaStream_t s = nullptr) {
-  if (!s) s = p->stream;
+static int launch_result(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned char* active,
+                         unsigned char* plastic, cudaStream_t s) {
   k_ccg_result<R><<<w.nt_comp, CM_THREADS, 0, s>>>(w.d_ccg, p->items, jac, active, plastic);
   g_launches += 1;
   if (x) {
@@ -1166,6 +1111,33 @@ static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned c
     g_launches += 1;
   }
   CK(cudaGetLastError());
+  return CM_OK;
+}
+
+// Solver states of n plans to the host with one synchronisation.
+template <typename R>
+static int read_states(int n, cm_plan* const* plans, std::vector<CcgState>& out, cudaStream_t s) {
+  CcgState* hb = nullptr;
+  if (cudaMallocHost(&hb, sizeof(CcgState) * n) != cudaSuccess) {
+    cudaGetLastError();
+    return CM_ERR_OOM;
+  }
+  int rc = CM_OK;
+  for (int i = 0; i < n && rc == CM_OK; ++i)
+    if (cudaMemcpyAsync(hb + i, work_of<R>(plans[i]).st, sizeof(CcgState), cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess)
+      rc = CM_ERR_CUDA;
+  if (rc == CM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = CM_ERR_CUDA;
+  if (rc == CM_OK) out.assign(hb, hb + n);
+  cudaFreeHost(hb);
+  return rc;
+}
+
+template <typename R>
+static int finish_ccg(cm_plan* p, Work<R>& w, double* x, double* jac, unsigned char* active,
+                      unsigned char* plastic, CcgState* fin, cudaStream_t s = nullptr) {
+  if (!s) s = p->stream;
+  CKS(launch_result<R>(p, w, x, jac, active, plastic, s));
   CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   *fin = *p->h_state;
@@ -1636,7 +1608,7 @@ int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
       return fail(CM_ERR_CUDA);
     p->own_stream = true;
   }
-  if (cudaMallocHost(&p->h_state, sizeof(CcgState)) != cudaSuccess) {
+  if (cudaMallocHost(&p->h_state, 3 * sizeof(CcgState)) != cudaSuccess) {
     p->h_state = nullptr;
     return fail(CM_ERR_OOM);
   }
@@ -1806,9 +1778,8 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
     CKS(ensure_ccg(p, p->w64));
     f64 = p->w64.u;  // borrow: overwritten by the refinement's own initialisation
   }
-  const int fpar = fin.parity;
   k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, p->stream>>>(
-      p->w32.f[fpar], p->tx, p->ty, f64, p->nx, p->ny);
+      p->w32.st, p->w32.f[0], p->w32.f[1], p->tx, p->ty, f64, p->nx, p->ny);
   CK(cudaGetLastError());
   // k_init_f reads f64 before the operator overwrites u, so the borrow is safe
   SolveInput in2{h, nullptr, f64, p->ny};
@@ -1823,6 +1794,132 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   res->ms_fp64 = ms_since(t1);
   res->ms_total = ms_since(t0);
   res->polls = g_polls;
+  return CM_OK;
+}
+
+// Shared memory of the per-pass bodies on a plan's tiles: twiddles plus two
+// buffers of a row tile or of a column tile, whichever is larger.
+static size_t pass_smem(const cm_plan* p, const Tiles& t, size_t csize) {
+  const size_t r = (2 * (size_t)(t.row_tile / 2) * p->ny + p->ny) * csize;
+  const size_t c = (2 * (size_t)t.col_tile * p->nx + p->nx) * csize;
+  return std::max(r, c);
+}
+
+// Whether a batch runs in the persistent kernel: elastic solves (no
+// plastic bisection) without a wall-clock timeout whose passes fit.
+static bool batch_persistent_ok(int n, cm_plan* const* plans, const cm_ccg_params* params,
+                                int prec) {
+  if (!g_batch_persistent.load()) return false;
+  for (int i = 0; i < n; ++i) {
+    if (params[i].has_hardness || params[i].timeout_s > 0) return false;
+    if (prec != CM_FP64 && !plans[i]->w32.tiles.generic_ok) return false;
+    if (prec != CM_FP32 && !plans[i]->w64.tiles.generic_ok) return false;
+  }
+  return true;
+}
+
+// The whole batch in one launch of the persistent kernel: FP32 phase, FP64
+// refinement and result fields of every solve.
+static int batch_persistent(int n, cm_plan* const* plans, const cm_ccg_params* params,
+                            const double* const* h, const double* const* u0, double* const* x,
+                            double* const* jac, unsigned char* const* active,
+                            unsigned char* const* plastic, cm_ccg_result* res, cudaStream_t s) {
+  typedef std::chrono::steady_clock clk;
+  const auto t0 = clk::now();
+  const int prec = params[0].precision;
+  const bool use32 = prec != CM_FP64, use64 = prec != CM_FP32;
+  size_t smem = 0;
+  for (int i = 0; i < n; ++i) {
+    cm_plan* p = plans[i];
+    if (use32) {
+      CKS(ensure_ccg(p, p->w32));
+      smem = std::max(smem, pass_smem(p, p->w32.tiles, sizeof(float2)));
+    }
+    if (use64) {
+      CKS(ensure_ccg(p, p->w64));
+      smem = std::max(smem, pass_smem(p, p->w64.tiles, sizeof(double2)));
+    }
+  }
+  if (smem > CM_SMEM_DYN_MAX) return CM_ERR_SIZE;
+  const size_t jb = sizeof(BatchJob) * (size_t)n, ob = sizeof(int) * (size_t)(n + 1);
+  unsigned char* hbuf = nullptr;
+  if (cudaMallocHost(&hbuf, jb + ob) != cudaSuccess) {
+    cudaGetLastError();
+    return CM_ERR_OOM;
+  }
+  BatchJob* hj = reinterpret_cast<BatchJob*>(hbuf);
+  int* ho = reinterpret_cast<int*>(hbuf + jb);
+  for (int i = 0; i < n; ++i) {
+    cm_plan* p = plans[i];
+    const cm_ccg_params& P = params[i];
+    BatchJob& J = hj[i];
+    memset(&J, 0, sizeof(J));
+    if (use32) {
+      J.s32 = base_slot(p, p->w32);
+      const int mi = prec == CM_MIXED ? fp32_cap(P.maxiter, false) : P.maxiter;
+      initial_state(p, &P, prec == CM_MIXED ? 1e-5 : 0.0, mi, J.init32);
+    }
+    if (use64) {
+      J.s64 = base_slot(p, p->w64);
+      initial_state(p, &P, 0.0, P.maxiter, J.init64);
+    }
+    J.h64 = h[i];
+    J.u0 = u0 ? u0[i] : nullptr;
+    J.x = x ? x[i] : nullptr;
+    J.jac = jac ? jac[i] : nullptr;
+    J.active = active ? active[i] : nullptr;
+    J.plastic = plastic ? plastic[i] : nullptr;
+    J.prec = prec;
+    J.pentol_auto = P.pentol <= 0;
+    J.maxiter = P.maxiter;
+    J.rel_pentol32 = prec == CM_MIXED ? (P.fp32_pentol_rel > 0 ? P.fp32_pentol_rel : 2e-6) : 0.0;
+    ho[i] = i;
+  }
+  // largest grids first: the last solves to start are the shortest
+  std::stable_sort(ho, ho + n, [&](int a, int b) {
+    return (long)plans[a]->nx * plans[a]->ny > (long)plans[b]->nx * plans[b]->ny;
+  });
+  ho[n] = 0;  // the queue counter
+  unsigned char* dbuf = nullptr;
+  int rc = CM_OK;
+  if (cudaMalloc(&dbuf, jb + ob) != cudaSuccess) {
+    cudaGetLastError();
+    rc = CM_ERR_OOM;
+  }
+  int clusters = 0;
+  if (rc == CM_OK && cudaMemcpyAsync(dbuf, hbuf, jb + ob, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = CM_ERR_CUDA;
+  if (rc == CM_OK) {
+    int* d_order = reinterpret_cast<int*>(dbuf + jb);
+    if (batch_solve_launch(reinterpret_cast<const BatchJob*>(dbuf), d_order, n, d_order + n, smem,
+                           s, &clusters) != 0)
+      rc = CM_ERR_CUDA;
+    else
+      g_launches += 1;
+  }
+  std::vector<CcgState> st32, st64;
+  if (rc == CM_OK && use32) rc = read_states<float>(n, plans, st32, s);
+  if (rc == CM_OK && use64) rc = read_states<double>(n, plans, st64, s);
+  if (rc != CM_OK) cudaStreamSynchronize(s);  // nothing may still read the buffers
+  cudaFree(dbuf);
+  cudaFreeHost(hbuf);
+  CKS(rc);
+  const double ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  for (int i = 0; i < n; ++i) {
+    if (use32) CKS(status_error(st32[i]));
+    const CcgState& fin = use64 ? st64[i] : st32[i];
+    CKS(status_error(fin));
+    fill_result(fin, &res[i]);
+    if (prec == CM_MIXED) {
+      res[i].nit += st32[i].it;
+      res[i].nfev += st32[i].nfev;
+      res[i].nit_fp32 = st32[i].it;
+    } else if (prec == CM_FP32) {
+      res[i].nit_fp32 = st32[i].it;
+    }
+    res[i].ms_total = ms;
+    res[i].polls = 1;
+  }
   return CM_OK;
 }
 
@@ -1851,6 +1948,8 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
     timeout = std::max(timeout, params[i].timeout_s);
   }
   g_polls = 0;
+  if (batch_persistent_ok(n, plans, params, prec))
+    return batch_persistent(n, plans, params, h, u0, x, jac, active, plastic, res, s);
   typedef std::chrono::steady_clock clk;
   const auto t0 = clk::now();
   std::vector<int> nit32(n, 0), nfev32(n, 0);
@@ -1863,18 +1962,18 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
       CKS(ccg_init<float>(plans[i], plans[i]->w32, &params[i], in, rp, rf, mi, s));
     }
     CKS(batch_loop<float>(n, plans, bisect, maxiter, timeout, s, &g_polls));
+    if (prec == CM_FP32)
+      for (int i = 0; i < n; ++i)
+        CKS(launch_result<float>(plans[i], plans[i]->w32, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
+                                 active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, s));
+    std::vector<CcgState> st32;
+    CKS(read_states<float>(n, plans, st32, s));
     for (int i = 0; i < n; ++i) {
-      CcgState st;
-      CK(cudaMemcpyAsync(plans[i]->h_state, plans[i]->w32.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      st = *plans[i]->h_state;
-      CKS(status_error(st));
-      nit32[i] = st.it;
-      nfev32[i] = st.nfev;
+      CKS(status_error(st32[i]));
+      nit32[i] = st32[i].it;
+      nfev32[i] = st32[i].nfev;
       if (prec == CM_FP32) {
-        CKS(finish_ccg<float>(plans[i], plans[i]->w32, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
-                              active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, &st, s));
-        fill_result(st, &res[i]);
+        fill_result(st32[i], &res[i]);
         res[i].nit_fp32 = nit32[i];
       }
     }
@@ -1889,11 +1988,8 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
     cm_plan* p = plans[i];
     if (prec == CM_MIXED) {
       CKS(ensure_ccg(p, p->w64));
-      CK(cudaMemcpyAsync(p->h_state, p->w32.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      const int fpar = p->h_state->parity;
       k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
-          p->w32.f[fpar], p->tx, p->ty, p->w64.u, p->nx, p->ny);
+          p->w32.st, p->w32.f[0], p->w32.f[1], p->tx, p->ty, p->w64.u, p->nx, p->ny);
       SolveInput in{h[i], nullptr, p->w64.u, p->ny};
       CKS(ccg_init<double>(p, p->w64, &params[i], in, 0.0, 0.0,
                            std::max(1, params[i].maxiter - nit32[i]), s));
@@ -1905,10 +2001,13 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
   CKS(batch_loop<double>(n, plans, bisect, maxiter, timeout, s, &g_polls));
   const double ms64 = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   const double ms32 = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  for (int i = 0; i < n; ++i)
+    CKS(launch_result<double>(plans[i], plans[i]->w64, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
+                              active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, s));
+  std::vector<CcgState> st64;
+  CKS(read_states<double>(n, plans, st64, s));
   for (int i = 0; i < n; ++i) {
-    CcgState st;
-    CKS(finish_ccg<double>(plans[i], plans[i]->w64, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
-                           active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, &st, s));
+    const CcgState& st = st64[i];
     CKS(status_error(st));
     fill_result(st, &res[i]);
     res[i].nit += nit32[i];
@@ -2011,7 +2110,7 @@ int cm_ccg_handover(cm_stepper* stp, cm_plan* p, const double* h, int* finished)
     p->nfev32 = st.nfev;
     CKS(ensure_ccg(p, p->w64));
     k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
-        p->w32.f[st.parity], p->tx, p->ty, p->w64.u, p->nx, p->ny);
+        p->w32.st, p->w32.f[0], p->w32.f[1], p->tx, p->ty, p->w64.u, p->nx, p->ny);
     SolveInput in{h, nullptr, p->w64.u, p->ny};
     CKS(ccg_init<double>(p, p->w64, &p->params, in, 0.0, 0.0,
                          std::max(1, p->params.maxiter - st.it), s));
@@ -2173,6 +2272,12 @@ int cm_tuning_set_batch_threads(int precision, int threads) {
   if (threads < 32 || threads > CM_FFT_THREADS || (threads & 31)) return CM_ERR_ARG;
   std::lock_guard<std::mutex> g(g_tune_mu);
   g_batch_threads[precision == CM_FP64 ? 0 : 1] = threads;
+  return CM_OK;
+}
+
+int cm_tuning_set_batch_persistent(int enable) {
+  if (enable != 0 && enable != 1) return CM_ERR_ARG;
+  g_batch_persistent.store(enable);
   return CM_OK;
 }
 

@@ -99,3 +99,23 @@ struct Slot {
   double* partials;
   unsigned int* counter;
 };
+
+// One solve of the persistent batch kernel (cm_batch.cu): its slots of the
+// two precisions, the initial state of each phase (the final ones go to the
+// slots' st), the FP64 inputs and the result buffers.
+struct BatchJob {
+  Slot<float> s32;       // FP32 phase (prec CM_FP32 or CM_MIXED)
+  Slot<double> s64;      // FP64 phase (prec CM_FP64 or CM_MIXED)
+  CcgState init32, init64;
+  const double* h64;     // heights (tx, ty)
+  const double* u0;      // initial displacement (nx, ny) or null
+  double* x;             // results, each may be null: displacement (nx, ny)
+  double* jac;           // -force (tx, ty)
+  unsigned char* active;   // (tx, ty)
+  unsigned char* plastic;  // (tx, ty)
+  int prec;              // CM_FP64 / CM_FP32 / CM_MIXED
+  int pentol_auto;       // pentol from the heights (the reference's default)
+  int maxiter;           // iteration budget of the whole solve
+  double rel_pentol32;   // FP32 phase of a mixed solve: pentol >= this * (max h - min h)
+};
+

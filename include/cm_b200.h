@@ -320,6 +320,17 @@ int cm_tuning_set_batch_threads(int precision, int threads);
 int cm_tuning_get(int precision, int length, int* tile_elems, int* batch_threads);
 
 /*
+ * With enable = 1, batches of elastic solves without a timeout run in one
+ * launch of the persistent cluster kernel: each thread-block cluster takes
+ * whole solves (FP32 phase, FP64 refinement, result fields) from a device
+ * queue.  enable = 0 (the default) runs every batch on the lockstep per-pass
+ * kernels (a graph of launches per group of iterations), measured faster on
+ * a B200; plastic or timed batches always take it.  No reference
+ * counterpart.
+ */
+int cm_tuning_set_batch_persistent(int enable);
+
+/*
  * Number of kernels this library has launched in the process (graph nodes
  * count once per replay).  Instrumentation; no reference counterpart.
  */

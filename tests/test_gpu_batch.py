@@ -1,9 +1,12 @@
 """Batched solves: each member of a batch equals its solve alone.
 
-FP64 batch members agree with the single-solve path to 1e-10 (relative
-displacement) with identical active sets; a member's result is bitwise the
-same whether it is solved in a batch of one or among other solves; mixed
-precision members are within 1e-6 of the FP64 oracle.
+Both batch paths are covered: the persistent cluster kernel (elastic
+batches, one launch for the whole batch) and the lockstep per-pass kernels
+(any batch; plastic batches always take it).  FP64 batch members agree with
+the single-solve path to 1e-10 (relative displacement) with identical
+active sets; a member's result is bitwise the same whether it is solved in
+a batch of one or among other solves; mixed precision members are within
+1e-6 of the FP64 oracle.
 """
 import numpy as np
 import pytest
@@ -30,6 +33,23 @@ CASES = [
     ("free", (48, 40), None, None, None, 0.03, None),
     ("periodic", (64, 64), 0.7, 0.2, 4e-3, None, 0.05),
 ]
+
+
+ELASTIC = [c for c in CASES if c[6] is None]
+
+
+@pytest.fixture(params=["persistent", "lockstep"])
+def path(request, cm):
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
+    assert L.cm_tuning_set_batch_persistent(1 if request.param == "persistent" else 0) == 0
+    yield request.param
+    L.cm_tuning_set_batch_persistent(0)
+
+
+def _cases(path):
+    # a plastic member sends a batch to the lockstep kernels
+    return ELASTIC if path == "persistent" else CASES
 
 
 def _problem(cm, case, seed):
@@ -64,8 +84,8 @@ def _batch(cm, problems, precision):
     return cm.constrained_conjugate_gradients_batch(subs, hs, precision=precision, maxiter=5000, **kw)
 
 
-def test_batch_fp64_matches_single_solves(cm):
-    problems = [_problem(cm, c, seed=30 + i) for i, c in enumerate(CASES)]
+def test_batch_fp64_matches_single_solves(cm, path):
+    problems = [_problem(cm, c, seed=30 + i) for i, c in enumerate(_cases(path))]
     batch = _batch(cm, problems, "fp64")
     for (sub, o, h, kw), rb in zip(problems, batch):
         rs = cm.constrained_conjugate_gradients(sub, h, precision="fp64", **kw)
@@ -77,18 +97,20 @@ def test_batch_fp64_matches_single_solves(cm):
         np.testing.assert_array_equal(rb.active_set, rs.active_set)
 
 
-def test_batch_member_same_alone_and_in_the_mix(cm):
-    problems = [_problem(cm, c, seed=40 + i) for i, c in enumerate(CASES)]
+def test_batch_member_same_alone_and_in_the_mix(cm, path):
+    cases = _cases(path)
+    problems = [_problem(cm, c, seed=40 + i) for i, c in enumerate(cases)]
     mixed = _batch(cm, problems, "mixed")
-    for k in (0, 3, 4):
+    ks = (0, 3, 4) if path == "lockstep" else range(len(cases))
+    for k in ks:
         alone = _batch(cm, [problems[k]], "mixed")[0]
         assert np.array_equal(alone.x, mixed[k].x)
         assert np.array_equal(alone.jac, mixed[k].jac)
         assert alone.nit == mixed[k].nit
 
 
-def test_batch_mixed_vs_oracle(cm):
-    problems = [_problem(cm, c, seed=50 + i) for i, c in enumerate(CASES)]
+def test_batch_mixed_vs_oracle(cm, path):
+    problems = [_problem(cm, c, seed=50 + i) for i, c in enumerate(_cases(path))]
     batch = _batch(cm, problems, "mixed")
     for (sub, o, h, kw), rb in zip(problems, batch):
         ref = oc.constrained_conjugate_gradients(o, h, **kw)
@@ -118,3 +140,51 @@ def test_batch_under_other_launch_shapes(cm):
         ref = oc.constrained_conjugate_gradients(o, h, **kw)
         assert r.success and ref["success"]
         np.testing.assert_allclose(r.x, ref["x"], rtol=0, atol=1e-10 * abs(ref["x"]).max())
+
+
+def test_persistent_batch_is_one_launch(cm):
+    """An elastic batch (FP32 phase, FP64 refinement and results of every
+    solve) is one kernel launch of the library."""
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
+    problems = [_problem(cm, c, seed=60 + i) for i, c in enumerate(ELASTIC)]
+    try:
+        assert L.cm_tuning_set_batch_persistent(1) == 0
+        _batch(cm, problems, "mixed")  # plans' solver buffers allocated
+        before = L.cm_launch_count()
+        res = _batch(cm, problems, "mixed")
+        assert L.cm_launch_count() - before == 1
+    finally:
+        L.cm_tuning_set_batch_persistent(0)
+    assert all(r.success for r in res)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+def test_persistent_and_lockstep_agree(cm, precision):
+    """The two batch paths reach the same solutions (to the precision's
+    rounding) with the same iteration counts up to a couple of steps."""
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
+    problems = [_problem(cm, c, seed=70 + i) for i, c in enumerate(ELASTIC)]
+    if precision == "fp32":
+        # tolerances an FP32 solve reaches; offset control's test on the
+        # relative change of the total force (thermotol) is below FP32
+        # rounding, so only the load-controlled solves
+        problems = [p for p, c in zip(problems, ELASTIC) if c[4] is not None]
+        for sub, o, h, kw in problems:
+            kw["pentol"] = 1e-5 * float(h.max() - h.min())
+            kw["forcetol"] = 1e-7
+    lock = _batch(cm, problems, precision)
+    try:
+        assert L.cm_tuning_set_batch_persistent(1) == 0
+        pers = _batch(cm, problems, precision)
+    finally:
+        L.cm_tuning_set_batch_persistent(0)
+    tol = {"fp64": 1e-10, "mixed": 1e-6, "fp32": 1e-4}[precision]
+    for (sub, o, h, kw), a, b in zip(problems, pers, lock):
+        assert a.success and b.success
+        nb = sub.nb_grid_pts
+        xa, xb = a.x[:nb[0], :nb[1]], b.x[:nb[0], :nb[1]]
+        assert np.linalg.norm(xa - xb) / np.linalg.norm(xb) < tol
+        assert abs(a.nit - b.nit) <= 3, (a.nit, b.nit)
+

@@ -21,8 +21,9 @@ on the device and compares with the FP64 oracle on the same seeded inputs:
       PlasticNonSmoothContactSystem against the oracle.
 * C3  eight solves of the batched benchmark's size mix (sides from
       {64, 96, 128, 192, 256, 384, 512}, the 96/192/384 sides on the
-      mixed-radix transforms) through the batched solver and through the
-      continuous-batching server, each against the oracle to 1e-6.
+      mixed-radix transforms) through the batched solver (lockstep graph and
+      persistent cluster kernel) and through the continuous-batching
+      server, each against the oracle to 1e-6.
 
 Tolerances are the benchmark's: pentol = 1e-9 (max h - min h), forcetol =
 1e-12 F (C1: tighter, as in the reference's Hertz checks).
@@ -200,13 +201,20 @@ def c3_cases():
     return cases
 
 
-def test_c3_size_mix_batched_vs_oracle(cm, c3_cases):
+@pytest.mark.parametrize("persistent", [0, 1], ids=["lockstep", "persistent"])
+def test_c3_size_mix_batched_vs_oracle(cm, c3_cases, persistent):
+    from contactmechanics_b200 import _lib
+    L = _lib.lib()
     subs = [cm.PeriodicFFTElasticHalfSpace(nb, 1.0, (1.0, 1.0)) for nb, _, _, _ in c3_cases]
-    res = cm.constrained_conjugate_gradients_batch(
-        subs, [h for _, h, _, _ in c3_cases],
-        external_force=[kw["external_force"] for _, _, kw, _ in c3_cases],
-        pentol=[kw["pentol"] for _, _, kw, _ in c3_cases],
-        forcetol=[kw["forcetol"] for _, _, kw, _ in c3_cases], precision="mixed")
+    try:
+        assert L.cm_tuning_set_batch_persistent(persistent) == 0
+        res = cm.constrained_conjugate_gradients_batch(
+            subs, [h for _, h, _, _ in c3_cases],
+            external_force=[kw["external_force"] for _, _, kw, _ in c3_cases],
+            pentol=[kw["pentol"] for _, _, kw, _ in c3_cases],
+            forcetol=[kw["forcetol"] for _, _, kw, _ in c3_cases], precision="mixed")
+    finally:
+        L.cm_tuning_set_batch_persistent(0)
     for (nb, h, kw, ref), r in zip(c3_cases, res):
         assert r.success
         e = rel(r.x, ref["x"])
