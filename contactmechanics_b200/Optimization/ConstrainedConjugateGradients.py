@@ -9,9 +9,14 @@ mixing step with its offset bisection and the convergence test -- runs on
 the device (``cm_ccg_solve`` of libcm_b200.so); the host only polls a
 convergence flag every few iterations.
 
+``callback(it, f_r, d)`` and the logger's per-iteration rows follow the
+reference (:436-489): every iteration that does not converge is reported
+(the loop then polls the device after each iteration instead of every few);
+``f_r`` is the iteration's force field on the domain (a CUDA tensor when
+the heights were one, else a numpy array).  In a mixed-precision solve the
+FP64 refinement continues the FP32 phase's iteration count.
+
 Differences that follow from keeping the loop on the device:
-* ``callback`` and ``logger`` see the final iteration only (the reference
-  calls them every iteration, :436-489);
 * masked (``np.ma``) heights and MPI domain decomposition are not supported;
 * a scalar ``hardness`` must be positive (the reference fails later, inside
   its bisection, for ``hardness == 0``).
@@ -165,6 +170,14 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
     P.check_every = int(check_every) if check_every else 0
     P.timeout_s = float(timeout) if timeout else 0.0
     res = _lib.CcgResult()
+    errors = []
+    observer = None
+    if callback is not None or logger is not quiet:
+        fbuf = torch.empty(dshape, dtype=torch.float64, device="cuda")
+        observer = _observer(callback, logger, verbose, hardness is not None, maxiter, fbuf, dom,
+                             as_torch, float(np.prod(tshape)), forcetol, errors)
+        P.on_iteration = observer
+        P.iteration_forces = fbuf.data_ptr()
 
     def ptr(t):
         return ctypes.c_void_p(t.data_ptr()) if t is not None else None
@@ -172,6 +185,8 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
     torch.cuda.current_stream().synchronize()
     code = plan._L.cm_ccg_solve(plan.ptr, ctypes.byref(P), ptr(h_dev), ptr(u0), ptr(f0),
                                 ptr(x), ptr(jac), ptr(active), ptr(plastic), ctypes.byref(res))
+    if errors:
+        raise errors[0]  # the callback's own exception stopped the solve
     if code == _lib.CM_ERR_NAN:
         raise RuntimeError("nan encountered.")
     if code == _lib.CM_ERR_BISECT:
@@ -223,13 +238,50 @@ def constrained_conjugate_gradients(substrate, topography, hardness=None, extern
     logger.pr(f"maxiter = {maxiter}")
     logger.pr(f"pentol = {res.pentol_used}")
     logger.st(log_headers, log_values, force_print=True)
-    if callback is not None:
-        callback(res.nit, -result.jac,
-                 dict(area=int(res.area), rms_penetration=res.rms_pen,
-                      max_penetration=res.max_pen, max_pressure=res.max_pres,
-                      pad_pressure=res.pad_pres, penetration_tol=res.pentol_used,
-                      pressure_tol=forcetol))
     return result
+
+
+_MODE_STR = {1: "sd", 2: "cg", 3: "mix"}
+
+
+def _observer(callback, logger, verbose, plastic, maxiter, fbuf, dom, as_torch, n_surface,
+              forcetol, errors):
+    """The per-iteration observer handed to cm_ccg_solve: the reference's
+    logger row and callback(it, f_r, d) (ConstrainedConjugateGradients.py
+    :436-489) from the iteration's state and forces.  An exception stops the
+    solve and is re-raised by the caller."""
+    def on_iteration(user, info_p):
+        try:
+            i = info_p.contents
+            if logger is not quiet and i.it < maxiter:
+                hdr = ["status", "it", "area", "frac. area", "cg area", "total force", "offset"]
+                val = [_MODE_STR.get(i.mode, "sd"), i.it, i.area, i.area / n_surface, i.cg_area,
+                       i.total_force, i.offset]
+                if plastic:
+                    hdr += ["plast. area", "frac.plast. area"]
+                    val += [i.plastic_area, i.plastic_area / n_surface]
+                if verbose:
+                    hdr += ["rms pen.", "max. pen.", "max. force", "max. pad force", "max. du",
+                            "CG area", "frac. CG area", "sum(nc_r)"]
+                    val += [i.rms_pen, i.max_pen, i.max_pres, i.pad_pres, i.maxdu, i.cg_area,
+                            i.cg_area / n_surface, i.nc_count]
+                    hdr += ["mixfac"] if i.mode == 3 else ["tau"]
+                    val += [i.mixfac] if i.mode == 3 else [i.tau]
+                logger.st(hdr, val)
+            if callback is not None:
+                f_r = fbuf.reshape(dom)
+                if not as_torch:
+                    f_r = f_r.cpu().numpy()
+                d = dict(area=int(i.area), fractional_area=i.area / n_surface,
+                         rms_penetration=i.rms_pen, max_penetration=i.max_pen,
+                         max_pressure=i.max_pres, pad_pressure=i.pad_pres,
+                         penetration_tol=i.pentol, pressure_tol=forcetol)
+                callback(i.it, f_r, d)
+            return 0
+        except BaseException as e:  # cannot cross the C frames: stop and re-raise
+            errors.append(e)
+            return 1
+    return _lib.ITERATION_FN(on_iteration)
 
 
 def _params(precision, external_force, offset, hardness, pentol, forcetol, thermotol, mixfac,

@@ -1,9 +1,9 @@
 """Minimal column logger with the interface the solver uses
 (``pr`` and ``st``, ContactMechanics/Tools/Logger.py:102-233).
 
-The device-resident solve has no per-iteration host round trip, so the
-solver reports the final iteration only (``force_print=True`` line of the
-reference, ConstrainedConjugateGradients.py:454-456, 495).
+A solver given a logger other than ``quiet`` reports every iteration that
+did not converge through the library's per-iteration observer, then the
+final ``force_print=True`` line (ConstrainedConjugateGradients.py:436-495).
 """
 import sys
 

@@ -21,6 +21,7 @@ CM_ERR_NAN = 6
 CM_ERR_BISECT = 7
 CM_ERR_BISECT_CONV = 8
 CM_ERR_TIMEOUT = 9
+CM_ERR_STOPPED = 10
 
 CM_PERIODIC = 0
 CM_FREE = 1
@@ -50,6 +51,23 @@ class PlanDesc(ctypes.Structure):
                 ("periodic_y", ctypes.c_int), ("n_images", ctypes.c_int)]
 
 
+class Iteration(ctypes.Structure):
+    """cm_iteration: one CCG iteration as the per-iteration observer sees it."""
+    _fields_ = [("it", ctypes.c_int), ("precision", ctypes.c_int), ("mode", ctypes.c_int),
+                ("done", ctypes.c_int), ("area", ctypes.c_longlong),
+                ("cg_area", ctypes.c_longlong), ("plastic_area", ctypes.c_longlong),
+                ("nc_count", ctypes.c_longlong),
+                ("rms_pen", ctypes.c_double), ("max_pen", ctypes.c_double),
+                ("max_pres", ctypes.c_double), ("pad_pres", ctypes.c_double),
+                ("maxdu", ctypes.c_double), ("total_force", ctypes.c_double),
+                ("offset", ctypes.c_double), ("tau", ctypes.c_double),
+                ("mixfac", ctypes.c_double), ("pentol", ctypes.c_double),
+                ("forcetol", ctypes.c_double), ("forces", ctypes.c_void_p)]
+
+
+ITERATION_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(Iteration))
+
+
 class CcgParams(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("load_control", ctypes.c_int),
                 ("external_force", ctypes.c_double), ("offset", ctypes.c_double),
@@ -58,7 +76,9 @@ class CcgParams(ctypes.Structure):
                 ("thermotol", ctypes.c_double), ("mixfac", ctypes.c_double),
                 ("mixdecfac", ctypes.c_double), ("minmixsteps", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("check_every", ctypes.c_int),
-                ("fp32_pentol_rel", ctypes.c_double), ("timeout_s", ctypes.c_double)]
+                ("fp32_pentol_rel", ctypes.c_double), ("timeout_s", ctypes.c_double),
+                ("on_iteration", ITERATION_FN), ("user", ctypes.c_void_p),
+                ("iteration_forces", ctypes.c_void_p)]
 
 
 class CcgResult(ctypes.Structure):

@@ -555,6 +555,10 @@ k_col(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
 CM_DEVINL void ccg_converge(CcgState& s, double maxdu_in, double maxpen_in) {
   // convergence test (ConstrainedConjugateGradients.py:391-434, 491-492)
   const CcgParams& P = s.p;
+  s.rep_area = s.A_contact;
+  s.rep_cg_area = s.A_cg;
+  s.rep_offset = s.offset;
+  s.rep_mode = s.mode;
   s.maxdu = maxdu_in;
   s.nfev += (s.branch == 0) ? 2 : 1;
   s.G_old = s.G;

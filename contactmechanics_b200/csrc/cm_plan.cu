@@ -487,6 +487,7 @@ struct cm_plan {
   int phase_prec = 0;     // CM_FP32 / CM_FP64 / CM_MIXED of the solve
   int nit32 = 0, nfev32 = 0;
   cm_ccg_params params{};
+  int obs_it_offset = 0;  // observer: iterations of earlier phases of the solve
 };
 
 template <typename R> static Work<R>& work_of(cm_plan* p);
@@ -1075,6 +1076,8 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     const long work = (long)p->nx * p->ny;
     every = work >= (1L << 20) ? (w.by_value ? 8 : 4) : (work >= (1L << 16) ? 8 : 16);
   }
+  const bool observe = prm->on_iteration != nullptr && prm->iteration_forces != nullptr;
+  if (observe) every = 1;
   auto t0 = std::chrono::steady_clock::now();
   cudaGraphExec_t g;
   CKS(get_graph<R>(p, w, bisect, every, &g));
@@ -1085,6 +1088,40 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     ++g_polls;
+    if (observe) {
+      const CcgState st = *p->h_state;
+      if (!(st.done && st.status == CMS_CONVERGED)) {
+        // the reference reports every iteration that did not converge
+        k_force_to_domain<R><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
+            w.st, w.f[0], w.f[1], p->tx, p->ty, prm->iteration_forces, p->nx, p->ny);
+        g_launches += 1;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        cm_iteration info;
+        memset(&info, 0, sizeof(info));
+        info.it = p->obs_it_offset + (st.done ? st.it : st.it - 1);
+        info.precision = sizeof(R) == 8 ? CM_FP64 : CM_FP32;
+        info.mode = st.rep_mode;
+        info.done = st.done;
+        info.area = st.rep_area;
+        info.cg_area = st.rep_cg_area;
+        info.plastic_area = st.A_fl;
+        info.nc_count = st.n_nc;
+        info.rms_pen = st.rms_pen;
+        info.max_pen = st.max_pen;
+        info.max_pres = st.max_pres;
+        info.pad_pres = st.pad_pres;
+        info.maxdu = st.maxdu;
+        info.total_force = st.total_force;
+        info.offset = st.rep_offset;
+        info.tau = st.tau;
+        info.mixfac = st.cur_mixfac;
+        info.pentol = st.p.pentol;
+        info.forcetol = std::max(st.p.forcetol, st.p.rel_forcetol * st.fmax);
+        info.forces = prm->iteration_forces;
+        if (prm->on_iteration(prm->user, &info) != 0) return CM_ERR_STOPPED;
+      }
+    }
     if (p->h_state->done) break;
     if (prm->timeout_s > 0) {
       const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1563,6 +1600,7 @@ const char* cm_status_string(int status) {
     case CM_ERR_BISECT: return "f(a) and f(b) must have different signs";
     case CM_ERR_BISECT_CONV: return "Failed to converge after 100 iterations";
     case CM_ERR_TIMEOUT: return "solve exceeded its time budget";
+    case CM_ERR_STOPPED: return "stopped by the per-iteration observer";
     default: return "unknown status";
   }
 }
@@ -1746,6 +1784,7 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   auto ms_since = [](clk::time_point a) {
     return std::chrono::duration<double, std::milli>(clk::now() - a).count();
   };
+  p->obs_it_offset = 0;
   if (prm->precision == CM_FP64) {
     CKS(run_ccg<double>(p, p->w64, prm, in, 0.0, 0.0, prm->maxiter, &fin));
     CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
@@ -1784,6 +1823,7 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   // k_init_f reads f64 before the operator overwrites u, so the borrow is safe
   SolveInput in2{h, nullptr, f64, p->ny};
   const int rem = std::max(1, prm->maxiter - nit32);
+  p->obs_it_offset = nit32;
   CKS(run_ccg<double>(p, p->w64, prm, in2, 0.0, 0.0, rem, &fin));
   CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
   fill_result(fin, res);

@@ -60,6 +60,12 @@ struct CcgState {
   // scipy-compatible bisection state (offset of the mixing step)
   double bs_xa, bs_dm, bs_fa;
   double bs_cand[CM_BIS_CAND + 1];
+  // the finished iteration's start-of-iteration values, kept by the
+  // convergence test for the per-iteration observer (a fused pass may have
+  // started the next iteration already)
+  long long rep_area, rep_cg_area;
+  double rep_offset;
+  int rep_mode;
 };
 
 // Grid barrier (count of arrivals, generation, abort flag) of the kernels

@@ -43,6 +43,7 @@ extern "C" {
 #define CM_ERR_BISECT 7       /* offset bisection sign error (ValueError) */
 #define CM_ERR_BISECT_CONV 8  /* offset bisection did not converge (RuntimeError) */
 #define CM_ERR_TIMEOUT 9      /* a solve exceeded its host-side time budget */
+#define CM_ERR_STOPPED 10     /* the per-iteration observer asked the solve to stop */
 
 /* substrate kinds */
 #define CM_PERIODIC 0
@@ -86,6 +87,31 @@ typedef struct {
   int n_images;
 } cm_plan_desc;
 
+/*
+ * One CCG iteration as a per-iteration observer sees it (the reference's
+ * callback(it, f_r, d) and logger rows, ConstrainedConjugateGradients.py
+ * :436-489).
+ */
+typedef struct {
+  int it;                /* iteration number, 1-based; the FP64 refinement of a
+                            CM_MIXED solve continues the FP32 count */
+  int precision;         /* CM_FP32 or CM_FP64: the phase the iteration ran in */
+  int mode;              /* step kind: 1 steepest descent, 2 conjugate gradient,
+                            3 mixing step (delta_str 'sd', 'cg', 'mix') */
+  int done;              /* 1 if the iteration ended the phase (maximum
+                            iterations or an error) */
+  long long area, cg_area, plastic_area;
+  long long nc_count;    /* points whose sign constraint was violated (sum(nc_r)) */
+  double rms_pen, max_pen, max_pres, pad_pres, maxdu;
+  double total_force, offset, tau, mixfac;
+  double pentol, forcetol;
+  const double* forces;  /* device: the iteration's forces on the domain
+                            (nxd, nyd), FP64, valid during the call */
+} cm_iteration;
+
+/* returns 0 to continue; any other value stops the solve (CM_ERR_STOPPED) */
+typedef int (*cm_iteration_fn)(void* user, const cm_iteration* info);
+
 typedef struct {
   int precision;         /* CM_FP64, CM_FP32 or CM_MIXED */
   int load_control;      /* 1: external_force given; 0: offset given */
@@ -100,6 +126,14 @@ typedef struct {
   double fp32_pentol_rel;  /* CM_MIXED: FP32 phase pentol = max(pentol, rel * height range);
                              <= 0: 2e-6 */
   double timeout_s;      /* host-side wall-clock budget; <= 0: none */
+  /* cm_ccg_solve only: called on the calling thread after every iteration
+     that did not converge, as the reference calls its callback; the solve
+     then polls after every iteration.  iteration_forces: caller-owned
+     device buffer of nxd * nyd doubles that receives the forces first.
+     NULL: no observer (other entry points ignore it). */
+  cm_iteration_fn on_iteration;
+  void* user;
+  double* iteration_forces;
 } cm_ccg_params;
 
 typedef struct {
