@@ -282,6 +282,10 @@ def run_gpu(args, rank, world, local_rank):
         res = None
         for _ in range(steps):
             flush.fill_(1.0)
+            # the previous step's results go back to the allocator's cache
+            # before this step allocates its own (else every other step pays
+            # for fresh device allocations)
+            res = None
             res = sweep(precision, host=host, lat=lat)
         e1.record()
         barrier()
