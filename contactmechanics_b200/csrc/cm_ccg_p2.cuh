@@ -233,7 +233,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
   const int tx = a.tx, ty = a.ty, nx = a.op.nx;
-  const int rows_total = (MODE == MODE_T) ? tx : nx;
+  const int rows_total = (MODE == MODE_T) ? tx : a.u_rows;
   const int ntiles = (rows_total + ROWS - 1) / ROWS;
   const R off = (R)cv.offset;
   const R hdn = neg_down<R>(cv.H);
@@ -247,7 +247,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
   R du = 0, pmax = -INFINITY;                     // MODE_F: extrema, exact in R
   R gmax = -INFINITY, gmin = INFINITY;
   int n_c = 0, n_cg = 0;                          // counts, exact in int
-  double s_cg = 0;
+  double s_cg = 0, s_cg2 = 0;                     // sums of g and g^2 over the CG area
   const R* __restrict__ fn_buf = a.f[cv.par ^ 1];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int x0 = tile * ROWS;
@@ -313,6 +313,10 @@ k_ccg_row_inv(CcgArgs<R> a) {
             n_c += c0;
             n_cg += c;
             if (c) s_cg += (double)g;
+            // the reference sums c g^2 over the whole topography, so a NaN
+            // gap outside the contact set makes G NaN as well
+            if (c) s_cg2 += (double)g * (double)g;
+            else if (isnan(g)) s_cg2 += (double)g;
             gmax = fmax(gmax, g);
             gmin = fmin(gmin, g);
           }
@@ -327,14 +331,26 @@ k_ccg_row_inv(CcgArgs<R> a) {
     tile_finish<1>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds,
                    [&](double (&r)[1]) { fin_tau(*st, r); });
   } else {
-    double vr[7] = {(double)du, (double)pmax, (double)n_c, (double)n_cg, s_cg, (double)gmax,
-                    (double)gmin};
-    const int kinds[7] = {RED_MAX, RED_MAX, RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN};
-    tile_finish<7>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds, [&](double (&r)[7]) {
+    double vr[8] = {(double)du, (double)pmax, (double)n_c, (double)n_cg, s_cg, (double)gmax,
+                    (double)gmin, s_cg2};
+    const int kinds[8] = {RED_MAX, RED_MAX, RED_SUM, RED_SUM, RED_SUM, RED_MAX, RED_MIN, RED_SUM};
+    const int fuse = a.fuse_gsum;
+    tile_finish<8>(a.partials, a.counter, blockIdx.x, gridDim.x, vr, kinds, [&](double (&r)[8]) {
       ccg_converge(*st, r[0], r[1]);
       if (!st->done) {
         double b[5] = {r[2], r[3], r[4], r[5], r[6]};
         fin_begin(*st, b);
+        if (fuse && st->branch == 0) {
+          // G = sum over c of (g - offset)^2 from the sums over c of g^2
+          // and g (each g^2 of an FP32 gap is exact in FP64); near
+          // convergence this loses about eps64 * sum g^2 / G, far below the
+          // FP32 gaps' own rounding
+          const double off = st->offset;
+          double G = r[7] - 2.0 * off * r[4] + (double)st->A_cg * off * off;
+          if (G < 0) G = 0;  // rounding (a NaN stays NaN)
+          double gv[1] = {G};
+          fin_gsum(*st, gv);
+        }
       }
     });
   }

@@ -71,6 +71,13 @@ struct CcgArgs {
   int tx, ty;
   int ny;        // row length of u (domain columns)
   int ew_grid;   // blocks of the vectorised element-wise passes
+  int u_rows;    // rows of u the displacement pass updates: nx, or tx in the
+                 // FP32 phase of a mixed solve (the padding's displacement
+                 // feeds only max |du| and the result, which the FP64 phase
+                 // recomputes from the forces)
+  int fuse_gsum; // the displacement pass also forms the next iteration's G
+                 // (FP32 phase of a mixed solve; the iterations then run
+                 // without the gsum pass)
 };
 // Launch with programmatic stream serialization: the kernel may start while
 // its predecessor on the stream finishes, and calls pdl_wait before reading

@@ -176,7 +176,7 @@ int ccg_row_inv(const CcgArgs<R>& a, cudaStream_t s, bool launch = true) {
                                                                        info);
   }
   if (rc || !launch) return rc;
-  const int rows = MODE == MODE_T ? a.tx : a.op.nx;
+  const int rows = MODE == MODE_T ? a.tx : a.u_rows;
   const int tiles = (rows + 2 * Sh::NP - 1) / (2 * Sh::NP);
   const int grid = std::max(1, std::min(tiles, info.grid_per_sm * sm_count()));
   launch_pdl(k_ccg_row_inv<R, MODE, LOGN>, grid, Sh::THREADS, Sh::smem(), s, a);

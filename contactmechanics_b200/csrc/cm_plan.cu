@@ -461,6 +461,7 @@ struct Work {
   CcgArgs<R> ccg_args{};    // their arguments
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [bisect passes]
   int graph_iters[2] = {0, 0};
+  int graph_variant[2] = {0, 0};  // ccg_args.u_rows and fuse_gsum the graph was captured with
   int nt_comp = 0, nt_rowt = 0, nt_rowd = 0, nt_col = 0;
   int partial_blocks = 0;   // blocks whose reduction partials fit the partials buffer
 };
@@ -668,6 +669,8 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
     a.ty = p->ty;
     a.ny = p->ny;
     a.ew_grid = 0;
+    a.u_rows = p->nx;
+    a.fuse_gsum = 0;
     w.by_value = CM_BY_VALUE_PASSES && lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw);
     if (w.by_value) {
       const int rc = ccg_p2_prepare<R>(a, lx, ly);
@@ -880,7 +883,8 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   }
   mark();
   if (w.by_value) {
-    ccg_p2_gsum<R>(w.ccg_args, s, chain);
+    // with fuse_gsum the previous iteration's displacement pass formed G
+    if (!w.ccg_args.fuse_gsum) ccg_p2_gsum<R>(w.ccg_args, s, chain);
     chain = true;
   } else {
     elementwise(k_ccg_gsum<R>, 1);
@@ -895,7 +899,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     OpArgs<R> col_t = a.op, col_f = a.op;
     col_t.out_rows = p->tx;
     col_t.cg_only = 1;
-    col_f.out_rows = p->nx;
+    col_f.out_rows = a.u_rows;
     ccg_p2_row_fwd<R, MODE_T>(a, ry, s);
     mark();
     ccg_p2_col<R>(col_t, rx, s);
@@ -937,7 +941,8 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
 template <typename R>
 static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphExec_t* out) {
   const int gi = bisect ? 1 : 0;
-  if (w.graph[gi] && w.graph_iters[gi] == iters) {
+  const int variant = 2 * w.ccg_args.u_rows + w.ccg_args.fuse_gsum;
+  if (w.graph[gi] && w.graph_iters[gi] == iters && w.graph_variant[gi] == variant) {
     *out = w.graph[gi];
     return CM_OK;
   }
@@ -965,6 +970,7 @@ static int get_graph(cm_plan* p, Work<R>& w, bool bisect, int iters, cudaGraphEx
   }
   CK(e);
   w.graph_iters[gi] = iters;
+  w.graph_variant[gi] = variant;
   *out = w.graph[gi];
   return CM_OK;
 }
@@ -1042,13 +1048,21 @@ static int ccg_init(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solv
 template <typename R>
 static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
                    double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
-                   int prof_iters = 0, float* prof_ms = nullptr) {
+                   int prof_iters = 0, float* prof_ms = nullptr, bool topo_u = false) {
   cudaStream_t s = p->stream;
+  // topo_u (FP32 phase of a mixed solve): the displacement pass updates
+  // the topography's rows only and forms the next iteration's G as well
+  w.ccg_args.u_rows = topo_u ? p->tx : p->nx;
+  w.ccg_args.fuse_gsum = topo_u ? 1 : 0;
   CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   if (w.by_value) {
     // start of the first iteration; later ones come from k_ccg_row_inv<MODE_F>
     k_ccg_begin<R><<<w.ew_grid[0], CM_THREADS, 0, s>>>(w.d_ccg, p->items, w.nt_comp);
     g_launches += 1;
+    if (w.ccg_args.fuse_gsum) {
+      CKS(ccg_p2_gsum<R>(w.ccg_args, s, true) == 0 ? CM_OK : CM_ERR_CUDA);
+      g_launches += 1;
+    }
   }
   const bool bisect = prm->has_hardness && prm->load_control;
   if (prof_iters > 0) {
@@ -1084,7 +1098,8 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
   for (int done_iters = 0;; done_iters += every) {
     CK(cudaGraphLaunch(g, s));
     g_launches += (unsigned long long)every *
-                   iteration_launches(bisect, w.by_value, w.by_value && w.ew_grid[4] > 0);
+                   (iteration_launches(bisect, w.by_value, w.by_value && w.ew_grid[4] > 0) -
+                    (w.by_value && w.ccg_args.fuse_gsum ? 1 : 0));
     CK(cudaMemcpyAsync(p->h_state, w.st, sizeof(CcgState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     ++g_polls;
@@ -1798,7 +1813,10 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   // FP32 phase: tolerances widened to FP32 resolution; a phase that cannot
   // reach them within its iteration cap hands over to the FP64 refinement
   const int cap32 = prm->precision == CM_MIXED ? fp32_cap(prm->maxiter, prm->has_hardness) : prm->maxiter;
-  CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin));
+  // the FP32 phase of a mixed solve leaves the padding's displacement alone:
+  // the refinement recomputes u = G f on the whole domain from its forces
+  CKS(run_ccg<float>(p, p->w32, prm, in, rp, rf, cap32, &fin, 0, nullptr,
+                     prm->precision == CM_MIXED));
   const double ms32 = ms_since(t0);
   if (prm->precision == CM_FP32) {
     CKS(finish_ccg<float>(p, p->w32, x, jac, active, plastic, &fin));
