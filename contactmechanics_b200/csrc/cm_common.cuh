@@ -109,6 +109,35 @@ CM_DEVINL bool mbar_wait(unsigned long long* b, unsigned parity) {
   return true;
 }
 
+// Division by a divisor that is fixed for a pass, as a high multiply and a
+// shift (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): for d >= 2 with l = ceil(log2 d),
+// m = ceil(2^(31+l) / d) < 2^32, and floor(x / d) = (x m) >> (31 + l) for
+// every 0 <= x < 2^31.  The multiplier is computed on the host (one 64-bit
+// division per divisor); m = 0 encodes d = 1.
+struct FastDiv {
+  unsigned d, m, s;  // divisor, multiplier, shift applied to the high word
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.d = d;
+  f.m = 0;
+  f.s = 0;
+  if (d >= 2) {
+    unsigned l = 0;
+    while ((1ull << l) < d) ++l;
+    f.m = (unsigned)(((1ull << (31 + l)) + d - 1) / d);
+    f.s = l - 1;
+  }
+  return f;
+}
+
+// floor(x / f.d) for 0 <= x < 2^31
+CM_DEVINL int fdiv(const FastDiv& f, int x) {
+  return f.m ? (int)(__umulhi((unsigned)x, f.m) >> f.s) : x;
+}
+
 enum { RED_SUM = 0, RED_MAX = 1, RED_MIN = 2 };
 
 CM_DEVINL double red_neutral(int kind) {

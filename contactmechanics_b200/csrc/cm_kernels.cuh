@@ -345,13 +345,14 @@ CM_DEVINL void row_fwd_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
   const int x0 = tile * row_tile;
   const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
+  const FastDiv dny = Sp->dv_ny, dnyh = Sp->dv_nyh;
   C* __restrict__ spec = Sp->spec;
 
   if (MODE == MODE_PLAIN || MODE == MODE_FWD) {
     const R* __restrict__ in = Sp->in;
     const int in_cols = Sp->in_cols, in_ld = Sp->in_ld;
     batched_loop<4>(npairs * ny, [&](int e) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       const int xa = x0 + 2 * p;
       R va = 0, vb = 0;
       if (y < in_cols) {
@@ -368,7 +369,7 @@ CM_DEVINL void row_fwd_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
     const R off = (R)cv.offset;
     struct In { R f[2], u[2], h[2], t[2]; };
     batched_loop<2>(npairs * ny, [&](int e) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       In v;
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
@@ -386,7 +387,7 @@ CM_DEVINL void row_fwd_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
       }
       return v;
     }, [&](int e, const In& v) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       R vv[2] = {0, 0};
       if (y < ty) {
 #pragma unroll
@@ -428,7 +429,7 @@ CM_DEVINL void row_fwd_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
   __syncthreads();
   const C* res = fft_smem<C, false>(buf, scratch, fd, npairs, ny, 1, false, tws);
   for (int e = threadIdx.x; e < npairs * nyh; e += blockDim.x) {
-    const int p = e / nyh, k = e - p * nyh;
+    const int p = fdiv(dnyh, e), k = e - p * nyh;
     const C z = res[p * ny + k];
     const C zm = res[p * ny + (k == 0 ? 0 : ny - k)];
     const int xa = x0 + 2 * p;
@@ -611,17 +612,18 @@ CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
   const int x0 = tile * row_tile;
   const int nrows = min(row_tile, rows_total - x0);
   const int npairs = (nrows + 1) >> 1;
+  const FastDiv dny = Sp->dv_ny, dnyh = Sp->dv_nyh;
   const C* __restrict__ spec = Sp->spec;
   struct XY { C X, Y; };
   batched_loop<4>(npairs * nyh, [&](int e) {
-    const int p = e / nyh, k = e - p * nyh;
+    const int p = fdiv(dnyh, e), k = e - p * nyh;
     const int xa = x0 + 2 * p;
     XY v;
     v.X = ldf(spec + spec_at(xa, k, nx, lw));
     v.Y = (xa + 1 < x0 + nrows) ? ldf(spec + spec_at(xa + 1, k, nx, lw)) : czero<C>();
     return v;
   }, [&](int e, XY v) {
-    const int p = e / nyh, k = e - p * nyh;
+    const int p = fdiv(dnyh, e), k = e - p * nyh;
     C X = v.X, Y = v.Y;
     const bool selfconj = (k == 0) || (2 * k == ny);
     if (selfconj) { X.y = 0; Y.y = 0; }
@@ -634,7 +636,7 @@ CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
     R* __restrict__ out = Sp->out;
     const int out_cols = Sp->out_cols, out_ld = Sp->out_ld;
     for (int e = threadIdx.x; e < npairs * ny; e += blockDim.x) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       if (y >= out_cols) continue;
       const C z = res[e];
       const int xa = x0 + 2 * p;
@@ -645,7 +647,7 @@ CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
     const R* __restrict__ t = Sp->t;
     struct T2 { R a, b; };
     batched_loop<4>(npairs * ny, [&](int e) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       const int xa = x0 + 2 * p;
       T2 v{0, 0};
       if (y < ty) {
@@ -665,7 +667,7 @@ CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
     const R off = (R)cv.offset;
     struct UF { R uo[2], fa[2], h[2]; unsigned char gn[2]; };
     batched_loop<2>(npairs * ny, [&](int e) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       UF v;
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
@@ -682,7 +684,7 @@ CM_DEVINL void row_inv_tile(const Slot<R>* __restrict__ Sp, const CcgView& cv, i
       }
       return v;
     }, [&](int e, const UF& v) {
-      const int p = e / ny, y = e - p * ny;
+      const int p = fdiv(dny, e), y = e - p * ny;
       const C z = res[e];
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
@@ -744,21 +746,22 @@ k_row_inv(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
 // Fields of one comp tile (rows [cx0, cx0+crows) of the topography) in registers.
 template <typename R>
 struct CompTile {
-  int cx0, cn, ty, ny, lty;  // lty: log2 of ty when ty is a power of two, else -1
+  int cx0, cn, ty, ny;
+  FastDiv dty;
   const R* __restrict__ u;
   const R* __restrict__ h;
   CM_DEVINL CompTile(const Slot<R>* Sp, int tile) {
     ty = Sp->ty;
     ny = Sp->ny;
+    dty = Sp->dv_ty;
     cx0 = tile * Sp->comp_rows;
     cn = min(Sp->comp_rows, Sp->tx - cx0) * ty;
     u = Sp->u;
     h = Sp->h;
-    lty = (ty & (ty - 1)) == 0 ? __ffs(ty) - 1 : -1;
   }
   // topography index and displacement index of element e of the tile
   CM_DEVINL void at(int e, size_t& ic, size_t& iu) const {
-    const int r = lty >= 0 ? e >> lty : e / ty, y = e - r * ty;
+    const int r = fdiv(dty, e), y = e - r * ty;
     ic = (size_t)cx0 * ty + e;
     iu = (size_t)(cx0 + r) * ny + y;
   }

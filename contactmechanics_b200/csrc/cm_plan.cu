@@ -569,6 +569,9 @@ static Slot<R> base_slot(cm_plan* p, Work<R>& w) {
   s.nt_rowt = (p->tx + s.row_tile - 1) / s.row_tile;
   s.nt_rowd = (p->nx + s.row_tile - 1) / s.row_tile;
   s.nt_col = w.tiles.ntile_cols;
+  s.dv_ny = make_fastdiv(p->ny);
+  s.dv_nyh = make_fastdiv(p->nyh);
+  s.dv_ty = make_fastdiv(p->ty);
   s.fx = p->fx;
   s.fy = p->fy;
   s.twx = w.twx;
@@ -1218,22 +1221,6 @@ static void fill_result(const CcgState& st, cm_ccg_result* r) {
 // ---------------------------------------------------------------------------
 // batches of independent solves
 // ---------------------------------------------------------------------------
-// Count the solves of a batch that have not finished.
-template <typename R>
-__global__ void k_count_running(const Slot<R>* __restrict__ slots, int n, int* out) {
-  int c = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) c += slots[i].st->done ? 0 : 1;
-  c = __reduce_add_sync(0xffffffffu, c);
-  __shared__ int sm[32];
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int t = 0;
-    for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) t += sm[i];
-    *out = t;
-  }
-}
-
 // Device arrays of one batch: slot descriptors and the (slot, tile) work
 // lists of the four tile spaces.
 template <typename R>
@@ -1241,7 +1228,7 @@ struct BatchDev {
   Slot<R>* slots = nullptr;
   int2* items[4] = {nullptr, nullptr, nullptr, nullptr};  // comp, rows<tx, rows<nx, columns
   int n_items[4] = {0, 0, 0, 0};
-  int* running = nullptr;
+  int* running = nullptr;  // count of running solves, then one done flag per solve
   size_t smem_row = 0, smem_col = 0;
   std::vector<void*> allocs;
   ~BatchDev() {
@@ -1249,19 +1236,40 @@ struct BatchDev {
   }
 };
 
+// Work lists of the solves `which` (indices into the batch's slot array).
+template <typename R>
+static int batch_items(cm_plan* const* plans, const std::vector<int>& which, BatchDev<R>& b,
+                       cudaStream_t s) {
+  std::vector<int2> it[4];
+  for (int i : which) {
+    const Work<R>& w = work_of<R>(plans[i]);
+    for (int t = 0; t < w.nt_comp; ++t) it[0].push_back(make_int2(i, t));
+    for (int t = 0; t < w.nt_rowt; ++t) it[1].push_back(make_int2(i, t));
+    for (int t = 0; t < w.nt_rowd; ++t) it[2].push_back(make_int2(i, t));
+    for (int t = 0; t < w.nt_col; ++t) it[3].push_back(make_int2(i, t));
+  }
+  for (int k = 0; k < 4; ++k) {
+    b.n_items[k] = (int)it[k].size();
+    CK(cudaMemcpyAsync(b.items[k], it[k].data(), sizeof(int2) * it[k].size(),
+                       cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return CM_OK;
+}
+
 template <typename R>
 static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_t s) {
   std::vector<Slot<R>> hs(n);
-  std::vector<int2> it[4];
+  size_t cap[4] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i)
     if (!work_of<R>(plans[i]).tiles.generic_ok) return CM_ERR_SIZE;  // single-solve passes only
   for (int i = 0; i < n; ++i) {
     Work<R>& w = work_of<R>(plans[i]);
     hs[i] = base_slot(plans[i], w);
-    for (int t = 0; t < hs[i].nt_comp; ++t) it[0].push_back(make_int2(i, t));
-    for (int t = 0; t < hs[i].nt_rowt; ++t) it[1].push_back(make_int2(i, t));
-    for (int t = 0; t < hs[i].nt_rowd; ++t) it[2].push_back(make_int2(i, t));
-    for (int t = 0; t < hs[i].nt_col; ++t) it[3].push_back(make_int2(i, t));
+    cap[0] += hs[i].nt_comp;
+    cap[1] += hs[i].nt_rowt;
+    cap[2] += hs[i].nt_rowd;
+    cap[3] += hs[i].nt_col;
     b.smem_row = std::max(b.smem_row, w.tiles.smem_row);
     b.smem_col = std::max(b.smem_col, w.tiles.smem_col);
   }
@@ -1272,14 +1280,11 @@ static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_
   };
   CKS(al((void**)&b.slots, sizeof(Slot<R>) * n));
   CK(cudaMemcpyAsync(b.slots, hs.data(), sizeof(Slot<R>) * n, cudaMemcpyHostToDevice, s));
-  for (int k = 0; k < 4; ++k) {
-    b.n_items[k] = (int)it[k].size();
-    CKS(al((void**)&b.items[k], sizeof(int2) * std::max<size_t>(1, it[k].size())));
-    CK(cudaMemcpyAsync(b.items[k], it[k].data(), sizeof(int2) * it[k].size(), cudaMemcpyHostToDevice, s));
-  }
-  CKS(al((void**)&b.running, sizeof(int)));
-  CK(cudaStreamSynchronize(s));
-  return CM_OK;
+  for (int k = 0; k < 4; ++k) CKS(al((void**)&b.items[k], sizeof(int2) * std::max<size_t>(1, cap[k])));
+  CKS(al((void**)&b.running, sizeof(int) * (1 + n)));  // count, then the done flags
+  std::vector<int> all(n);
+  for (int i = 0; i < n; ++i) all[i] = i;
+  return batch_items<R>(plans, all, b, s);
 }
 
 // One iteration of every solve of the batch (generic transforms: the solves
@@ -1302,7 +1307,30 @@ static void launch_iteration_batch(const BatchDev<R>& b, bool bisect, cudaStream
   k_row_inv<R, MODE_F><<<b.n_items[2], TT, b.smem_row, s>>>(S, b.items[2]);
 }
 
-// Run the CCG loop of every solve of the batch to completion.
+// Count the solves of a batch that have not finished; done flags after it.
+template <typename R>
+__global__ void k_batch_running(const Slot<R>* __restrict__ slots, int n, int* out) {
+  int c = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int d = slots[i].st->done;
+    out[1 + i] = d;
+    c += d ? 0 : 1;
+  }
+  c = __reduce_add_sync(0xffffffffu, c);
+  __shared__ int sm[32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) t += sm[i];
+    out[0] = t;
+  }
+}
+
+// Run the CCG loop of every solve of the batch to completion.  The work
+// lists (and the graph of `every` iterations over them) are rebuilt for the
+// running solves whenever their number has halved since the last build, so
+// the launches of a batch's tail cover only the solves still iterating.
 template <typename R>
 static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, double timeout_s,
                       cudaStream_t s, int* polls) {
@@ -1312,23 +1340,32 @@ static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, do
   long work = 0;
   for (int i = 0; i < n; ++i) work += (long)plans[i]->nx * plans[i]->ny;
   const int every = work >= (1L << 22) ? 4 : 16;
-  cudaGraph_t g;
-  cudaGraphExec_t ge;
-  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-  for (int i = 0; i < every; ++i) launch_iteration_batch<R>(b, bisect, s);
-  k_count_running<R><<<1, 256, 0, s>>>(b.slots, n, b.running);
-  CK(cudaStreamEndCapture(s, &g));
-  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-  cudaGraphDestroy(g);
-  CK(e);
-  int running = n;
+  cudaGraphExec_t ge = nullptr;
+  auto capture = [&]() -> int {
+    if (ge) cudaGraphExecDestroy(ge);
+    ge = nullptr;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    for (int i = 0; i < every; ++i) launch_iteration_batch<R>(b, bisect, s);
+    k_batch_running<R><<<1, 256, 0, s>>>(b.slots, n, b.running);
+    CK(cudaStreamEndCapture(s, &g));
+    const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    return CM_OK;
+  };
+  CKS(capture());
+  std::vector<int> flags(1 + n);
+  int running = n, built = n;
   int rc = CM_OK;
   auto t0 = std::chrono::steady_clock::now();
   for (int done_iters = 0; running > 0; done_iters += every) {
     if (cudaGraphLaunch(ge, s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
     g_launches += (unsigned long long)every * (iteration_launches(bisect, false)) + 1;
-    if (cudaMemcpyAsync(&running, b.running, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+    if (cudaMemcpyAsync(flags.data(), b.running, sizeof(int) * (1 + n), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) { rc = CM_ERR_CUDA; break; }
+    running = flags[0];
     if (polls) ++*polls;
     if (timeout_s > 0 &&
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s) {
@@ -1336,8 +1373,16 @@ static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, do
       break;
     }
     if (done_iters > maxiter + 2 * every) { rc = CM_ERR_CUDA; break; }
+    if (running > 0 && 2 * running <= built) {
+      std::vector<int> which;
+      for (int i = 0; i < n; ++i)
+        if (!flags[1 + i]) which.push_back(i);
+      if ((rc = batch_items<R>(plans, which, b, s)) != CM_OK) break;
+      if ((rc = capture()) != CM_OK) break;
+      built = running;
+    }
   }
-  cudaGraphExecDestroy(ge);
+  if (ge) cudaGraphExecDestroy(ge);
   return rc;
 }
 
@@ -2241,6 +2286,7 @@ int cm_apply_periodic_noalloc(int nx, int ny, double sx, double sy, double young
   sv.nx = nx; sv.ny = ny; sv.nyh = nyh; sv.tx = nx; sv.ty = ny;
   sv.row_tile = T.row_tile; sv.col_tile = T.col_tile; sv.lw = T.lw; sv.comp_rows = T.comp_rows;
   sv.nt_rowt = nt_row; sv.nt_rowd = nt_row; sv.nt_col = T.ntile_cols; sv.nt_comp = 0;
+  sv.dv_ny = make_fastdiv(ny); sv.dv_nyh = make_fastdiv(nyh); sv.dv_ty = make_fastdiv(ny);
   sv.fx = fx; sv.fy = fy; sv.twx = d_twx; sv.twy = d_twy; sv.spec = d_spec;
   sv.tab[0] = d_tab; sv.tab[1] = d_tab; sv.table_sel = 0;
   sv.in = in; sv.out = out;

@@ -86,6 +86,7 @@ struct Slot {
   int row_tile, col_tile, comp_rows;       // tile shapes (col_tile = 2^lw)
   int lw;                                  // log2 of the spectrum column-tile width
   int nt_comp, nt_rowt, nt_rowd, nt_col;   // tiles over comp rows, rows<tx, rows<nx, columns
+  FastDiv dv_ny, dv_nyh, dv_ty;            // the element loops' divisors
   FftDesc fx, fy;
   const C* twx;
   const C* twy;
