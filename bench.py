@@ -454,7 +454,7 @@ def run_batched(fp64_subset=48):
         L.cm_tuning_set_batch_persistent(0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     idx = list(range(0, C3_N, C3_N // fp64_subset))[:fp64_subset]
-    for i in idx[:4]:  # warm-up of the single-solve path
+    for i in idx:  # warm-up of the single-solve path: every plan's graphs captured
         cm.constrained_conjugate_gradients(subs[i], hs[i], external_force=F[i], pentol=PT[i],
                                            forcetol=FT[i], precision="fp64")
     torch.cuda.synchronize()
