@@ -356,14 +356,15 @@ k_h_prep(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, cons
   const int2 item = items[blockIdx.x];
   const Slot<R>* __restrict__ Sp = slots + item.x;
   double v[3] = {-INFINITY, INFINITY, 0.0};
-  h_prep_tile<R>(Sp, item.y, h64, v[0], v[1], v[2]);
+  h_prep_tile<R>(Sp, item.y, h64 ? h64 : Sp->h64, v[0], v[1], v[2]);
   const int kinds[3] = {RED_MAX, RED_MIN, RED_SUM};
   CcgState* st = Sp->st;
   tile_finish<3>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
                  [&](double (&a)[3]) { fin_h_prep(*st, a); });
 }
 
-// rms height and the default penetration tolerance
+// rms height and the default penetration tolerance; pentol_auto < 0: from
+// the solve's own parameters (pentol <= 0), batches of mixed callers
 template <typename R>
 __global__ void __launch_bounds__(CM_THREADS)
 k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const double* h64,
@@ -372,12 +373,79 @@ k_h_var(const Slot<R>* __restrict__ slots, const int2* __restrict__ items, const
   const Slot<R>* __restrict__ Sp = slots + item.x;
   CcgState* st = Sp->st;
   double v[1] = {0.0};
-  h_var_tile<R>(Sp, item.y, h64, st->sum_cg / st->p.n_surface, v[0]);
+  h_var_tile<R>(Sp, item.y, h64 ? h64 : Sp->h64, st->sum_cg / st->p.n_surface, v[0]);
   const int kinds[1] = {RED_SUM};
   const int tx = Sp->tx, ty = Sp->ty;
   tile_finish<1>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds, [&](double (&a)[1]) {
-    fin_h_var(*st, a, pentol_auto, rel_pentol, tx, ty);
+    const int automatic = pentol_auto >= 0 ? pentol_auto : (st->p.pentol <= 0);
+    fin_h_var(*st, a, automatic, rel_pentol, tx, ty);
   });
+}
+
+// Lockstep batches: every solve's initial state (staged in `init`) to its
+// slot, reduction ticket cleared.
+template <typename R>
+__global__ void k_put_states(const Slot<R>* __restrict__ slots, const CcgState* __restrict__ init,
+                             int n) {
+  const int words = (int)(sizeof(CcgState) / sizeof(int));
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int* src = reinterpret_cast<const int*>(init + i);
+    int* dst = reinterpret_cast<int*>(slots[i].st);
+    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+    if (threadIdx.x == 0) *slots[i].counter = 0;
+  }
+}
+
+// Lockstep batches: initial displacement of the domain rows of a row tile
+template <typename R>
+__global__ void k_init_u_rows(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>& S = slots[item.x];
+  const int x0 = item.y * S.row_tile;
+  const int rows = min(S.row_tile, S.nx - x0);
+  const double off = S.st->p.offset0;
+  const long base = (long)x0 * S.ny, n = (long)rows * S.ny;
+  for (long e = threadIdx.x; e < n; e += blockDim.x) init_u_at<R>(S, S.u0, off, base + e);
+}
+
+// Lockstep batches, FP64 phase of mixed solves: f = the FP32 phase's forces
+// over a comp tile
+template <typename R>
+__global__ void k_init_f_prev(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  const CompTile<R> T(Sp, item.y);
+  const float* __restrict__ fp = Sp->prev_f[Sp->prev_st->parity & 1];
+  R* __restrict__ f = Sp->f[0];
+  const size_t base = (size_t)T.cx0 * T.ty;
+  for (int e = threadIdx.x; e < T.cn; e += blockDim.x) f[base + e] = (R)fp[base + e];
+}
+
+// Lockstep batches: result fields of every solve (outputs from the slots)
+template <typename R>
+__global__ void __launch_bounds__(CM_THREADS)
+k_ccg_result_slots(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>* __restrict__ Sp = slots + item.x;
+  CcgState* st = Sp->st;
+  double v[4] = {0, 0, 0, 0};
+  result_tile<R>(Sp, item.y, st->parity, st->p.has_h, st->branch == 1, st->p.H, Sp->jac_out,
+                 Sp->act_out, Sp->pl_out, v);
+  const int kinds[4] = {RED_SUM, RED_SUM, RED_SUM, RED_SUM};
+  tile_finish<4>(Sp->partials, Sp->counter, item.y, Sp->nt_comp, v, kinds,
+                 [&](double (&a)[4]) { fin_result(*st, a); });
+}
+
+// Lockstep batches: the displacement of a row tile's domain rows to FP64
+template <typename R>
+__global__ void k_x_rows(const Slot<R>* __restrict__ slots, const int2* __restrict__ items) {
+  const int2 item = items[blockIdx.x];
+  const Slot<R>& S = slots[item.x];
+  if (!S.x_out) return;
+  const int x0 = item.y * S.row_tile;
+  const int rows = min(S.row_tile, S.nx - x0);
+  const long base = (long)x0 * S.ny, n = (long)rows * S.ny;
+  for (long e = threadIdx.x; e < n; e += blockDim.x) S.x_out[base + e] = (double)ldf(S.u + base + e);
 }
 
 template <typename R>
@@ -1257,8 +1325,8 @@ static int batch_items(cm_plan* const* plans, const std::vector<int>& which, Bat
   return CM_OK;
 }
 
-template <typename R>
-static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_t s) {
+template <typename R, typename Fill>
+static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_t s, Fill fill) {
   std::vector<Slot<R>> hs(n);
   size_t cap[4] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i)
@@ -1266,6 +1334,7 @@ static int batch_build(int n, cm_plan* const* plans, BatchDev<R>& b, cudaStream_
   for (int i = 0; i < n; ++i) {
     Work<R>& w = work_of<R>(plans[i]);
     hs[i] = base_slot(plans[i], w);
+    fill(i, hs[i]);
     cap[0] += hs[i].nt_comp;
     cap[1] += hs[i].nt_rowt;
     cap[2] += hs[i].nt_rowd;
@@ -1332,11 +1401,8 @@ __global__ void k_batch_running(const Slot<R>* __restrict__ slots, int n, int* o
 // running solves whenever their number has halved since the last build, so
 // the launches of a batch's tail cover only the solves still iterating.
 template <typename R>
-static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, double timeout_s,
-                      cudaStream_t s, int* polls) {
-  set_smem_attrs<R>();
-  BatchDev<R> b;
-  CKS(batch_build<R>(n, plans, b, s));
+static int batch_loop(int n, cm_plan* const* plans, BatchDev<R>& b, bool bisect, int maxiter,
+                      double timeout_s, cudaStream_t s, int* polls) {
   long work = 0;
   for (int i = 0; i < n; ++i) work += (long)plans[i]->nx * plans[i]->ny;
   const int every = work >= (1L << 22) ? 4 : 16;
@@ -1384,6 +1450,92 @@ static int batch_loop(int n, cm_plan* const* plans, bool bisect, int maxiter, do
   }
   if (ge) cudaGraphExecDestroy(ge);
   return rc;
+}
+
+// One phase of a lockstep batch in precision R: every solve's initial
+// state, working heights (with the default pentol), initial field and
+// operator are set up by a few launches over the batch's work lists (not a
+// sequence per solve), then the loop runs, then (final) the result fields;
+// `out` receives the solves' states.  from_fp32: warm start from the FP32
+// phase's forces (the FP64 phase of mixed solves), else from u0.
+template <typename R>
+static int lockstep_phase(int n, cm_plan* const* plans, const cm_ccg_params* params,
+                          const double* const* h, const double* const* u0, double* const* x,
+                          double* const* jac, unsigned char* const* active,
+                          unsigned char* const* plastic, bool from_fp32, double rel_pentol,
+                          double rel_forcetol, const std::vector<int>& maxiters, bool final,
+                          bool bisect, int maxiter_all, double timeout, cudaStream_t s, int* polls,
+                          std::vector<CcgState>& out) {
+  set_smem_attrs<R>();
+  for (int i = 0; i < n; ++i) CKS(ensure_ccg(plans[i], work_of<R>(plans[i])));
+  BatchDev<R> b;
+  CKS(batch_build<R>(n, plans, b, s, [&](int i, Slot<R>& sl) {
+    cm_plan* p = plans[i];
+    sl.h64 = h[i];
+    sl.u0 = (!from_fp32 && u0) ? u0[i] : nullptr;
+    sl.prev_f[0] = p->w32.f[0];
+    sl.prev_f[1] = p->w32.f[1];
+    sl.prev_st = p->w32.st;
+    sl.x_out = x ? x[i] : nullptr;
+    sl.jac_out = jac ? jac[i] : nullptr;
+    sl.act_out = active ? active[i] : nullptr;
+    sl.pl_out = plastic ? plastic[i] : nullptr;
+    // the set-up's operator: f = K u from u0, or u = G f from the FP32 forces
+    if (!from_fp32) {
+      sl.in = sl.u; sl.in_rows = p->nx; sl.in_cols = p->ny; sl.in_ld = p->ny;
+      sl.out = sl.f[0]; sl.out_rows = p->tx; sl.out_cols = p->ty; sl.out_ld = p->ty;
+      sl.table_sel = 1;
+    } else {
+      sl.in = sl.f[0]; sl.in_rows = p->tx; sl.in_cols = p->ty; sl.in_ld = p->ty;
+      sl.out = sl.u; sl.out_rows = p->nx; sl.out_cols = p->ny; sl.out_ld = p->ny;
+      sl.table_sel = 0;
+    }
+  }));
+  // initial states through one pinned staging copy
+  CcgState* hst = nullptr;
+  if (cudaMallocHost(&hst, sizeof(CcgState) * n) != cudaSuccess) {
+    cudaGetLastError();
+    return CM_ERR_OOM;
+  }
+  for (int i = 0; i < n; ++i) initial_state(plans[i], &params[i], rel_forcetol, maxiters[i], hst[i]);
+  CcgState* dst = nullptr;
+  int rc = CM_OK;
+  if (cudaMalloc(&dst, sizeof(CcgState) * n) != cudaSuccess) { cudaGetLastError(); rc = CM_ERR_OOM; }
+  else b.allocs.push_back(dst);
+  if (rc == CM_OK && cudaMemcpyAsync(dst, hst, sizeof(CcgState) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = CM_ERR_CUDA;
+  if (rc == CM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = CM_ERR_CUDA;
+  cudaFreeHost(hst);
+  CKS(rc);
+  const int TT = g_batch_threads[sizeof(R) == 8 ? 0 : 1];
+  const Slot<R>* S = b.slots;
+  k_put_states<R><<<std::min(n, 1024), 128, 0, s>>>(S, dst, n);
+  k_h_prep<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], nullptr);
+  k_h_var<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0], nullptr, -1, rel_pentol);
+  if (!from_fp32) {
+    k_init_u_rows<R><<<b.n_items[2], 256, 0, s>>>(S, b.items[2]);
+    k_row_fwd<R, MODE_PLAIN><<<b.n_items[2], TT, b.smem_row, s>>>(S, b.items[2]);
+    k_col<R, MODE_PLAIN><<<b.n_items[3], TT, b.smem_col, s>>>(S, b.items[3]);
+    k_row_inv<R, MODE_PLAIN><<<b.n_items[1], TT, b.smem_row, s>>>(S, b.items[1]);
+  } else {
+    k_init_f_prev<R><<<b.n_items[0], 256, 0, s>>>(S, b.items[0]);
+    k_row_fwd<R, MODE_PLAIN><<<b.n_items[1], TT, b.smem_row, s>>>(S, b.items[1]);
+    k_col<R, MODE_PLAIN><<<b.n_items[3], TT, b.smem_col, s>>>(S, b.items[3]);
+    k_row_inv<R, MODE_PLAIN><<<b.n_items[2], TT, b.smem_row, s>>>(S, b.items[2]);
+  }
+  g_launches += 7;
+  CK(cudaGetLastError());
+  CKS(batch_loop<R>(n, plans, b, bisect, maxiter_all, timeout, s, polls));
+  if (final) {
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i) all[i] = i;
+    CKS(batch_items<R>(plans, all, b, s));  // the loop kept only the last running solves
+    k_ccg_result_slots<R><<<b.n_items[0], CM_THREADS, 0, s>>>(S, b.items[0]);
+    k_x_rows<R><<<b.n_items[2], 256, 0, s>>>(S, b.items[2]);
+    g_launches += 2;
+    CK(cudaGetLastError());
+  }
+  return read_states<R>(n, plans, out, s);
 }
 
 static int status_error(const CcgState& st) {
@@ -2059,18 +2211,12 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
   if (prec != CM_FP64) {
     const double rp = prec == CM_MIXED ? (params[0].fp32_pentol_rel > 0 ? params[0].fp32_pentol_rel : 2e-6) : 0.0;
     const double rf = prec == CM_MIXED ? 1e-5 : 0.0;
-    for (int i = 0; i < n; ++i) {
-      SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, plans[i]->ny};
-      const int mi = prec == CM_MIXED ? fp32_cap(params[i].maxiter, params[i].has_hardness) : params[i].maxiter;
-      CKS(ccg_init<float>(plans[i], plans[i]->w32, &params[i], in, rp, rf, mi, s));
-    }
-    CKS(batch_loop<float>(n, plans, bisect, maxiter, timeout, s, &g_polls));
-    if (prec == CM_FP32)
-      for (int i = 0; i < n; ++i)
-        CKS(launch_result<float>(plans[i], plans[i]->w32, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
-                                 active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, s));
+    std::vector<int> mi(n);
+    for (int i = 0; i < n; ++i)
+      mi[i] = prec == CM_MIXED ? fp32_cap(params[i].maxiter, params[i].has_hardness) : params[i].maxiter;
     std::vector<CcgState> st32;
-    CKS(read_states<float>(n, plans, st32, s));
+    CKS(lockstep_phase<float>(n, plans, params, h, u0, x, jac, active, plastic, false, rp, rf, mi,
+                              prec == CM_FP32, bisect, maxiter, timeout, s, &g_polls, st32));
     for (int i = 0; i < n; ++i) {
       CKS(status_error(st32[i]));
       nit32[i] = st32[i].it;
@@ -2087,28 +2233,14 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
     }
   }
   const auto t1 = clk::now();
-  for (int i = 0; i < n; ++i) {
-    cm_plan* p = plans[i];
-    if (prec == CM_MIXED) {
-      CKS(ensure_ccg(p, p->w64));
-      k_force_to_domain<float><<<grid_for((long)p->nx * p->ny), 256, 0, s>>>(
-          p->w32.st, p->w32.f[0], p->w32.f[1], p->tx, p->ty, p->w64.u, p->nx, p->ny);
-      SolveInput in{h[i], nullptr, p->w64.u, p->ny};
-      CKS(ccg_init<double>(p, p->w64, &params[i], in, 0.0, 0.0,
-                           std::max(1, params[i].maxiter - nit32[i]), s));
-    } else {
-      SolveInput in{h[i], u0 ? u0[i] : nullptr, nullptr, p->ny};
-      CKS(ccg_init<double>(p, p->w64, &params[i], in, 0.0, 0.0, params[i].maxiter, s));
-    }
-  }
-  CKS(batch_loop<double>(n, plans, bisect, maxiter, timeout, s, &g_polls));
+  std::vector<int> mi(n);
+  for (int i = 0; i < n; ++i)
+    mi[i] = prec == CM_MIXED ? std::max(1, params[i].maxiter - nit32[i]) : params[i].maxiter;
+  std::vector<CcgState> st64;
+  CKS(lockstep_phase<double>(n, plans, params, h, u0, x, jac, active, plastic, prec == CM_MIXED,
+                             0.0, 0.0, mi, true, bisect, maxiter, timeout, s, &g_polls, st64));
   const double ms64 = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   const double ms32 = std::chrono::duration<double, std::milli>(t1 - t0).count();
-  for (int i = 0; i < n; ++i)
-    CKS(launch_result<double>(plans[i], plans[i]->w64, x ? x[i] : nullptr, jac ? jac[i] : nullptr,
-                              active ? active[i] : nullptr, plastic ? plastic[i] : nullptr, s));
-  std::vector<CcgState> st64;
-  CKS(read_states<double>(n, plans, st64, s));
   for (int i = 0; i < n; ++i) {
     const CcgState& st = st64[i];
     CKS(status_error(st));

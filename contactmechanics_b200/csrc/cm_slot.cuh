@@ -105,6 +105,16 @@ struct Slot {
   CcgState* st;
   double* partials;
   unsigned int* counter;
+  // lockstep batches: per-solve inputs and results of the batched set-up
+  // and result kernels (unused elsewhere)
+  const double* h64;        // FP64 heights (tx, ty)
+  const double* u0;         // initial displacement (nx, ny) or null
+  const float* prev_f[2];   // FP64 phase of a mixed solve: the FP32 phase's forces
+  const CcgState* prev_st;  // ... and its state (which buffer holds them)
+  double* x_out;            // results, each may be null
+  double* jac_out;
+  unsigned char* act_out;
+  unsigned char* pl_out;
 };
 
 // One solve of the persistent batch kernel (cm_batch.cu): its slots of the
