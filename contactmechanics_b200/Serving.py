@@ -11,12 +11,14 @@ to the FP64 refinement, and retires finished solves.  A solve's result does
 not depend on which other solves share its steps.
 
 Large requests (at least ``large_points`` domain points) skip the lockstep
-batch: a worker thread solves them one at a time with the single-solve path
-(``constrained_conjugate_gradients``, which on power-of-two domains runs the
-by-value passes of a CUDA graph on the plan's own stream) while the loop
-keeps stepping the small ones; their results are those of
-``constrained_conjugate_gradients`` for the same arguments.  Without a
-running loop thread, ``step`` solves a waiting large request itself.
+batch: ``large_workers`` worker threads solve them with the single-solve
+path (``constrained_conjugate_gradients``, which on power-of-two domains runs
+the by-value passes of a CUDA graph on the plan's own stream), each one
+request at a time, while the loop keeps stepping the small ones; the
+single-solve passes are latency-bound, so two large solves on their own
+streams overlap on the device.  Their results are those of
+``constrained_conjugate_gradients`` for the same arguments.  Without
+running threads, ``step`` solves a waiting large request itself.
 
 Each request returns the same ``OptimizeResult`` as
 ``constrained_conjugate_gradients`` (numpy arrays), plus ``latency_s`` from
@@ -101,12 +103,13 @@ class ContactServer:
                      (default: torch.cuda.mem_get_info)
     precision        "mixed", "fp64" or "fp32"
     large_points     requests with at least this many domain points are
-                     solved one at a time by the single-solve path
-                     (None: every request is batched)
+                     solved by the single-solve path (None: every request
+                     is batched)
+    large_workers    threads solving large requests concurrently
     """
 
     def __init__(self, max_active=512, iters_per_step=8, hbm_reserve=1 << 30, mem_info=None,
-                 precision="mixed", large_points=1 << 20):
+                 precision="mixed", large_points=1 << 20, large_workers=2):
         torch = _torch()
         self._L = _lib.lib()
         self._torch = torch
@@ -121,8 +124,9 @@ class ContactServer:
         self._pending = collections.deque()
         self._large = collections.deque()
         self.large_points = large_points
-        self._large_busy = False
-        self._worker = None
+        self._large_busy = 0       # large requests being solved
+        self.large_workers = max(1, int(large_workers))
+        self._workers = []
         self._active = []
         self._pool = collections.defaultdict(list)
         self._lock = threading.Lock()
@@ -180,8 +184,8 @@ class ContactServer:
     def step(self):
         """One scheduling round: admit, advance, hand over, retire.
         Returns the number of solves in flight after the round."""
-        if self._worker is None and self._large:
-            self._solve_next_large()  # no worker thread: solve it here
+        if not self._workers and self._large:
+            self._solve_next_large()  # no worker threads: solve it here
         self._admit()
         if not self._active:
             return 0
@@ -212,7 +216,7 @@ class ContactServer:
     def run_until_idle(self, timeout=None):
         t0 = time.perf_counter()
         while self._pending or self._active or self._large or self._large_busy:
-            if not self.step() and self._worker is not None:
+            if not self.step() and self._workers:
                 time.sleep(0.0005)
             if timeout is not None and time.perf_counter() - t0 > timeout:
                 raise TimeoutError("server did not drain")
@@ -251,8 +255,10 @@ class ContactServer:
                         self._large_wake.wait(0.001)
                         self._large_wake.clear()
 
-        self._worker = threading.Thread(target=large_loop, daemon=True)
-        self._worker.start()
+        for _ in range(self.large_workers):
+            w = threading.Thread(target=large_loop, daemon=True)
+            w.start()
+            self._workers.append(w)
 
     def stop(self):
         if self._thread is None:
@@ -262,9 +268,9 @@ class ContactServer:
         self._large_wake.set()
         self._thread.join()
         self._thread = None
-        if self._worker is not None:
-            self._worker.join()
-            self._worker = None
+        for w in self._workers:
+            w.join()
+        self._workers = []
 
     def close(self):
         self.stop()
@@ -286,7 +292,7 @@ class ContactServer:
             if not self._large:
                 return False
             req = self._large.popleft()
-            self._large_busy = True
+            self._large_busy += 1
         try:
             with self._lock:
                 sub = self._substrate(req)
@@ -310,7 +316,8 @@ class ContactServer:
                     self._pool[req.key].append(sub)
             req.done_event.set()
         finally:
-            self._large_busy = False
+            with self._lock:
+                self._large_busy -= 1
         return True
 
     def _substrate(self, req):

@@ -35,6 +35,7 @@
 // lockstep launches keep several tiles of different solves in flight on
 // every SM.  The kernel is therefore opt-in (cm_tuning_set_batch_persistent).
 #include <algorithm>
+#include <mutex>
 
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
@@ -421,13 +422,13 @@ k_batch_solve(const BatchJob* __restrict__ jobs, const int* __restrict__ order, 
 
 int batch_solve_launch(const BatchJob* jobs, const int* order, int n, int* next, size_t smem,
                        cudaStream_t s, int* clusters) {
-  static bool attrs = false;
-  if (!attrs) {
-    if (cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)CM_SMEM_DYN_MAX) != cudaSuccess)
-      return 1;
-    attrs = true;
-  }
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)CM_SMEM_DYN_MAX);
+  });
+  if (attr_err != cudaSuccess) return 1;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;

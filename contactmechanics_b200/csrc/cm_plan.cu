@@ -594,10 +594,19 @@ static int grid_for(long n) {
 }
 
 template <typename R>
+static void set_smem_attrs_once();
+
+// Shared-memory attributes of the per-pass kernels, set once per process
+// before any thread's first launch (callers from several threads wait for
+// the first to finish).
+template <typename R>
 static void set_smem_attrs() {
-  static bool done = false;
-  if (done) return;
-  done = true;
+  static std::once_flag once;
+  std::call_once(once, set_smem_attrs_once<R>);
+}
+
+template <typename R>
+static void set_smem_attrs_once() {
   set_p2_attrs<R>();
   const int mx = CM_SMEM_DYN_MAX;
   const int carve = cudaSharedmemCarveoutMaxShared;
