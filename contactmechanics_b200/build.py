@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "lib", "libcm_b200.so")
-SOURCES = ["cm_plan.cu", "cm_p2.cu", "cm_op_p2.cu", "cm_batch.cu"]  # compiled in parallel
+SOURCES = ["cm_plan.cu", "cm_op_p2.cu", "cm_batch.cu"]  # compiled in parallel
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -3,8 +3,8 @@
 // value, blocks of 2*NP rows walking their tiles with a grid stride, the
 // pair-major spectrum stored and loaded straight from the transform
 // registers (the column pass splits and packs the row pairs).  The
-// solver's element-wise work rides on the transforms as in the per-pass
-// kernels of cm_kernels_p2.cuh (same formulas):
+// solver's element-wise work rides on the transforms with the formulas of
+// the per-pass kernels of cm_kernels.cuh:
 //
 //   k_ccg_row_fwd<MODE_T>  search direction t (ConstrainedConjugateGradients.py
 //                          :276-279), sum c g t, rows of the topography;

@@ -1,6 +1,6 @@
 // Host-side declarations shared by the translation units of the library:
-// launchers of the power-of-two FFT passes (cm_p2.cu, cm_op_p2.cu) and the
-// types their callers need.
+// launchers of the power-of-two passes (cm_op_p2.cu), of the persistent batch
+// kernel (cm_batch.cu) and the types their callers need.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -15,21 +15,6 @@
 #define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 // the by-value operator and solver passes also cover 2^13
 #define CM_OP_P2_CASES(X) CM_P2_CASES(X) X(13)
-
-// Launch one power-of-two pass of the CCG iteration (MODE_T or MODE_F) for
-// sides 2^logn; false if logn has no specialisation.
-template <typename R, int MODE>
-bool p2_row_fwd(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
-                const int2* it);
-template <typename R, int MODE>
-bool p2_col(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
-            const int2* it);
-template <typename R, int MODE>
-bool p2_row_inv(int logn, int grid, int threads, size_t smem, cudaStream_t s, const Slot<R>* S,
-                const int2* it);
-// Shared-memory attributes of every power-of-two pass (once per process).
-template <typename R>
-void set_p2_attrs();
 
 // The plain operator on power-of-two domains (cm_op_p2.cuh): three launches
 // on stream s.  op_p2_supported: whether sides 2^logx x 2^logy with column

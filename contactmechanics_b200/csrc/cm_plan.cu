@@ -106,8 +106,6 @@ struct Tiles {
   bool generic_ok;                  // the per-pass kernels fit (else only the by-value passes)
   int row_tile, col_tile, lw, comp_rows;
   int threads_row, threads_col;
-  bool p2;                          // both sides 2^6..2^12: specialised transforms
-  int p2_threads_row, p2_threads_col;
   size_t smem_row, smem_col;
   int ntile_cols;  // number of spectrum column tiles
 };
@@ -146,8 +144,9 @@ static int tuned_elems(size_t csize, int length, int dflt) {
 // and its buffers do not fit (FP64 sides of 8192), generic_ok is false and
 // only the power-of-two by-value passes can serve the plan.
 static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, Tiles* t) {
-  // 2048 transform elements per tile: 256 threads for the register-resident
-  // transforms, so two blocks share an SM and overlap memory with compute
+  // 2048 transform elements per tile by default (the autotuner's table sets
+  // others per sequence length): several blocks share an SM and overlap
+  // memory with compute
   const size_t elems_max = CM_SMEM_ROW / (2 * csize);
   const size_t elems = std::min<size_t>(elems_max, 2048);
   const size_t relems = std::min<size_t>(std::max(tuned_elems(csize, ny, (int)elems), 1), elems_max);
@@ -169,22 +168,6 @@ static int choose_tiles(int nx, int ny, int nyh, int tx, int ty, size_t csize, T
   t->threads_col = pow2_threads(((size_t)1 << lw) * nx);
   t->ntile_cols = (nyh + t->col_tile - 1) / t->col_tile;
   t->comp_rows = std::max(1, std::min(tx, CM_COMP_ELEMS / std::max(1, ty)));
-  // register-resident power-of-two transforms: one thread per 8 elements;
-  // their shared buffers carry one padding slot per 8 elements
-  t->p2_threads_row = np * (ny / 8);
-  t->p2_threads_col = (1 << lw) * (nx / 8);
-  const size_t p2row = (size_t)(2 * smem_padded(np * ny) + ny) * csize;
-  const size_t p2col = (size_t)(2 * smem_padded((1 << lw) * nx) + nx) * csize;
-  // the FP64 power-of-two kernels are compiled for at most half the threads
-  const int p2max = csize == 16 ? CM_FFT_THREADS / 2 : CM_FFT_THREADS;
-  auto is_p2 = [](int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; };
-  t->p2 = is_p2(nx) && is_p2(ny) && t->p2_threads_row >= 32 && t->p2_threads_row <= p2max &&
-          t->p2_threads_col >= 32 && t->p2_threads_col <= p2max && p2row <= CM_SMEM_DYN_MAX &&
-          p2col <= CM_SMEM_DYN_MAX;
-  if (t->p2) {
-    t->smem_row = std::max(t->smem_row, p2row);
-    t->smem_col = std::max(t->smem_col, p2col);
-  }
   return CM_OK;
 }
 
@@ -607,7 +590,6 @@ static void set_smem_attrs() {
 
 template <typename R>
 static void set_smem_attrs_once() {
-  set_p2_attrs<R>();
   const int mx = CM_SMEM_DYN_MAX;
   const int carve = cudaSharedmemCarveoutMaxShared;
   cudaFuncSetAttribute(k_row_fwd<R, MODE_T>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
@@ -970,7 +952,6 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     elementwise(k_ccg_gsum<R>, 1);
   }
   mark();
-  const bool p2 = T.p2;
   const int ly = p->fy.n, lx = p->fx.n;
   const int ry = log2_exact(ly), rx = log2_exact(lx);
   if (w.by_value) {
@@ -996,25 +977,19 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
     mark();
     return;
   }
-  if (!(p2 && p2_row_fwd<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
-    k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  k_row_fwd<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
-  if (!(p2 && p2_col<R, MODE_T>(rx, w.nt_col, T.p2_threads_col, T.smem_col, s, S, it)))
-    k_col<R, MODE_T><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  k_col<R, MODE_T><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
   mark();
-  if (!(p2 && p2_row_inv<R, MODE_T>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
-    k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  k_row_inv<R, MODE_T><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
   k_ccg_update<R><<<w.nt_comp, CM_THREADS, 0, s>>>(S, it, 0);
   mark();
-  if (!(p2 && p2_row_fwd<R, MODE_F>(ry, w.nt_rowt, T.p2_threads_row, T.smem_row, s, S, it)))
-    k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
+  k_row_fwd<R, MODE_F><<<w.nt_rowt, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
-  if (!(p2 && p2_col<R, MODE_F>(rx, w.nt_col, T.p2_threads_col, T.smem_col, s, S, it)))
-    k_col<R, MODE_F><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
+  k_col<R, MODE_F><<<w.nt_col, T.threads_col, T.smem_col, s>>>(S, it);
   mark();
-  if (!(p2 && p2_row_inv<R, MODE_F>(ry, w.nt_rowd, T.p2_threads_row, T.smem_row, s, S, it)))
-    k_row_inv<R, MODE_F><<<w.nt_rowd, T.threads_row, T.smem_row, s>>>(S, it);
+  k_row_inv<R, MODE_F><<<w.nt_rowd, T.threads_row, T.smem_row, s>>>(S, it);
   mark();
 }
 
