@@ -626,7 +626,7 @@ def c5_requests(n, seed):
     return out
 
 
-def run_serving(n_requests=200, seed=7):
+def run_serving(n_requests=200, seed=7, **server_kw):
     """Capacity of the serving loop on `n_requests` requests of the serving
     mix (a closed loop: every request submitted at once), then the same
     requests as an open-loop Poisson stream at 80 % of that capacity: p50 /
@@ -655,7 +655,7 @@ def run_serving(n_requests=200, seed=7):
             kw["forcetol"] = 1e-9 * p
         return kw
 
-    srv = ContactServer(iters_per_step=8)
+    srv = ContactServer(iters_per_step=8, **server_kw)
     # warm-up: one request of every kind and side, so plans, tables and kernels exist
     warm = []
     for kind, sides in (("periodic", C5_SIDES), ("free", C5_FREE_SIDES)):
