@@ -1105,11 +1105,12 @@ static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const Solve
                    double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
                    int prof_iters = 0, float* prof_ms = nullptr, bool topo_u = false) {
   cudaStream_t s = p->stream;
+  CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   // topo_u (FP32 phase of a mixed solve): the displacement pass updates
   // the topography's rows only and forms the next iteration's G as well
+  // (set after ccg_init, whose first call on a plan initialises the arguments)
   w.ccg_args.u_rows = topo_u ? p->tx : p->nx;
   w.ccg_args.fuse_gsum = topo_u ? 1 : 0;
-  CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   if (w.by_value) {
     // start of the first iteration; later ones come from k_ccg_row_inv<MODE_F>
     k_ccg_begin<R><<<w.ew_grid[0], CM_THREADS, 0, s>>>(w.d_ccg, p->items, w.nt_comp);
