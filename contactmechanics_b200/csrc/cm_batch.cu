@@ -41,7 +41,9 @@
 #include "cm_kernels.cuh"
 #include "cm_launch.h"
 
+#ifndef CM_BATCH_CLUSTER
 #define CM_BATCH_CLUSTER 8     // blocks per cluster (the portable maximum)
+#endif
 #ifndef CM_BATCH_THREADS
 #define CM_BATCH_THREADS 256
 #endif
