@@ -14,9 +14,20 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "cm_b200.h"
 #include "cm_kernels.cuh"
 #include "cm_launch.h"
+
+// Named range of a timeline (NVTX): the library's entry points and solve
+// phases show up in profilers that record NVTX (no cost without one).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 #define CM_SMEM_ROW (64 * 1024)   // ping-pong buffers of a row tile
 #define CM_COMP_ELEMS 2048
@@ -1104,6 +1115,7 @@ template <typename R>
 static int run_ccg(cm_plan* p, Work<R>& w, const cm_ccg_params* prm, const SolveInput& in,
                    double rel_pentol, double rel_forcetol, int maxiter, CcgState* fin,
                    int prof_iters = 0, float* prof_ms = nullptr, bool topo_u = false) {
+  NvtxRange range(sizeof(R) == 8 ? "ccg phase fp64" : "ccg phase fp32");
   cudaStream_t s = p->stream;
   CKS(ccg_init(p, w, prm, in, rel_pentol, rel_forcetol, maxiter, s));
   // topo_u (FP32 phase of a mixed solve): the displacement pass updates
@@ -1451,6 +1463,7 @@ static int lockstep_phase(int n, cm_plan* const* plans, const cm_ccg_params* par
                           double rel_forcetol, const std::vector<int>& maxiters, bool final,
                           bool bisect, int maxiter_all, double timeout, cudaStream_t s, int* polls,
                           std::vector<CcgState>& out) {
+  NvtxRange range(sizeof(R) == 8 ? "batch phase fp64" : "batch phase fp32");
   set_smem_attrs<R>();
   for (int i = 0; i < n; ++i) CKS(ensure_ccg(plans[i], work_of<R>(plans[i])));
   BatchDev<R> b;
@@ -1803,6 +1816,7 @@ const char* cm_status_string(int status) {
 }
 
 int cm_plan_create(const cm_plan_desc* desc, void* stream, cm_plan** out) {
+  NvtxRange range("cm_plan_create");
   if (!desc || !out) return CM_ERR_ARG;
   *out = nullptr;
   if (desc->kind != CM_PERIODIC && desc->kind != CM_FREE && desc->kind != CM_SEMI) return CM_ERR_ARG;
@@ -1955,6 +1969,7 @@ int cm_plan_greens_host(cm_plan* p, double* out) {
 
 int cm_apply(cm_plan* p, int op, int precision, const void* in, int in_rows, int in_cols, int in_ld,
              void* out, int out_rows, int out_cols, int out_ld, void* stream) {
+  NvtxRange range("cm_apply");
   if (!p || !in || !out) return CM_ERR_ARG;
   if (op != CM_OP_DISP && op != CM_OP_FORCE) return CM_ERR_ARG;
   if (precision != CM_FP64 && precision != CM_FP32) return CM_ERR_ARG;
@@ -1968,6 +1983,7 @@ int cm_apply(cm_plan* p, int op, int precision, const void* in, int in_rows, int
 int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const double* u0,
                  const double* f0, double* x, double* jac, unsigned char* active,
                  unsigned char* plastic, cm_ccg_result* res) {
+  NvtxRange range("cm_ccg_solve");
   if (!p || !prm || !h || !res) return CM_ERR_ARG;
   if (prm->precision != CM_FP64 && prm->precision != CM_FP32 && prm->precision != CM_MIXED) return CM_ERR_ARG;
   if (prm->maxiter < 1) return CM_ERR_ARG;
@@ -2064,6 +2080,7 @@ static int batch_persistent(int n, cm_plan* const* plans, const cm_ccg_params* p
                             const double* const* h, const double* const* u0, double* const* x,
                             double* const* jac, unsigned char* const* active,
                             unsigned char* const* plastic, cm_ccg_result* res, cudaStream_t s) {
+  NvtxRange range("batch persistent kernel");
   typedef std::chrono::steady_clock clk;
   const auto t0 = clk::now();
   const int prec = params[0].precision;
@@ -2167,6 +2184,7 @@ int cm_ccg_solve_batch(int n, cm_plan* const* plans, const cm_ccg_params* params
                        const double* const* h, const double* const* u0, double* const* x,
                        double* const* jac, unsigned char* const* active,
                        unsigned char* const* plastic, cm_ccg_result* res, void* stream) {
+  NvtxRange range("cm_ccg_solve_batch");
   if (n < 1 || !plans || !params || !h || !res) return CM_ERR_ARG;
   const int prec = params[0].precision;
   bool bisect = false;
@@ -2296,6 +2314,7 @@ int cm_ccg_begin(cm_stepper* stp, cm_plan* p, const cm_ccg_params* prm, const do
 }
 
 int cm_ccg_step(cm_stepper* stp, int n, cm_plan* const* plans, int iters, int* done) {
+  NvtxRange range("cm_ccg_step");
   if (!stp || n < 0 || (n > 0 && (!plans || !done)) || iters < 1) return CM_ERR_ARG;
   std::vector<cm_plan*> g32, g64;
   std::vector<int> i32, i64;
