@@ -40,8 +40,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
     mbar_init(&mbar, 1);
     mbar_init_fence();
   }
-  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
-  const C* tw = Sh::ONEBUF ? a.op.twy : tws;
+  const C* tw = stage_twiddles<LOGN, Sh::LR, Sh::THREADS, Sh::ONEBUF>(tws, a.op.twy);
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;
@@ -222,8 +221,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
   C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.op.twy);
-  const C* tw = Sh::ONEBUF ? a.op.twy : tws;
+  const C* tw = stage_twiddles<LOGN, Sh::LR, Sh::THREADS, Sh::ONEBUF>(tws, a.op.twy);
   pdl_wait();
   CcgState* st = a.st;
   if (st->done) return;

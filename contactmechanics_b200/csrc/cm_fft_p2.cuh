@@ -99,20 +99,52 @@ CM_DEVINL void dft_rr(C* v) {
 
 // Per-stage twiddle tables for 2^LR elements per thread: stage s (Ns butterfly
 // groups) holds tw[toff(s) + (q-1)*Ns + k] = W^(q k N/(RAD Ns)), q = 1..RAD-1,
-// k < Ns; at most N entries in all.  Entries of the table tw_n[m] = W^m.
-template <int LOGN, int LR, typename C>
+// k < Ns; N - FIRST entries in all (toff(s) = Ns - FIRST).  Entries of the
+// table tw_n[m] = W^m.
+
+// index into tw_n of staged entry i
+template <int LOGN, int LR>
+CM_DEVINL int tw_stage_index(int i) {
+  typedef P2PlanR<LOGN, LR> P;
+  constexpr int N = P::N;
+  // Ns = FIRST * RAD^j with Ns <= i + FIRST < Ns * RAD
+  const int lg = 31 - __clz(i + P::FIRST);  // floor(log2(i + FIRST))
+  const int j = (lg - P::FL) / LR;
+  const int lns = P::FL + j * LR, Ns = 1 << lns;
+  const int r = i - (Ns - P::FIRST);
+  const int q = 1 + (r >> lns), k = r & (Ns - 1);
+  const int lstep = LOGN - lns - LR;  // step = N / (Ns RAD)
+  return (q * k << lstep) & (N - 1);
+}
+
+// Stage the tables with NT threads a block: every thread issues all of its
+// loads before its first store, so the staging costs one round trip.
+template <int LOGN, int LR, int NT, typename C>
 CM_DEVINL void stage_tw_p2r(C* tws, const C* __restrict__ tw_n) {
   typedef P2PlanR<LOGN, LR> P;
-  constexpr int N = P::N, RAD = P::RAD;
-  int toff = 0;
+  constexpr int TOT = P::N - P::FIRST, PER = (TOT + NT - 1) / NT;
+  C w[PER];
 #pragma unroll
-  for (int s = 1, Ns = P::FIRST; s < P::NST; ++s, Ns *= RAD) {
-    const int step = N / (Ns * RAD);
-    for (int i = threadIdx.x; i < (RAD - 1) * Ns; i += blockDim.x) {
-      const int q = 1 + i / Ns, k = i & (Ns - 1);
-      tws[toff + i] = __ldg(tw_n + ((q * k * step) & (N - 1)));
-    }
-    toff += (RAD - 1) * Ns;
+  for (int r = 0; r < PER; ++r) {
+    const int i = threadIdx.x + r * NT;
+    if (i < TOT) w[r] = __ldg(tw_n + tw_stage_index<LOGN, LR>(i));
+  }
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int i = threadIdx.x + r * NT;
+    if (i < TOT) tws[i] = w[r];
+  }
+}
+
+// Twiddle staging of a pass with NT threads a block; returns the table the
+// transforms take (tw_n itself when ONEBUF: those transforms read it directly).
+template <int LOGN, int LR, int NT, bool ONEBUF, typename C>
+CM_DEVINL const C* stage_twiddles(C* tws, const C* __restrict__ tw_n) {
+  if constexpr (ONEBUF) {
+    return tw_n;
+  } else {
+    stage_tw_p2r<LOGN, LR, NT>(tws, tw_n);
+    return tws;
   }
 }
 

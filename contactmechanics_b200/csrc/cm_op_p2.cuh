@@ -163,8 +163,7 @@ k_op_row_fwd(OpArgs<R> a) {
   C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
-  const C* tw = Sh::ONEBUF ? a.twy : tws;
+  const C* tw = stage_twiddles<LOGN, Sh::LR, Sh::THREADS, Sh::ONEBUF>(tws, a.twy);
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
@@ -264,8 +263,7 @@ k_op_col(OpArgs<R> a) {
   C* bufA = Sh::ONEBUF ? tws : tws + NX;
   C* bufB = bufA + smem_padded(Sh::NG * NX * W);
   pdl_trigger();
-  if (!Sh::ONEBUF) stage_tw_p2r<LOGX, Sh::LR>(tws, a.twx);
-  const C* tw = Sh::ONEBUF ? a.twx : tws;
+  const C* tw = stage_twiddles<LOGX, Sh::LR, Sh::THREADS, Sh::ONEBUF>(tws, a.twx);
   pdl_wait();
   if (a.st && (a.st->done || (a.cg_only && a.st->branch != 0))) return;
   __syncthreads();
@@ -318,8 +316,7 @@ k_op_row_inv(OpArgs<R> a) {
   C* bufA = Sh::ONEBUF ? tws : tws + N;
   C* bufB = bufA + smem_padded(NP * N);
   pdl_trigger();
-  if (!Sh::ONEBUF) stage_tw_p2r<LOGN, Sh::LR>(tws, a.twy);
-  const C* tw = Sh::ONEBUF ? a.twy : tws;
+  const C* tw = stage_twiddles<LOGN, Sh::LR, Sh::THREADS, Sh::ONEBUF>(tws, a.twy);
   pdl_wait();
   __syncthreads();
   const int s = threadIdx.x >> P::LTPS, tt = threadIdx.x & (P::TPS - 1);
