@@ -104,6 +104,7 @@ SIGNATURES = {
     "cm_plan_create": (_i, [ctypes.POINTER(PlanDesc), _vp, ctypes.POINTER(_vp)]),
     "cm_plan_destroy": (_i, [_vp]),
     "cm_plan_shape": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "cm_plan_engine": (_i, [_vp, _i, ctypes.POINTER(_i)]),
     "cm_plan_greens_host": (_i, [_vp, _vp]),
     "cm_apply": (_i, [_vp, _i, _i, _vp, _i, _i, _i, _vp, _i, _i, _i, _vp]),
     "cm_ccg_solve": (_i, [_vp, ctypes.POINTER(CcgParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp,

@@ -27,8 +27,8 @@ template <typename R, int MODE, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_ccg_row_fwd(CcgArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
+  typedef typename Sh::P P;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long mbar;
@@ -181,11 +181,11 @@ k_ccg_row_fwd(CcgArgs<R> a) {
     C v[Sh::E];
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
-    fft_p2x<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (xa < tx) {
-      C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N + tt;
+      C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N;
 #pragma unroll
-      for (int q = 0; q < Sh::E; ++q) srow[q * P::TPS] = v[q];
+      for (int q = 0; q < Sh::E; ++q) srow[kfreq<LOGN, Sh::LR>(tt, q)] = v[q];
     }
     __syncthreads();  // buffers free for the next tile
   }
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(InvShape<R, MODE, LOGN>::THREADS, InvShape<R, 
 k_ccg_row_inv(CcgArgs<R> a) {
   typedef typename CT<R>::C C;
   typedef InvShape<R, MODE, LOGN> Sh;
-  typedef P2PlanR<LOGN, Sh::LR> P;
+  typedef typename Sh::P P;
   constexpr int N = P::N, NP = Sh::NP, ROWS = 2 * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
@@ -252,12 +252,12 @@ k_ccg_row_inv(CcgArgs<R> a) {
     const int xa = x0 + 2 * s;
     C v[Sh::E];
     {
-      const C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N + tt;
+      const C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N;
       const bool have = xa < rows_total;
 #pragma unroll
-      for (int q = 0; q < Sh::E; ++q) v[q] = have ? srow[q * P::TPS] : czero<C>();
+      for (int q = 0; q < Sh::E; ++q) v[q] = have ? srow[kfreq<LOGN, Sh::LR>(tt, q)] : czero<C>();
     }
-    fft_p2x<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (MODE == MODE_T) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) {
@@ -356,7 +356,8 @@ k_ccg_row_inv(CcgArgs<R> a) {
 
 // ---------------------------------------------------------------------------
 // Element-wise passes of the single-solve path, vectorised.  The topography
-// fields (h, f, t: tx x ty, rows of a power-of-two length ty >= 64) and the
+// fields (h, f, t: tx x ty, rows of a length ty >= 64 that is a multiple of
+// four) and the
 // displacement (u: rows of length ny on the domain) are read in 16-byte
 // vectors of V = 16 / sizeof(R) consecutive elements of one row; every
 // thread has U vectors of each field in flight, the grid is one resident
@@ -372,34 +373,49 @@ struct alignas(16) Vec16 {
 
 #define CM_EW_THREADS 256
 
-// vector j of the topography: element index (topography) and displacement index
+// vector j of the topography: element index (topography) and displacement
+// index.  P2: the vectors per topography row are a power of two (a shift
+// finds the row), else a multiply-shift division does.
+template <bool P2>
 struct EwIndex {
-  int lvr;      // log2 of the vectors per topography row
+  int lvr;      // log2 of the vectors per topography row (P2)
+  FastDiv vpr;  // vectors per topography row
   int ny;       // displacement row length
   int V;
   CM_DEVINL void at(long j, size_t& ic, size_t& iu) const {
-    const long x = j >> lvr;
-    const long y = (j - (x << lvr)) * V;
+    long x, y;
+    if constexpr (P2) {
+      x = j >> lvr;
+      y = (j - (x << lvr)) * V;
+    } else {
+      x = fdiv(vpr, (int)j);
+      y = (j - x * (long)vpr.d) * V;
+    }
     ic = (size_t)j * V;
     iu = (size_t)x * ny + y;
   }
 };
 
-template <typename R>
-CM_DEVINL EwIndex ew_index(const CcgArgs<R>& a) {
-  EwIndex e;
+template <bool P2, typename R>
+CM_DEVINL EwIndex<P2> ew_index(const CcgArgs<R>& a) {
+  EwIndex<P2> e;
   e.V = Vec16<R>::V;
-  e.lvr = (__ffs(a.ty) - 1) - (__ffs(Vec16<R>::V) - 1);
+  e.vpr = a.ew_vpr;
+  e.lvr = __ffs(e.vpr.d) - 1;
   e.ny = a.ny;
   return e;
 }
 
+// whether the element-wise passes of a solve take the shift (EwIndex<true>)
+template <typename R>
+inline bool ew_pow2(const CcgArgs<R>& a) { return (a.ew_vpr.d & (a.ew_vpr.d - 1)) == 0; }
+
 // G = sum over the CG area of g^2 (ConstrainedConjugateGradients.py:273-279)
-template <typename R, int U>
+template <typename R, int U, bool P2>
 __global__ void __launch_bounds__(CM_EW_THREADS) k_ew_gsum(CcgArgs<R> a) {
   typedef Vec16<R> VR;
   constexpr int V = VR::V;
-  const EwIndex ix = ew_index(a);
+  const EwIndex<P2> ix = ew_index<P2>(a);
   const long nvec = (long)a.tx * a.ty / V;
   pdl_trigger();
   pdl_wait();
@@ -448,11 +464,11 @@ __global__ void __launch_bounds__(CM_EW_THREADS) k_ew_gsum(CcgArgs<R> a) {
 
 // Force update, projection onto [0, H] and the constraint bookkeeping
 // (ConstrainedConjugateGradients.py:296, 320-389)
-template <typename R, int U>
+template <typename R, int U, bool P2>
 __global__ void __launch_bounds__(CM_EW_THREADS) k_ew_update(CcgArgs<R> a) {
   typedef Vec16<R> VR;
   constexpr int V = VR::V;
-  const EwIndex ix = ew_index(a);
+  const EwIndex<P2> ix = ew_index<P2>(a);
   const long nvec = (long)a.tx * a.ty / V;
   pdl_trigger();
   pdl_wait();

@@ -44,6 +44,40 @@ struct P2PlanR {
   static constexpr int NST = 1 + (LOGN - FL) / LR;
 };
 
+// Transform lengths of the register-resident passes, by code: L < 32 is
+// N = 2^L, L = 32 + m is N = 3 * 2^m.
+#define CM_T3(m) (32 + (m))
+template <int L>
+struct LenCode {
+  static constexpr int F = L >= 32 ? 3 : 1;
+  static constexpr int LOGM = L >= 32 ? L - 32 : L;
+  static constexpr int M = 1 << LOGM;
+  static constexpr int N = F * M;
+};
+
+// Thread layout of a length-N transform with 2^LR elements of each of its F
+// power-of-two parts per thread: thread tt of a sequence owns the E elements
+// at time index tt + q TPS, q < E.
+template <int L, int LR>
+struct FftLen {
+  static constexpr int F = LenCode<L>::F, LOGM = LenCode<L>::LOGM;
+  static constexpr int M = LenCode<L>::M, N = LenCode<L>::N;
+  static constexpr int RAD = 1 << LR;
+  static constexpr int E = F * RAD;    // elements per thread
+  static constexpr int TPS = M / RAD;  // threads per sequence
+  static constexpr int LTPS = LOGM - LR;
+};
+
+// Frequency index of register q after a forward transform (and of the input
+// of an inverse one): tt + q TPS for N = 2^L; for N = 3M the radix-3 split
+// leaves X(3k + j) in register j RAD + qq with k = tt + qq TPS.
+template <int L, int LR>
+CM_DEVINL int kfreq(int tt, int q) {
+  typedef FftLen<L, LR> P;
+  if constexpr (P::F == 1) return tt + q * P::TPS;
+  else return 3 * (tt + (q & (P::RAD - 1)) * P::TPS) + (q >> LR);
+}
+
 // a * W16^M (W16 = exp(-2 pi i / 16); conjugate for the inverse), M in
 // {1, 2, 3, 4, 6, 9}: the internal twiddles of the length-16 DFT
 template <bool INV, int M, typename C>
@@ -136,51 +170,81 @@ CM_DEVINL void stage_tw_p2r(C* tws, const C* __restrict__ tw_n) {
   }
 }
 
-// Twiddle staging of a pass with NT threads a block; returns the table the
-// transforms take (tw_n itself when ONEBUF: those transforms read it directly).
-template <int LOGN, int LR, int NT, bool ONEBUF, typename C>
+// Tables of a length-3M transform (M = 2^LOGM): the sub-transforms' tables
+// of stage_tw_p2r for length M (W_M^m = W_N^(3m) of the length-N table tw_n)
+// followed by W_N^m for m < 2M, the twiddles of the radix-3 split.
+template <int LOGM, int LR, int NT, typename C>
+CM_DEVINL void stage_tw_t3(C* tws, const C* __restrict__ tw_n) {
+  typedef P2PlanR<LOGM, LR> P;
+  constexpr int M = P::N, SUB = M - P::FIRST, TOT = SUB + 2 * M, PER = (TOT + NT - 1) / NT;
+  C w[PER];
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int i = threadIdx.x + r * NT;
+    if (i < TOT) w[r] = __ldg(tw_n + (i < SUB ? 3 * tw_stage_index<LOGM, LR>(i) : i - SUB));
+  }
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int i = threadIdx.x + r * NT;
+    if (i < TOT) tws[i] = w[r];
+  }
+}
+
+// Twiddle staging of a pass with NT threads a block for length code L;
+// returns the table the transforms take (tw_n itself when ONEBUF: those
+// transforms read it directly).
+template <int L, int LR, int NT, bool ONEBUF, typename C>
 CM_DEVINL const C* stage_twiddles(C* tws, const C* __restrict__ tw_n) {
   if constexpr (ONEBUF) {
+    static_assert(LenCode<L>::F == 1, "lengths 3 * 2^m keep both transform buffers");
     return tw_n;
+  } else if constexpr (LenCode<L>::F == 1) {
+    stage_tw_p2r<L, LR, NT>(tws, tw_n);
+    return tws;
   } else {
-    stage_tw_p2r<LOGN, LR, NT>(tws, tw_n);
+    stage_tw_t3<LenCode<L>::LOGM, LR, NT>(tws, tw_n);
     return tws;
   }
 }
 
-// Transform the thread's RAD elements {tt + q N/RAD} of one sequence in
-// place (tables of stage_tw_p2r; the result is left in v with no pending
-// shared-memory reads).
-template <typename C, bool INV, int LOGN, int LR>
-CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int tt,
+// Transform G sequences of the thread's RAD elements {tt + q N/RAD} each in
+// place: group g is v[g RAD .. g RAD + RAD - 1] and lives at shared offset
+// base + g gstride (tables of stage_tw_p2r; the result is left in v with no
+// pending shared-memory reads).  The groups share every barrier.
+template <typename C, bool INV, int LOGN, int LR, int G>
+CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int estride, int tt,
                        const C* tw) {
   typedef P2PlanR<LOGN, LR> P;
   constexpr int RAD = P::RAD;
-  {
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
     constexpr int R = P::FIRST;
     constexpr int B = RAD / R;
+    C* vg = v + g * RAD;
+    const int bg = base + g * gstride;
     C o[RAD];
 #pragma unroll
     for (int i = 0; i < B; ++i) {
-      C g[R];
+      C e[R];
 #pragma unroll
-      for (int q = 0; q < R; ++q) g[q] = v[i + B * q];
-      dft_rr<INV, R>(g);
+      for (int q = 0; q < R; ++q) e[q] = vg[i + B * q];
+      dft_rr<INV, R>(e);
 #pragma unroll
-      for (int q = 0; q < R; ++q) o[i * R + q] = g[q];
+      for (int q = 0; q < R; ++q) o[i * R + q] = e[q];
     }
     if (P::NST == 1) {
 #pragma unroll
-      for (int i = 0; i < RAD; ++i) v[i] = o[i];
-      return;
+      for (int i = 0; i < RAD; ++i) vg[i] = o[i];
+      continue;
     }
 #pragma unroll
     for (int i = 0; i < B; ++i) {
       const int j = tt + i * P::TPS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) sA[spad(base + (j * R + q) * estride)] = o[i * R + q];
+      for (int q = 0; q < R; ++q) sA[spad(bg + (j * R + q) * estride)] = o[i * R + q];
     }
   }
+  if (P::NST == 1) return;
   __syncthreads();
   C* src = sA;
   C* dst = sB;
@@ -189,23 +253,29 @@ CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int
 #pragma unroll
   for (int s = 1; s < P::NST; ++s) {
     const int k = tt & (Ns - 1);
-    C g[RAD];
 #pragma unroll
-    for (int q = 0; q < RAD; ++q) g[q] = src[spad(base + (tt + q * P::TPS) * estride)];
+    for (int g = 0; g < G; ++g) {
+      const int bg = base + g * gstride;
+      C e[RAD];
 #pragma unroll
-    for (int q = 1; q < RAD; ++q) {
-      const C w = tw[toff + (q - 1) * Ns + k];
-      g[q] = INV ? cmulc(g[q], w) : cmul(g[q], w);
+      for (int q = 0; q < RAD; ++q) e[q] = src[spad(bg + (tt + q * P::TPS) * estride)];
+#pragma unroll
+      for (int q = 1; q < RAD; ++q) {
+        const C w = tw[toff + (q - 1) * Ns + k];
+        e[q] = INV ? cmulc(e[q], w) : cmul(e[q], w);
+      }
+      dft_rr<INV, RAD>(e);
+      if (s == P::NST - 1) {
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) v[g * RAD + q] = e[q];
+      } else {
+        const int ob = (tt - k) * RAD + k;
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) dst[spad(bg + (ob + q * Ns) * estride)] = e[q];
+      }
     }
     toff += (RAD - 1) * Ns;
-    dft_rr<INV, RAD>(g);
-    if (s == P::NST - 1) {
-#pragma unroll
-      for (int q = 0; q < RAD; ++q) v[q] = g[q];
-    } else {
-      const int ob = (tt - k) * RAD + k;
-#pragma unroll
-      for (int q = 0; q < RAD; ++q) dst[spad(base + (ob + q * Ns) * estride)] = g[q];
+    if (s < P::NST - 1) {
       __syncthreads();
       C* t = src;
       src = dst;
@@ -213,6 +283,13 @@ CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int
     }
     Ns *= RAD;
   }
+}
+
+// One sequence: the thread's RAD elements {tt + q N/RAD}.
+template <typename C, bool INV, int LOGN, int LR>
+CM_DEVINL void fft_p2r(C (&v)[1 << LR], C* sA, C* sB, int base, int estride, int tt,
+                       const C* tw) {
+  fft_p2g<C, INV, LOGN, LR, 1>(v, sA, sB, base, 0, estride, tt, tw);
 }
 
 // The same transform for lengths whose ping-pong buffers and staged twiddle
@@ -287,4 +364,64 @@ CM_DEVINL void fft_p2x(C (&v)[1 << LR], C* bufA, C* bufB, int base, int estride,
                        const C* tw) {
   if constexpr (ONEBUF) fft_p2r_1buf<C, INV, LOGN, LR>(v, bufA, base, estride, tt, tw);
   else fft_p2r<C, INV, LOGN, LR>(v, bufA, bufB, base, estride, tt, tw);
+}
+
+// Length N = 3M (M = 2^LOGM).  The thread's elements v[qq + r RAD] (qq < RAD,
+// r < 3) sit at time index n + r M with n = tt + qq M/RAD.
+// Forward: the radix-3 split by decimation in frequency, in registers,
+//   a_j(n) = W_N^(j n) sum_r W_3^(r j) x(n + r M),   j < 3,
+// then the three length-M transforms of a_j, which share their barriers:
+// X(3k + j) = sum_n W_M^(n k) a_j(n) is left in v[j RAD + qq], k = tt + qq M/RAD
+// (kfreq).  Inverse: the mirror image (length-M inverse transforms of
+// X(3k + j) over k, the twiddle W_N^(-j n), the radix-3 combination), again
+// unnormalised, leaving x(n + r M) in v[qq + r RAD].  Sub-sequence j lives at
+// shared offset base + j M estride; tw holds the tables of stage_tw_t3.
+template <typename C, bool INV, int LOGM, int LR>
+CM_DEVINL void fft_t3(C (&v)[3 << LR], C* sA, C* sB, int base, int estride, int tt, const C* tw) {
+  typedef P2PlanR<LOGM, LR> P;
+  typedef decltype(v[0].x) R;
+  constexpr int RAD = P::RAD, M = P::N;
+  const C* __restrict__ w3 = tw + (M - P::FIRST);  // W_N^m, m < 2M
+  const R s3 = (R)0.86602540378443864676;         // sqrt(3) / 2
+  const R half = (R)0.5;
+  if (!INV) {
+#pragma unroll
+    for (int qq = 0; qq < RAD; ++qq) {
+      const int n = tt + qq * P::TPS;
+      const C x0 = v[qq], x1 = v[qq + RAD], x2 = v[qq + 2 * RAD];
+      const C sm = cadd(x1, x2), df = csub(x1, x2);
+      const C md = cmake<C>(x0.x - half * sm.x, x0.y - half * sm.y);
+      const C rt = cmake<C>(s3 * df.y, -s3 * df.x);  // -i sqrt(3)/2 (x1 - x2)
+      v[qq] = cadd(x0, sm);
+      v[qq + RAD] = cmul(cadd(md, rt), w3[n]);
+      v[qq + 2 * RAD] = cmul(csub(md, rt), w3[2 * n]);
+    }
+    fft_p2g<C, false, LOGM, LR, 3>(v, sA, sB, base, M * estride, estride, tt, tw);
+  } else {
+    fft_p2g<C, true, LOGM, LR, 3>(v, sA, sB, base, M * estride, estride, tt, tw);
+#pragma unroll
+    for (int qq = 0; qq < RAD; ++qq) {
+      const int n = tt + qq * P::TPS;
+      const C y0 = v[qq];
+      const C y1 = cmulc(v[qq + RAD], w3[n]), y2 = cmulc(v[qq + 2 * RAD], w3[2 * n]);
+      const C sm = cadd(y1, y2), df = csub(y1, y2);
+      const C md = cmake<C>(y0.x - half * sm.x, y0.y - half * sm.y);
+      const C rt = cmake<C>(-s3 * df.y, s3 * df.x);  // +i sqrt(3)/2 (y1 - y2)
+      v[qq] = cadd(y0, sm);
+      v[qq + RAD] = cadd(md, rt);
+      v[qq + 2 * RAD] = csub(md, rt);
+    }
+  }
+}
+
+// The transform of length code L: fft_p2x for 2^L, fft_t3 for 3 * 2^m.
+template <typename C, bool INV, int L, int LR, bool ONEBUF>
+CM_DEVINL void fft_len(C (&v)[FftLen<L, LR>::E], C* bufA, C* bufB, int base, int estride, int tt,
+                       const C* tw) {
+  if constexpr (LenCode<L>::F == 1) {
+    fft_p2x<C, INV, L, LR, ONEBUF>(v, bufA, bufB, base, estride, tt, tw);
+  } else {
+    static_assert(!ONEBUF, "lengths 3 * 2^m keep both transform buffers");
+    fft_t3<C, INV, LenCode<L>::LOGM, LR>(v, bufA, bufB, base, estride, tt, tw);
+  }
 }

@@ -15,6 +15,9 @@
 #define CM_P2_CASES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 // the by-value operator and solver passes also cover 2^13
 #define CM_OP_P2_CASES(X) CM_P2_CASES(X) X(13)
+// and lengths 3 * 2^m, m = 5..11 (96..6144), by their length codes 32 + m
+#define CM_T3_CASES(X) X(37) X(38) X(39) X(40) X(41) X(42) X(43)
+#define CM_OP_LEN_CASES(X) CM_OP_P2_CASES(X) CM_T3_CASES(X)
 
 // The plain operator on power-of-two domains (cm_op_p2.cuh): three launches
 // on stream s.  op_p2_supported: whether sides 2^logx x 2^logy with column
@@ -63,6 +66,7 @@ struct CcgArgs {
   int fuse_gsum; // the displacement pass also forms the next iteration's G
                  // (FP32 phase of a mixed solve; the iterations then run
                  // without the gsum pass)
+  FastDiv ew_vpr;  // 16-byte vectors per topography row (element-wise passes)
 };
 // Launch with programmatic stream serialization: the kernel may start while
 // its predecessor on the stream finishes, and calls pdl_wait before reading
@@ -120,9 +124,10 @@ template <typename R>
 int ccg_p2_gsum(const CcgArgs<R>& a, cudaStream_t s, bool chained);
 template <typename R>
 int ccg_p2_update(const CcgArgs<R>& a, cudaStream_t s, bool chained);
-// Resident blocks per SM of those passes (for sizing a.ew_grid), or -1.
+// Resident blocks per SM of those passes as a's solve launches them (for
+// sizing a.ew_grid), or -1.
 template <typename R>
-int ccg_p2_ew_blocks_per_sm();
+int ccg_p2_ew_blocks_per_sm(const CcgArgs<R>& a);
 
 // The persistent batch kernel (cm_batch.cu): one launch over n jobs taken in
 // queue order `order` (next: a zeroed device counter), smem bytes of dynamic

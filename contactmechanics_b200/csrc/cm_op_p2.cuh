@@ -90,25 +90,45 @@
 #define CM_ROW_LR_F64 3
 #endif
 
-// default log2 elements per thread of the row passes: FP64 transforms of
-// length 2^13 take 16 elements per thread (512 threads a sequence)
+// log2 of the elements per thread of each power-of-two part of a length
+// 3 * 2^m (three parts, so a thread holds three times as many), and the
+// threads of a row-pass block for those lengths.  Four elements a part in
+// FP32 too: the solver passes' epilogues then keep their fields in
+// registers (mixed solves 8-20 % faster than with eight, periodic 768..3072).
+#ifndef CM_T3_LR_F32
+#define CM_T3_LR_F32 2
+#endif
+#ifndef CM_T3_LR_F64
+#define CM_T3_LR_F64 2
+#endif
+#ifndef CM_T3_ROW_BASE
+#define CM_T3_ROW_BASE 256
+#endif
+
+// default log2 elements per thread (per part) of the row passes for length
+// code L (cm_fft_p2.cuh): FP64 transforms of length 2^13 take 16 elements
+// per thread (512 threads a sequence)
 template <typename R>
-constexpr int row_lr(int logn) {
-  return sizeof(R) == 8 ? (logn >= 13 ? 4 : CM_ROW_LR_F64) : CM_ROW_LR_F32;
+constexpr int row_lr(int code) {
+  return code >= 32 ? (sizeof(R) == 8 ? CM_T3_LR_F64 : CM_T3_LR_F32)
+                    : sizeof(R) == 8 ? (code >= 13 ? 4 : CM_ROW_LR_F64) : CM_ROW_LR_F32;
 }
 
-// threads of one block of the row passes for transform length 2^LOGN with
-// 2^LRV elements per thread.  ONEBUF: the ping-pong buffers and the staged
-// twiddles do not fit a block's shared memory (FP64 at 2^13), so the
+// threads of one block of the row passes for the transform of length code
+// LOGN (2^LOGN, or 3 * 2^m for LOGN = CM_T3(m)) with 2^LRV elements of each
+// power-of-two part per thread.  ONEBUF: the ping-pong buffers and the
+// staged twiddles do not fit a block's shared memory (FP64 at 2^13), so the
 // transform runs on one buffer with the twiddles read from global memory.
 template <typename R, int LOGN, int LRV = row_lr<R>(LOGN)>
 struct OpShape {
   typedef typename CT<R>::C C;
-  static constexpr int N = 1 << LOGN;
+  typedef FftLen<LOGN, LRV> P;
+  static constexpr int N = P::N;
   static constexpr int LR = LRV;
-  static constexpr int E = 1 << LR;  // elements per thread
-  static constexpr int TPS = N >> LR;
-  static constexpr int BASE = (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
+  static constexpr int E = P::E;  // elements per thread
+  static constexpr int TPS = P::TPS;
+  static constexpr int BASE = P::F == 3 ? CM_T3_ROW_BASE
+                                        : (sizeof(R) == 8 ? 256 : CM_ROW_F32_BASE) >> (LR - 3);
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // row pairs per block
   static constexpr size_t BUF = (size_t)(NP * N + ((NP * N) >> 3) + 1) * sizeof(C);
@@ -122,15 +142,18 @@ struct OpShape {
   static size_t smem() { return SMEM; }
 };
 
-// Column pass for columns of length 2^LOGX: 16 elements per thread, groups of
-// W = 2^LW columns with the column index fastest across threads.
+// Column pass for columns of length code LOGX: 16 elements per thread for
+// 2^LOGX (3 x 2^LR for 3 * 2^m), groups of W = 2^LW columns with the column
+// index fastest across threads.
 template <typename R, int LOGX>
 struct ColShape {
   typedef typename CT<R>::C C;
-  static constexpr int NX = 1 << LOGX;
-  static constexpr int LR = sizeof(R) == 8 ? CM_COL_LR_F64 : CM_COL_LR_F32;
-  static constexpr int E = 1 << LR;  // elements per thread
-  static constexpr int TPS = NX / E;
+  static constexpr int LR = LenCode<LOGX>::F == 3 ? (sizeof(R) == 8 ? CM_T3_LR_F64 : CM_T3_LR_F32)
+                            : sizeof(R) == 8 ? CM_COL_LR_F64 : CM_COL_LR_F32;
+  typedef FftLen<LOGX, LR> P;
+  static constexpr int NX = P::N;
+  static constexpr int E = P::E;  // elements per thread
+  static constexpr int TPS = P::TPS;
   static constexpr size_t smem_for(int lw) {
     return (size_t)(NX + 2 * (((NX << lw)) + ((NX << lw) >> 3) + 1)) * sizeof(C);
   }
@@ -155,8 +178,8 @@ template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_op_row_fwd(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
+  typedef typename Sh::P P;
   constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
@@ -181,11 +204,11 @@ k_op_row_fwd(OpArgs<R> a) {
       }
       v[q] = cmake<C>(ra, rb);
     }
-    fft_p2x<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
     if (p < npairs) {
-      C* __restrict__ row = a.spec + (size_t)p * N + tt;
+      C* __restrict__ row = a.spec + (size_t)p * N;
 #pragma unroll
-      for (int q = 0; q < Sh::E; ++q) row[q * P::TPS] = v[q];
+      for (int q = 0; q < Sh::E; ++q) row[kfreq<LOGN, Sh::LR>(tt, q)] = v[q];
     }
     __syncthreads();  // buffers free for the next pairs
   }
@@ -203,11 +226,12 @@ CM_DEVINL void col_split_load(C (&v)[E], const C* __restrict__ spec, int ny, int
   const C* __restrict__ sk = spec + k + (size_t)(tt >> 1) * ny;
   const C* __restrict__ skm = spec + km + (size_t)(tt >> 1) * ny;
   const int pstep = (TPS / 2) * ny;
+  constexpr int CH = E % 8 == 0 ? 8 : 4;  // loads in flight per chunk
 #pragma unroll
-  for (int h = 0; h < E; h += 8) {
-    C z[8], zm[8];
+  for (int h = 0; h < E; h += CH) {
+    C z[CH], zm[CH];
 #pragma unroll
-    for (int q = h; q < h + 8; ++q) {
+    for (int q = h; q < h + CH; ++q) {
       const int x = tt + q * TPS;
       z[q - h] = czero<C>();
       zm[q - h] = czero<C>();
@@ -217,7 +241,7 @@ CM_DEVINL void col_split_load(C (&v)[E], const C* __restrict__ spec, int ny, int
       }
     }
 #pragma unroll
-    for (int q = h; q < h + 8; ++q) {
+    for (int q = h; q < h + CH; ++q) {
       const C zk = z[q - h], zn = zm[q - h];
       v[q] = b ? cmake<C>((zk.y + zn.y) * (R)0.5, (zn.x - zk.x) * (R)0.5)
                : cmake<C>((zk.x + zn.x) * (R)0.5, (zk.y - zn.y) * (R)0.5);
@@ -256,7 +280,7 @@ __global__ void __launch_bounds__(ColShape<R, LOGX>::THREADS, 1)
 k_op_col(OpArgs<R> a) {
   typedef typename CT<R>::C C;
   typedef ColShape<R, LOGX> Sh;
-  typedef P2PlanR<LOGX, Sh::LR> P;
+  typedef typename Sh::P P;
   constexpr int NX = P::N, W = Sh::W, LW = Sh::LW, E = Sh::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
@@ -278,27 +302,30 @@ k_op_col(OpArgs<R> a) {
   for (int g0 = blockIdx.x * Sh::NG; g0 < ngroups; g0 += gridDim.x * Sh::NG) {
     const int k = (g0 + j) * W + c;
     const bool ok = k < units;
-    const int km = (ny - k) & (ny - 1);
+    const int km = k == 0 ? 0 : ny - k;  // the mirror column (ny need not be a power of two)
     C v[E];
     col_split_load<C, P::TPS, E>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
-    fft_p2x<C, false, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
+    fft_len<C, false, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
     if (a.fwd_real) {
       // forward transform only: the real part of the 2D transform, in the
       // natural (nx, ny/2 + 1) layout (a real, even kernel's Green's table)
       if (ok) {
 #pragma unroll
-        for (int q = 0; q < E; ++q) a.fwd_real[(size_t)(tt + q * P::TPS) * units + k] = v[q].x;
+        for (int q = 0; q < E; ++q) a.fwd_real[(size_t)kfreq<LOGX, Sh::LR>(tt, q) * units + k] = v[q].x;
       }
       __syncthreads();
       continue;
     }
-    const R* __restrict__ tb =
-        a.tab + ((size_t)(k >> tlw) * NX << tlw) + (k & (tW - 1)) + ((size_t)tt << tlw);
+    // the table's row of register q: its frequency index along x
+    const R* __restrict__ tb = a.tab + ((size_t)(k >> tlw) * NX << tlw) + (k & (tW - 1)) +
+                               (P::F == 1 ? (size_t)tt << tlw : 0);
 #pragma unroll
-    for (int q = 0; q < E; ++q)
-      v[q] = cscale(v[q], ok ? __ldg(tb + ((size_t)(q * P::TPS) << tlw)) : (R)0);
+    for (int q = 0; q < E; ++q) {
+      const size_t row = P::F == 1 ? (size_t)(q * P::TPS) : (size_t)kfreq<LOGX, Sh::LR>(tt, q);
+      v[q] = cscale(v[q], ok ? __ldg(tb + (row << tlw)) : (R)0);
+    }
     __syncthreads();
-    fft_p2x<C, true, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
+    fft_len<C, true, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
     col_pack_store<C, P::TPS, W, E>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
     __syncthreads();  // buffers free for the next group
   }
@@ -308,8 +335,8 @@ template <typename R, int LOGN>
 __global__ void __launch_bounds__(OpShape<R, LOGN>::THREADS, OpShape<R, LOGN>::MINB)
 k_op_row_inv(OpArgs<R> a) {
   typedef typename CT<R>::C C;
-  typedef P2PlanR<LOGN, OpShape<R, LOGN>::LR> P;
   typedef OpShape<R, LOGN> Sh;
+  typedef typename Sh::P P;
   constexpr int N = P::N, NP = Sh::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = reinterpret_cast<C*>(smem_raw);
@@ -324,10 +351,10 @@ k_op_row_inv(OpArgs<R> a) {
   for (int p0 = blockIdx.x * NP; p0 < npairs; p0 += gridDim.x * NP) {
     const int p = p0 + s, xa = 2 * p;
     C v[Sh::E];
-    const C* __restrict__ row = a.spec + (size_t)p * N + tt;
+    const C* __restrict__ row = a.spec + (size_t)p * N;
 #pragma unroll
-    for (int q = 0; q < Sh::E; ++q) v[q] = p < npairs ? row[q * P::TPS] : czero<C>();
-    fft_p2x<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    for (int q = 0; q < Sh::E; ++q) v[q] = p < npairs ? row[kfreq<LOGN, Sh::LR>(tt, q)] : czero<C>();
+    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;

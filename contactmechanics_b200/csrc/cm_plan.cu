@@ -580,6 +580,18 @@ static int log2_exact(int n) {
   return (1 << l) == n ? l : -1;
 }
 
+// Length code of the register-resident passes for a domain side
+// (cm_fft_p2.cuh): log2 n for n = 2^k, 32 + m for n = 3 * 2^m, -1 otherwise.
+static int len_code(int n) {
+  const int l = log2_exact(n);
+  if (l >= 0) return l;
+  if (n % 3 == 0) {
+    const int m = log2_exact(n / 3);
+    if (m >= 0) return 32 + m;
+  }
+  return -1;
+}
+
 static int grid_for(long n) {
   long g = (n + 255) / 256;
   if (g > 148L * 16) g = 148L * 16;
@@ -707,8 +719,8 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
   CK(cudaMemcpyAsync(w.d_ccg, &s, sizeof(s), cudaMemcpyHostToDevice, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   {
-    // by-value passes for power-of-two domains (single solves)
-    const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+    // by-value passes for domain sides 2^k and 3 * 2^m (single solves)
+    const int lx = len_code(p->nx), ly = len_code(p->ny);
     CcgArgs<R>& a = w.ccg_args;
     a.op.in = nullptr;
     a.op.out = nullptr;
@@ -744,6 +756,7 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
     a.ew_grid = 0;
     a.u_rows = p->nx;
     a.fuse_gsum = 0;
+    a.ew_vpr = make_fastdiv((unsigned)(p->ty / (16 / (int)sizeof(R))));
     w.by_value = CM_BY_VALUE_PASSES && lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw);
     if (w.by_value) {
       const int rc = ccg_p2_prepare<R>(a, lx, ly);
@@ -774,7 +787,7 @@ static int ensure_ccg(cm_plan* p, Work<R>& w) {
       if (w.ew_grid[4] && !w.bar) CKS(dalloc(p, &w.bar, 1));
       // the vectorised element-wise passes (gsum, force update): one resident
       // wave, no more blocks than vectors to walk or reduction partials
-      const int ew_per_sm = ccg_p2_ew_blocks_per_sm<R>();
+      const int ew_per_sm = ccg_p2_ew_blocks_per_sm<R>(a);
       if (ew_per_sm < 1) return CM_ERR_CUDA;
       const long nvec = (long)p->tx * p->ty / (16 / (long)sizeof(R));
       const long need = (nvec + 2L * 256 - 1) / (2L * 256);
@@ -801,8 +814,8 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
   hs.out_ld = out_ld;
   hs.table_sel = table_sel;
   if (mode == MODE_PLAIN) {
-    // power-of-two domains: the by-value operator passes (cm_op_p2.cuh)
-    const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+    // domain sides 2^k and 3 * 2^m: the by-value operator passes (cm_op_p2.cuh)
+    const int lx = len_code(p->nx), ly = len_code(p->ny);
     if (lx > 0 && ly > 0 && op_p2_supported<R>(lx, ly, w.tiles.lw)) {
       OpArgs<R> a;
       a.in = in;
@@ -851,10 +864,10 @@ static int launch_plain(cm_plan* p, Work<R>& w, int mode, int table_sel, const R
 }
 
 // G = Re FFT2(in) of a real FP64 domain field in the natural (nx, nyh) layout,
-// by the power-of-two row pass and a forward-only column pass; -1 when the
-// domain has no power-of-two passes
+// by the register-resident row pass and a forward-only column pass; -1 when
+// the domain has no such passes
 static int forward_real_p2(cm_plan* p, const double* in, double* out, cudaStream_t s) {
-  const int lx = log2_exact(p->nx), ly = log2_exact(p->ny);
+  const int lx = len_code(p->nx), ly = len_code(p->ny);
   if (!(lx > 0 && ly > 0 && op_p2_supported<double>(lx, ly, p->w64.tiles.lw))) return -1;
   set_smem_attrs<double>();
   OpArgs<double> a;
@@ -964,7 +977,7 @@ static void launch_iteration(cm_plan* p, Work<R>& w, bool bisect, cudaStream_t s
   }
   mark();
   const int ly = p->fy.n, lx = p->fx.n;
-  const int ry = log2_exact(ly), rx = log2_exact(lx);
+  const int ry = len_code(ly), rx = len_code(lx);
   if (w.by_value) {
     // by-value passes: one launch each; a launch error surfaces at the next check
     const CcgArgs<R>& a = w.ccg_args;
@@ -1957,6 +1970,16 @@ int cm_plan_shape(const cm_plan* p, int* nxd, int* nyd, int* nyh) {
   if (nxd) *nxd = p->nx;
   if (nyd) *nyd = p->ny;
   if (nyh) *nyh = p->nyh;
+  return CM_OK;
+}
+
+int cm_plan_engine(const cm_plan* p, int precision, int* engine) {
+  if (!p || !engine || (precision != CM_FP64 && precision != CM_FP32)) return CM_ERR_ARG;
+  const int lx = len_code(p->nx), ly = len_code(p->ny);
+  const bool ok = lx > 0 && ly > 0 &&
+                  (precision == CM_FP64 ? op_p2_supported<double>(lx, ly, p->w64.tiles.lw)
+                                        : op_p2_supported<float>(lx, ly, p->w32.tiles.lw));
+  *engine = ok ? 1 : 0;
   return CM_OK;
 }
 

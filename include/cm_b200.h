@@ -173,6 +173,15 @@ int cm_plan_destroy(cm_plan* plan);
 int cm_plan_shape(const cm_plan* plan, int* nxd, int* nyd, int* nyh);
 
 /*
+ * Which transform engine serves the plan's operator and single solves in
+ * `precision` (CM_FP64 or CM_FP32): *engine = 1 for the register-resident
+ * passes (domain sides 2^k and 3 * 2^m), 0 for the shared-memory
+ * mixed-radix passes of every other size.  No counterpart in the reference
+ * (numpy's FFT serves every size there).
+ */
+int cm_plan_engine(const cm_plan* plan, int precision, int* engine);
+
+/*
  * Copy the unscaled FP64 Green's table G(q) (surface displacement per unit
  * pressure in Fourier space) to host memory, layout (nxd, nyh) with the half
  * spectrum along y.  The reference stores the same real values halved along
