@@ -529,18 +529,20 @@ def run_plastic(reps=2):
 
 def run_operator(reps=50):
     """The standalone operator (evaluate_disp, device-resident fields) on the
-    C4 grid and the free 1024^2 grid: microseconds per call from CUDA events
-    around `reps` back-to-back calls, and the operator's algorithmic bytes
-    p (N + N_d) + p_t N_h against the measured HBM peak."""
+    C4 grid, the free 1024^2 grid and a periodic 3072^2 grid (sides 3 * 2^m):
+    microseconds per call from CUDA events around `reps` back-to-back calls,
+    and the operator's algorithmic bytes p (N + N_d) + p_t N_h against the
+    measured HBM peak."""
     import torch
     import contactmechanics_b200 as cm
     from contactmechanics_b200 import _lib
     L = _lib.lib()
     peak, peak_kind = peaks()
-    out = {"workload": "evaluate_disp on device-resident fields; periodic 2048^2 and free "
-                       "1024^2 (2048^2 domain); cufft_us: torch.fft.rfft2 x table x irfft2 "
-                       "(cuFFT) on the same fields", "peak_gbs": peak, "peak_source": peak_kind}
-    for kind, n in (("periodic", 2048), ("free", 1024)):
+    out = {"workload": "evaluate_disp on device-resident fields; periodic 2048^2, free "
+                       "1024^2 (2048^2 domain) and periodic 3072^2; cufft_us: torch.fft.rfft2 "
+                       "x table x irfft2 (cuFFT) on the same fields", "peak_gbs": peak,
+           "peak_source": peak_kind}
+    for kind, n in (("periodic", 2048), ("free", 1024), ("periodic", 3072)):
         cls = cm.FreeFFTElasticHalfSpace if kind == "free" else cm.PeriodicFFTElasticHalfSpace
         sub = cls((n, n), 1.0, (1.0, 1.0))
         nxd, nyd = sub.nb_domain_grid_pts
