@@ -599,14 +599,13 @@ def run_operator(reps=50):
 # serving: the request mix of the serving workload through the continuous-
 # batching loop
 # ---------------------------------------------------------------------------
-# sides log-uniform 64..4096 rounded to the nearest 7-smooth size of this set
-# (no Bluestein transform is needed); a free 3072 side would have a 6144-point
-# domain that neither the power-of-two passes nor the FP64 per-pass kernels
-# hold, so free requests round to the set without it
+# sides log-uniform 64..4096 rounded to the nearest size of this set (sides
+# 2^k and 3 * 2^m, which the register-resident passes serve; a free 3072 side
+# has a 6144-point domain)
 C5_SIDES = (64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096)
-C5_FREE_SIDES = tuple(x for x in C5_SIDES if x != 3072)
+C5_FREE_SIDES = C5_SIDES
 C5_WORKLOAD = ("requests with side log-uniform 64..4096 rounded to {64,96,128,192,256,384,512,768,"
-               "1024,1536,2048,3072,4096} (free: without 3072); 30% free (domain x2), 20% plastic "
+               "1024,1536,2048,3072,4096}; 30% free (domain x2), 20% plastic "
                "with hardness U[0.02,0.1] E*; mean pressure log-uniform 1e-4..1e-2 E*; self-affine "
                "H 0.8 slope 0.1 surfaces (8 seeds per side up to 1024, 2 above); pentol "
                "1e-9*(max h-min h), forcetol 1e-12*F (1e-9*F plastic); mixed precision")

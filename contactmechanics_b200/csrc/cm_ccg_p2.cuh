@@ -181,7 +181,7 @@ k_ccg_row_fwd(CcgArgs<R> a) {
     C v[Sh::E];
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = cmake<C>(out[0][q], out[1][q]);
-    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, s * N, 1, tt, tw);
     if (xa < tx) {
       C* __restrict__ srow = a.op.spec + (size_t)(xa >> 1) * N;
 #pragma unroll
@@ -257,7 +257,7 @@ k_ccg_row_inv(CcgArgs<R> a) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) v[q] = have ? srow[kfreq<LOGN, Sh::LR>(tt, q)] : czero<C>();
     }
-    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, s * N, 1, tt, tw);
     if (MODE == MODE_T) {
 #pragma unroll
       for (int q = 0; q < Sh::E; ++q) {

@@ -210,8 +210,10 @@ CM_DEVINL const C* stage_twiddles(C* tws, const C* __restrict__ tw_n) {
 // Transform G sequences of the thread's RAD elements {tt + q N/RAD} each in
 // place: group g is v[g RAD .. g RAD + RAD - 1] and lives at shared offset
 // base + g gstride (tables of stage_tw_p2r; the result is left in v with no
-// pending shared-memory reads).  The groups share every barrier.
-template <typename C, bool INV, int LOGN, int LR, int G>
+// pending shared-memory reads).  The groups share every barrier.  ONE: sA
+// and sB are the same buffer, so every stage reads all of its groups into
+// registers, waits, and only then writes (one barrier more per stage).
+template <typename C, bool INV, int LOGN, int LR, int G, bool ONE = false>
 CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int estride, int tt,
                        const C* tw) {
   typedef P2PlanR<LOGN, LR> P;
@@ -253,12 +255,23 @@ CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int
 #pragma unroll
   for (int s = 1; s < P::NST; ++s) {
     const int k = tt & (Ns - 1);
+    if constexpr (ONE) {
+      // every read of the stage before the buffer is rewritten
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int bg = base + g * gstride;
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) v[g * RAD + q] = src[spad(bg + (tt + q * P::TPS) * estride)];
+      }
+      if (s < P::NST - 1) __syncthreads();
+    }
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       const int bg = base + g * gstride;
       C e[RAD];
 #pragma unroll
-      for (int q = 0; q < RAD; ++q) e[q] = src[spad(bg + (tt + q * P::TPS) * estride)];
+      for (int q = 0; q < RAD; ++q)
+        e[q] = ONE ? v[g * RAD + q] : src[spad(bg + (tt + q * P::TPS) * estride)];
 #pragma unroll
       for (int q = 1; q < RAD; ++q) {
         const C w = tw[toff + (q - 1) * Ns + k];
@@ -376,7 +389,7 @@ CM_DEVINL void fft_p2x(C (&v)[1 << LR], C* bufA, C* bufB, int base, int estride,
 // X(3k + j) over k, the twiddle W_N^(-j n), the radix-3 combination), again
 // unnormalised, leaving x(n + r M) in v[qq + r RAD].  Sub-sequence j lives at
 // shared offset base + j M estride; tw holds the tables of stage_tw_t3.
-template <typename C, bool INV, int LOGM, int LR>
+template <typename C, bool INV, int LOGM, int LR, bool ONE = false>
 CM_DEVINL void fft_t3(C (&v)[3 << LR], C* sA, C* sB, int base, int estride, int tt, const C* tw) {
   typedef P2PlanR<LOGM, LR> P;
   typedef decltype(v[0].x) R;
@@ -396,9 +409,9 @@ CM_DEVINL void fft_t3(C (&v)[3 << LR], C* sA, C* sB, int base, int estride, int 
       v[qq + RAD] = cmul(cadd(md, rt), w3[n]);
       v[qq + 2 * RAD] = cmul(csub(md, rt), w3[2 * n]);
     }
-    fft_p2g<C, false, LOGM, LR, 3>(v, sA, sB, base, M * estride, estride, tt, tw);
+    fft_p2g<C, false, LOGM, LR, 3, ONE>(v, sA, sB, base, M * estride, estride, tt, tw);
   } else {
-    fft_p2g<C, true, LOGM, LR, 3>(v, sA, sB, base, M * estride, estride, tt, tw);
+    fft_p2g<C, true, LOGM, LR, 3, ONE>(v, sA, sB, base, M * estride, estride, tt, tw);
 #pragma unroll
     for (int qq = 0; qq < RAD; ++qq) {
       const int n = tt + qq * P::TPS;
@@ -415,13 +428,19 @@ CM_DEVINL void fft_t3(C (&v)[3 << LR], C* sA, C* sB, int base, int estride, int 
 }
 
 // The transform of length code L: fft_p2x for 2^L, fft_t3 for 3 * 2^m.
-template <typename C, bool INV, int L, int LR, bool ONEBUF>
+// ONEBUF: one buffer, twiddles read from the global table (2^L only);
+// ONESTG: one buffer (bufA), staged twiddles.
+template <typename C, bool INV, int L, int LR, bool ONEBUF, bool ONESTG = false>
 CM_DEVINL void fft_len(C (&v)[FftLen<L, LR>::E], C* bufA, C* bufB, int base, int estride, int tt,
                        const C* tw) {
   if constexpr (LenCode<L>::F == 1) {
-    fft_p2x<C, INV, L, LR, ONEBUF>(v, bufA, bufB, base, estride, tt, tw);
+    if constexpr (ONESTG)
+      fft_p2g<C, INV, L, LR, 1, true>(v, bufA, bufA, base, 0, estride, tt, tw);
+    else
+      fft_p2x<C, INV, L, LR, ONEBUF>(v, bufA, bufB, base, estride, tt, tw);
   } else {
-    static_assert(!ONEBUF, "lengths 3 * 2^m keep both transform buffers");
-    fft_t3<C, INV, LenCode<L>::LOGM, LR>(v, bufA, bufB, base, estride, tt, tw);
+    static_assert(!ONEBUF, "lengths 3 * 2^m stage their twiddles");
+    fft_t3<C, INV, LenCode<L>::LOGM, LR, ONESTG>(v, bufA, ONESTG ? bufA : bufB, base, estride, tt,
+                                                 tw);
   }
 }

@@ -118,7 +118,8 @@ constexpr int row_lr(int code) {
 // LOGN (2^LOGN, or 3 * 2^m for LOGN = CM_T3(m)) with 2^LRV elements of each
 // power-of-two part per thread.  ONEBUF: the ping-pong buffers and the
 // staged twiddles do not fit a block's shared memory (FP64 at 2^13), so the
-// transform runs on one buffer with the twiddles read from global memory.
+// transform runs on one buffer with the twiddles read from global memory;
+// ONESTG: one buffer and the staged twiddles fit (FP64 at 3 * 2^11).
 template <typename R, int LOGN, int LRV = row_lr<R>(LOGN)>
 struct OpShape {
   typedef typename CT<R>::C C;
@@ -132,9 +133,12 @@ struct OpShape {
   static constexpr int THREADS = TPS > BASE ? TPS : BASE;
   static constexpr int NP = THREADS / TPS;  // row pairs per block
   static constexpr size_t BUF = (size_t)(NP * N + ((NP * N) >> 3) + 1) * sizeof(C);
-  static constexpr bool ONEBUF = (N * sizeof(C) + 2 * BUF) > CM_SMEM_DYN_MAX;
-  static constexpr size_t SMEM = ONEBUF ? BUF : N * sizeof(C) + 2 * BUF;
-  static constexpr size_t STAGE = ONEBUF ? BUF : 2 * BUF;  // bytes for staging input rows
+  static constexpr bool TWO = N * sizeof(C) + 2 * BUF <= CM_SMEM_DYN_MAX;
+  // ONESTG: one buffer with the twiddles staged (FP64 at 3 * 2^11)
+  static constexpr bool ONESTG = !TWO && N * sizeof(C) + BUF <= CM_SMEM_DYN_MAX;
+  static constexpr bool ONEBUF = !TWO && !ONESTG;
+  static constexpr size_t SMEM = TWO ? N * sizeof(C) + 2 * BUF : ONESTG ? N * sizeof(C) + BUF : BUF;
+  static constexpr size_t STAGE = TWO ? 2 * BUF : BUF;  // bytes for staging input rows
   // resident blocks per SM the kernels are compiled for; one when a block
   // holds more than half of the shared memory
   static constexpr int MINB = SMEM > CM_SMEM_DYN_MAX / 2 ? 1
@@ -167,10 +171,13 @@ struct ColShape {
   static constexpr int THREADS = GROUP > CM_COL_BASE ? GROUP : CM_COL_BASE;
   static constexpr int NG = THREADS / GROUP;  // column groups per block
   static constexpr size_t BUF = (size_t)(NG * NX * W + ((NG * NX * W) >> 3) + 1) * sizeof(C);
-  // one buffer and global twiddles when even one column's ping-pong buffers
-  // do not fit (FP64 at 2^13)
-  static constexpr bool ONEBUF = NX * sizeof(C) + 2 * BUF > CM_SMEM_DYN_MAX;
-  static constexpr size_t SMEM = ONEBUF ? BUF : NX * sizeof(C) + 2 * BUF;
+  // one buffer when even one column's ping-pong buffers do not fit: with the
+  // twiddles staged where they fit beside it (ONESTG: FP64 at 3 * 2^11),
+  // else read from the global table (ONEBUF: FP64 at 2^13)
+  static constexpr bool TWO = NX * sizeof(C) + 2 * BUF <= CM_SMEM_DYN_MAX;
+  static constexpr bool ONESTG = !TWO && NX * sizeof(C) + BUF <= CM_SMEM_DYN_MAX;
+  static constexpr bool ONEBUF = !TWO && !ONESTG;
+  static constexpr size_t SMEM = TWO ? NX * sizeof(C) + 2 * BUF : ONESTG ? NX * sizeof(C) + BUF : BUF;
   static size_t smem() { return SMEM; }
 };
 
@@ -204,7 +211,7 @@ k_op_row_fwd(OpArgs<R> a) {
       }
       v[q] = cmake<C>(ra, rb);
     }
-    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, false, LOGN, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, s * N, 1, tt, tw);
     if (p < npairs) {
       C* __restrict__ row = a.spec + (size_t)p * N;
 #pragma unroll
@@ -305,7 +312,7 @@ k_op_col(OpArgs<R> a) {
     const int km = k == 0 ? 0 : ny - k;  // the mirror column (ny need not be a power of two)
     C v[E];
     col_split_load<C, P::TPS, E>(v, a.spec, ny, k, km, tt, a.in_rows, ok);
-    fft_len<C, false, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
+    fft_len<C, false, LOGX, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, base, W, tt, tw);
     if (a.fwd_real) {
       // forward transform only: the real part of the 2D transform, in the
       // natural (nx, ny/2 + 1) layout (a real, even kernel's Green's table)
@@ -325,7 +332,7 @@ k_op_col(OpArgs<R> a) {
       v[q] = cscale(v[q], ok ? __ldg(tb + (row << tlw)) : (R)0);
     }
     __syncthreads();
-    fft_len<C, true, LOGX, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, base, W, tt, tw);
+    fft_len<C, true, LOGX, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, base, W, tt, tw);
     col_pack_store<C, P::TPS, W, E>(v, a.spec, ny, k, km, tt, a.out_rows, ok);
     __syncthreads();  // buffers free for the next group
   }
@@ -354,7 +361,7 @@ k_op_row_inv(OpArgs<R> a) {
     const C* __restrict__ row = a.spec + (size_t)p * N;
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) v[q] = p < npairs ? row[kfreq<LOGN, Sh::LR>(tt, q)] : czero<C>();
-    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF>(v, bufA, bufB, s * N, 1, tt, tw);
+    fft_len<C, true, LOGN, Sh::LR, Sh::ONEBUF, Sh::ONESTG>(v, bufA, bufB, s * N, 1, tt, tw);
 #pragma unroll
     for (int q = 0; q < Sh::E; ++q) {
       const int y = tt + q * P::TPS;

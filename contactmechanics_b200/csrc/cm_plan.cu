@@ -34,6 +34,11 @@ struct NvtxRange {
 #define CM_MAX_PARTIAL_VALS 32
 #define CM_FP32_ITER_CAP 2000
 #define CM_FP32_ITER_CAP_PLASTIC 256
+// iterations the FP64 refinement of a mixed single solve may take before it
+// restarts cold: at least CM_REFINE_MIN_ITERS, else CM_REFINE_PER_FP32_ITER
+// per FP32-phase iteration (refinements seen: 10-170 iterations)
+#define CM_REFINE_MIN_ITERS 1000
+#define CM_REFINE_PER_FP32_ITER 4
 #ifndef CM_BY_VALUE_PASSES
 #define CM_BY_VALUE_PASSES 1  // single solves on power-of-two domains use cm_ccg_p2.cuh
 #endif
@@ -486,10 +491,20 @@ template <typename R>
 __global__ void k_force_to_domain(const CcgState* st, const R* f0, const R* f1, int tx, int ty,
                                   double* out, int nx, int ny) {
   const R* f = st->parity ? f1 : f0;  // the buffer holding the solver's current forces
+  // a force the phase set to the hardness cap (-H rounded to R) goes on
+  // exactly at -H, where the FP64 iteration would have put it
+  const bool cap = st->p.has_h != 0;
+  const double H = st->p.H;
+  const R fcap = (R)(-H);
   const long n = (long)nx * ny;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const int x = (int)(i / ny), y = (int)(i % ny);
-    out[i] = (x < tx && y < ty) ? (double)f[(size_t)x * ty + y] : 0.0;
+    double v = 0.0;
+    if (x < tx && y < ty) {
+      const R fv = f[(size_t)x * ty + y];
+      v = (cap && fv == fcap) ? -H : (double)fv;
+    }
+    out[i] = v;
   }
 }
 
@@ -2062,11 +2077,22 @@ int cm_ccg_solve(cm_plan* p, const cm_ccg_params* prm, const double* h, const do
   // k_init_f reads f64 before the operator overwrites u, so the borrow is safe
   SolveInput in2{h, nullptr, f64, p->ny};
   const int rem = std::max(1, prm->maxiter - nit32);
+  // A refinement that has not converged within its budget starts again
+  // cold from the caller's own start, i.e. becomes the FP64 solve (seen on a
+  // plastic request whose FP32 phase stopped at its cap: the refinement from
+  // those forces ran to maxiter, the cold FP64 solve converged in 169).
+  const int budget = std::min(rem, std::max(CM_REFINE_MIN_ITERS, CM_REFINE_PER_FP32_ITER * nit32));
   p->obs_it_offset = nit32;
-  CKS(run_ccg<double>(p, p->w64, prm, in2, 0.0, 0.0, rem, &fin));
+  CKS(run_ccg<double>(p, p->w64, prm, in2, 0.0, 0.0, budget, &fin));
+  int nit_refine = 0;
+  if (fin.status != CMS_CONVERGED && budget < rem) {
+    nit_refine = fin.it;
+    p->obs_it_offset = nit32 + nit_refine;
+    CKS(run_ccg<double>(p, p->w64, prm, in, 0.0, 0.0, rem - nit_refine, &fin));
+  }
   CKS(finish_ccg<double>(p, p->w64, x, jac, active, plastic, &fin));
   fill_result(fin, res);
-  res->nit += nit32;
+  res->nit += nit32 + nit_refine;
   res->nfev += nfev32;
   res->nit_fp32 = nit32;
   res->ms_fp32 = ms32;
