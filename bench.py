@@ -741,12 +741,21 @@ def main():
     ap.add_argument("--no-operator", action="store_true", help="skip the standalone operator")
     ap.add_argument("--profile-solve", choices=["mixed", "fp64", "fp32"], default=None,
                     help="run the first solve of the sweep once and exit (for profilers)")
+    ap.add_argument("--profile-periodic", type=int, default=0,
+                    help="with --profile-solve: a periodic N x N solve of a surface of the "
+                         "sweep's kind instead (e.g. 3072 for the 3 * 2^m passes)")
     args = ap.parse_args()
     if args.profile_solve:
         import torch
         import contactmechanics_b200 as cm
-        h = surface()
-        sub = cm.FreeFFTElasticHalfSpace((N_TOPO, N_TOPO), 1.0, (1.0, 1.0))
+        if args.profile_periodic:
+            from contactmechanics_b200.Generation import self_affine
+            n = args.profile_periodic
+            h = self_affine((n, n), (1.0, 1.0), 0.8, 0.1, seed=SEED, rolloff_wavelength=1.0 / 8)
+            sub = cm.PeriodicFFTElasticHalfSpace((n, n), 1.0, (1.0, 1.0))
+        else:
+            h = surface()
+            sub = cm.FreeFFTElasticHalfSpace((N_TOPO, N_TOPO), 1.0, (1.0, 1.0))
         F = float(PRESSURES[0])
         r = cm.constrained_conjugate_gradients(sub, torch.from_numpy(h).cuda(), external_force=F,
                                                precision=args.profile_solve, **tolerances(h, F))
