@@ -12,8 +12,8 @@ not depend on which other solves share its steps.
 
 Large requests (at least ``large_points`` domain points) skip the lockstep
 batch: ``large_workers`` worker threads solve them with the single-solve
-path (``constrained_conjugate_gradients``, which on power-of-two domains runs
-the by-value passes of a CUDA graph on the plan's own stream), each one
+path (``constrained_conjugate_gradients``, which on domains with sides 2^k or
+3 * 2^m runs the by-value passes of a CUDA graph on the plan's own stream), each one
 request at a time, while the loop keeps stepping the small ones; the
 single-solve passes are latency-bound, so two large solves on their own
 streams overlap on the device.  Their results are those of

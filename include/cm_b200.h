@@ -347,7 +347,8 @@ int cm_selftest_grid_barrier(int blocks, int phantom, double limit_us, int* gave
 
 /*
  * Tuning of the per-pass kernels that batched solves (cm_ccg_solve_batch),
- * the stepping interface and sizes without power-of-two passes run.
+ * the stepping interface and sizes without register-resident passes (sides
+ * other than 2^k and 3 * 2^m) run.
  * cm_tuning_set_tiles: transform elements per row or column tile for
  * sequences of `length` points (a row tile of a domain with ny columns holds
  * tile_elems / ny rows, a column tile up to tile_elems / nx columns), for
