@@ -89,6 +89,19 @@ CM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned lon
       : "memory");
 }
 
+// Hint: start bringing [p, p + bytes) into L2 ahead of the loads that will
+// read it.  Nothing is returned and nothing waits on it; L2 is the point of
+// coherence, so a range written later by another kernel is still read
+// correctly.  Skipped unless p is 16-byte aligned and bytes a multiple of 16.
+CM_DEVINL void prefetch_l2(const void* p, size_t bytes) {
+  if (bytes == 0 || ((reinterpret_cast<size_t>(p) | bytes) & 15) != 0) return;
+  const char* c = static_cast<const char*>(p);
+  for (size_t o = 0; o < bytes; o += 32768) {
+    const unsigned n = (unsigned)(bytes - o < 32768 ? bytes - o : 32768);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + o), "r"(n) : "memory");
+  }
+}
+
 CM_DEVINL bool mbar_try_wait(unsigned long long* b, unsigned parity) {
   unsigned done;
   asm volatile(
