@@ -757,9 +757,9 @@ def main():
             h = surface()
             sub = cm.FreeFFTElasticHalfSpace((N_TOPO, N_TOPO), 1.0, (1.0, 1.0))
         F = float(PRESSURES[0])
-        # the periodic case stops after 400 iterations: an FP32 solve does not
-        # reach the sweep's FP64 tolerance, and a profiler needs only a few
-        extra = {"maxiter": 400} if args.profile_periodic else {}
+        # FP32 solves stop after 400 iterations: they need not reach the
+        # sweep's FP64 tolerance, and a profiler needs only a few
+        extra = {"maxiter": 400} if args.profile_periodic or args.profile_solve == "fp32" else {}
         r = cm.constrained_conjugate_gradients(sub, torch.from_numpy(h).cuda(), external_force=F,
                                                precision=args.profile_solve, **tolerances(h, F),
                                                **extra)
