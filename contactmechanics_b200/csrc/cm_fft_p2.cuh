@@ -243,7 +243,7 @@ CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int
     for (int i = 0; i < B; ++i) {
       const int j = tt + i * P::TPS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) sA[spad(bg + (j * R + q) * estride)] = o[i * R + q];
+      for (int q = 0; q < R; ++q) sA[spad_t<sizeof(C)>(bg + (j * R + q) * estride)] = o[i * R + q];
     }
   }
   if (P::NST == 1) return;
@@ -261,7 +261,7 @@ CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int
       for (int g = 0; g < G; ++g) {
         const int bg = base + g * gstride;
 #pragma unroll
-        for (int q = 0; q < RAD; ++q) v[g * RAD + q] = src[spad(bg + (tt + q * P::TPS) * estride)];
+        for (int q = 0; q < RAD; ++q) v[g * RAD + q] = src[spad_t<sizeof(C)>(bg + (tt + q * P::TPS) * estride)];
       }
       if (s < P::NST - 1) __syncthreads();
     }
@@ -271,7 +271,7 @@ CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int
       C e[RAD];
 #pragma unroll
       for (int q = 0; q < RAD; ++q)
-        e[q] = ONE ? v[g * RAD + q] : src[spad(bg + (tt + q * P::TPS) * estride)];
+        e[q] = ONE ? v[g * RAD + q] : src[spad_t<sizeof(C)>(bg + (tt + q * P::TPS) * estride)];
 #pragma unroll
       for (int q = 1; q < RAD; ++q) {
         const C w = tw[toff + (q - 1) * Ns + k];
@@ -284,7 +284,7 @@ CM_DEVINL void fft_p2g(C (&v)[G << LR], C* sA, C* sB, int base, int gstride, int
       } else {
         const int ob = (tt - k) * RAD + k;
 #pragma unroll
-        for (int q = 0; q < RAD; ++q) dst[spad(bg + (ob + q * Ns) * estride)] = e[q];
+        for (int q = 0; q < RAD; ++q) dst[spad_t<sizeof(C)>(bg + (ob + q * Ns) * estride)] = e[q];
       }
     }
     toff += (RAD - 1) * Ns;
@@ -338,7 +338,7 @@ CM_DEVINL void fft_p2r_1buf(C (&v)[1 << LR], C* buf, int base, int estride, int 
     for (int i = 0; i < B; ++i) {
       const int j = tt + i * P::TPS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) buf[spad(base + (j * R + q) * estride)] = o[i * R + q];
+      for (int q = 0; q < R; ++q) buf[spad_t<sizeof(C)>(base + (j * R + q) * estride)] = o[i * R + q];
     }
   }
   __syncthreads();
@@ -349,7 +349,7 @@ CM_DEVINL void fft_p2r_1buf(C (&v)[1 << LR], C* buf, int base, int estride, int 
     const int step = N / (Ns * RAD);
     C g[RAD];
 #pragma unroll
-    for (int q = 0; q < RAD; ++q) g[q] = buf[spad(base + (tt + q * P::TPS) * estride)];
+    for (int q = 0; q < RAD; ++q) g[q] = buf[spad_t<sizeof(C)>(base + (tt + q * P::TPS) * estride)];
 #pragma unroll
     for (int q = 1; q < RAD; ++q) {
       const C w = __ldg(tw_n + ((q * k * step) & (N - 1)));
@@ -363,7 +363,7 @@ CM_DEVINL void fft_p2r_1buf(C (&v)[1 << LR], C* buf, int base, int estride, int 
       __syncthreads();  // every read of this stage is done before the buffer is rewritten
       const int ob = (tt - k) * RAD + k;
 #pragma unroll
-      for (int q = 0; q < RAD; ++q) buf[spad(base + (ob + q * Ns) * estride)] = g[q];
+      for (int q = 0; q < RAD; ++q) buf[spad_t<sizeof(C)>(base + (ob + q * Ns) * estride)] = g[q];
       __syncthreads();
     }
     Ns *= RAD;
