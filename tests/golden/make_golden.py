@@ -86,6 +86,23 @@ def main(ref_root):
         out[f"op_{name}_u"] = upad
         out[f"op_{name}_force"] = s.evaluate_force(upad)
 
+    # periodic grids with sides 3 * 2^m (the register-resident 3 * 2^m
+    # passes), on their own random stream so the vectors above are unchanged
+    rng3 = np.random.default_rng(20261204)
+    for name, nb, sizes, kw in [("p96x96", (96, 96), (1.3, 0.7), {}),
+                                ("p96x128_poisson", (96, 128), (2.0, 1.0), dict(poisson=0.3))]:
+        s = PeriodicFFTElasticHalfSpace(nb, 1.7, sizes, **kw)
+        out[f"op_{name}_config"] = np.array(json.dumps(dict(
+            kind="periodic", nb_grid_pts=list(nb), physical_sizes=list(sizes),
+            young=1.7, kwargs=kw)))
+        f = rng3.standard_normal(nb)
+        u = rng3.standard_normal(nb)
+        out[f"op_{name}_G"] = s.greens_function
+        out[f"op_{name}_f"] = f
+        out[f"op_{name}_u"] = u
+        out[f"op_{name}_disp"] = s.evaluate_disp(f)
+        out[f"op_{name}_force"] = s.evaluate_force(u)
+
     # ---- solves -----------------------------------------------------------
     from refstubs import Topography, PlasticTopography
 
