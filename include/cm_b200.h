@@ -53,7 +53,10 @@ extern "C" {
 /* precisions */
 #define CM_FP64 0   /* everything in FP64 */
 #define CM_FP32 1   /* FP32 fields and FFTs, FP64 reductions and scalars */
-#define CM_MIXED 2  /* FP32 solve, then FP64 refinement of the same solve */
+#define CM_MIXED 2  /* FP32 solve, then FP64 refinement of the same solve; a
+                       single solve's refinement that has not converged
+                       within max(1000, 4 x its FP32 iterations) restarts as
+                       the FP64 solve from the caller's own start */
 
 /* stiffness at q = 0 for periodic substrates */
 #define CM_Q0_DEFAULT 0  /* mean of the two lowest non-zero stiffnesses */
@@ -138,7 +141,8 @@ typedef struct {
 
 typedef struct {
   int status;            /* CM_SOLVE_CONVERGED or CM_SOLVE_MAXITER */
-  int nit, nfev;         /* iterations / operator calls (all phases) */
+  int nit, nfev;         /* iterations / operator calls (all phases, an
+                            abandoned refinement included) */
   int nit_fp32;          /* iterations run in FP32 (CM_MIXED / CM_FP32) */
   int last_step_mix;     /* 1 if the last iteration was a mixing step */
   double offset, fun;
